@@ -1,0 +1,202 @@
+/*
+ * snow_b200.h -- C ABI of libsnowb200.so, a B200 (sm_100a) implementation of the
+ * SnowSimulation per-substep solver.
+ *
+ * Every entry point replaces one function of the reference's CUDA host interface
+ * (cuda_simulation.cuh:13-75 and the host wrappers in cuda_simulation.cu); the
+ * citation is given beside each.  The reference passes C++ objects (ParticleSet*,
+ * CellData, SceneParams&); this ABI takes the same data as plain C structs of
+ * device pointers whose layout is identical to the reference's structs
+ * (ParticleDeviceData, CellData, SimParams, SceneParams), so a caller can pass
+ * &particle_set->m_device_data unchanged.  INTEGRATION.md shows the C++ shim that
+ * restores the reference's exact signatures on top of this ABI.
+ *
+ * Conventions (all entry points):
+ *   - buffers are owned by the caller and live in device memory of the current device;
+ *   - every function returns SNOWB_OK (0) or a negative SNOWB_ERR_* code and never
+ *     calls exit(); snowb_last_error_string() describes the last failure;
+ *   - work is issued on the stream set by snowb_set_stream (default: legacy stream 0).
+ */
+#ifndef SNOW_B200_H
+#define SNOW_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SNOWB_OK 0
+#define SNOWB_ERR_INVALID (-1)      /* bad argument (null pointer, size, grid) */
+#define SNOWB_ERR_CUDA (-2)         /* a CUDA runtime call failed */
+#define SNOWB_ERR_NO_PARAMS (-3)    /* snowb_set_sim_params was never called */
+#define SNOWB_ERR_DEVICE (-4)       /* a kernel reported an error flag */
+
+typedef struct snowb_float3 { float x, y, z; } snowb_float3;
+
+/* ParticleDeviceData (Particle.h:14-52): per-particle device arrays in original-index
+ * order, each sized full_size (connect_record / connect_length: full_size*maximum_connection,
+ * new_end: one element). */
+typedef struct snowb_particle_data {
+    snowb_float3 *positions, *predict_positions, *new_positions, *velocity, *force, *correction;
+    float *mass, *massInv, *density, *C, *lambda, *volume;
+    float *T, *new_T;
+    float *contrib;
+    float *mass_scale;
+    uint32_t *predicate, *scan_index, *new_end;
+    uint32_t *connect_record, *iter_end;
+    float *connect_length;
+    uint32_t *new_index;
+    uint32_t *trackId;
+} snowb_particle_data;
+
+/* CellData (NeighborSearch.h:19-26): grid_hash/grid_index/sorted_pos sized to the set,
+ * cell_start/cell_end sized num_cells. */
+typedef struct snowb_cell_data {
+    uint32_t *grid_hash, *grid_index, *cell_start, *cell_end;
+    snowb_float3 *sorted_pos;
+} snowb_cell_data;
+
+/* SimParams (SimParams.h:7-62), member for member. */
+typedef struct snowb_sim_params {
+    float gravity[3];
+    float global_damping, maximum_speed, minimum_speed;
+    float epsilon, pbd_epsilon, kernel_epsilon, effective_radius, particle_radius;
+    float rest_density, scorr_coeff, scorr_divisor;
+    float boundary_damping, static_friction, kinematic_friction;
+    float k_stretch;
+    float k_water, k_snow, C_water, C_snow, freezing_point;
+    float blending_speed;
+    float sor_coeff, sph_viscosity, dem_viscosity;
+    float world_origin[3];
+    float cell_size[3];
+    uint32_t grid_size[3];
+    uint32_t num_cells;
+    float poly6, poly6_G, spiky, spiky_G, viscosity_laplacian;
+    uint32_t maximum_connection;
+    float T_homogeneous, k_refreezing, break_threshold;
+} snowb_sim_params;
+
+/* SceneParams (SceneParams.h:4-9). */
+typedef struct snowb_scene_params {
+    float fluid_start_time, solid_start_time, current_time;
+} snowb_scene_params;
+
+/* Quirk modes.  REFERENCE (default) reproduces the reference's deterministic
+ * behaviour including its defects (partial cell-table clear, own-cell heat sum x27,
+ * SPH index used for new snow particles, stale launch sizes after a phase change,
+ * XSPH of the snow set limited to the water launch size, unseeded coupling s_corr
+ * taken as 0).  FIXED applies the intended physics for each of those. */
+#define SNOWB_QUIRKS_REFERENCE 0
+#define SNOWB_QUIRKS_FIXED 1
+
+/* Options of snowb_snow_simulation_ex. */
+typedef struct snowb_step_options {
+    int quirks;          /* SNOWB_QUIRKS_* */
+    int substeps;        /* substeps to run back to back (sizes stay on the device between them); >= 1 */
+    int stop_after;      /* debugging: 0 = full substep, else stop after the numbered stage */
+    int use_graph;       /* 1: capture the substep in a CUDA graph and replay it for substeps >= 2 */
+    int sync;            /* 1: wait for completion and write the new set sizes back (required by
+                            the reference contract; 0 leaves *sph_size/*dem_size untouched and
+                            the sizes on the device, see snowb_read_sizes) */
+} snowb_step_options;
+
+/* ---- reference interface (cuda_simulation.cuh:13-75) ---------------------------------- */
+
+/* allocate_array (cuda_simulation.cu:1410-1413) */
+int snowb_allocate_array(void** dev_ptr, size_t size);
+
+/* set_sim_params (cuda_simulation.cu:1415-1419): the constants for all later calls. */
+int snowb_set_sim_params(const snowb_sim_params* params);
+
+/* compute_grid_size (cuda_simulation.cu:348-357): the reference's 1-D launch shape. */
+int snowb_compute_grid_size(uint32_t n, uint32_t block_size, uint32_t* num_blocks, uint32_t* num_threads);
+
+/* calculate_hash (cuda_simulation.cu:359-375 / calcHashD :194-212):
+ * grid_hash[i] = cell hash of pos[i], grid_index[i] = i. */
+int snowb_calculate_hash(snowb_cell_data cell_data, const snowb_float3* pos, uint32_t num_particles);
+
+/* sort_particles (cuda_simulation.cu:1455-1468): stable sort of (grid_hash, grid_index) by hash. */
+int snowb_sort_particles(snowb_cell_data cell_data, uint32_t num_particles);
+
+/* reorder_data (cuda_simulation.cu:377-396 / reorderDataAndFindCellStartD :242-301):
+ * clears cell_start[0, num_cells), writes cell_start/cell_end of occupied cells and
+ * sorted_pos[i] = old_pos[grid_index[i]]. */
+int snowb_reorder_data(snowb_cell_data cell_data, const snowb_float3* old_pos, uint32_t num_particles,
+                       uint32_t num_cells);
+
+/* compute_boundary_volume (cuda_simulation.cu:422-433 / :303-346): Akinci boundary volume. */
+int snowb_compute_boundary_volume(snowb_cell_data cell_data, float* mass, float* volume, uint32_t num_particles);
+
+/* integrate_pbd (cuda_simulation.cu:1422-1453): gravity, walls, speed clamp, prediction. */
+int snowb_integrate_pbd(snowb_particle_data* particles, float dt, uint32_t num_particles, int cd_on);
+
+/* connect_and_record (cuda_simulation.cu:4286-4292): interlink formation pass over the
+ * snow set; the cell data must come from a sort of the same positions. */
+int snowb_connect_and_record(snowb_particle_data* dem, uint32_t dem_size, snowb_cell_data dem_cell_data,
+                             int dynamic_max_connections);
+
+/* snow_simulation (cuda_simulation.cu:4861-5157): one substep.  *sph_size / *dem_size are
+ * ParticleSet::m_size on entry and receive the sizes after freezing/melting (the reference
+ * calls ParticleSet::setSize); scene->current_time advances by dt. */
+int snowb_snow_simulation(snowb_particle_data* sph, uint32_t* sph_size,
+                          snowb_particle_data* dem, uint32_t* dem_size,
+                          snowb_particle_data* boundary, uint32_t boundary_size,
+                          uint32_t full_size,
+                          snowb_particle_data* phase_change_buffer,
+                          snowb_cell_data sph_cell_data, snowb_cell_data dem_cell_data,
+                          snowb_cell_data b_cell_data,
+                          snowb_scene_params* scene_params,
+                          float dt, int iterations,
+                          int sph_dem_correction, int sph_sph_correction, int dem_friction,
+                          int compute_temperature, int change_phase, int simulate_freezing,
+                          int simulate_melting, int dem_viscosity, int use_interlink,
+                          int dynamic_max_connections, int cd_on, float temperature_variation);
+
+/* ---- extensions (no reference counterpart) -------------------------------------------- */
+
+/* snow_simulation with options (quirk mode, several substeps per call, CUDA graph replay). */
+int snowb_snow_simulation_ex(snowb_particle_data* sph, uint32_t* sph_size,
+                             snowb_particle_data* dem, uint32_t* dem_size,
+                             snowb_particle_data* boundary, uint32_t boundary_size,
+                             uint32_t full_size,
+                             snowb_particle_data* phase_change_buffer,
+                             snowb_cell_data sph_cell_data, snowb_cell_data dem_cell_data,
+                             snowb_cell_data b_cell_data,
+                             snowb_scene_params* scene_params,
+                             float dt, int iterations,
+                             int sph_dem_correction, int sph_sph_correction, int dem_friction,
+                             int compute_temperature, int change_phase, int simulate_freezing,
+                             int simulate_melting, int dem_viscosity, int use_interlink,
+                             int dynamic_max_connections, int cd_on, float temperature_variation,
+                             const snowb_step_options* options);
+
+/* Set sizes kept on the device by the last call with options->sync = 0 (blocks). */
+int snowb_read_sizes(uint32_t* sph_size, uint32_t* dem_size);
+
+/* Default quirk mode of snowb_snow_simulation (SNOWB_QUIRKS_REFERENCE initially). */
+int snowb_set_quirks(int mode);
+
+/* Stream for all later work (a cudaStream_t; NULL = legacy default stream). */
+int snowb_set_stream(void* stream);
+
+/* Block until the library's stream is idle. */
+int snowb_synchronize(void);
+
+/* FP64 reductions over the live particles: out[0] = sum m*C*T (heat energy, J),
+ * out[1..3] = sum m*v (momentum).  Computed on the GPU in double precision. */
+int snowb_energy_momentum(const snowb_particle_data* sph, uint32_t sph_size,
+                          const snowb_particle_data* dem, uint32_t dem_size, double out[4]);
+
+/* Release the library's internal device buffers (they are re-created on demand). */
+int snowb_release(void);
+
+/* Last error code and message of this thread. */
+int snowb_last_error(void);
+const char* snowb_last_error_string(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SNOW_B200_H */

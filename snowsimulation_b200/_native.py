@@ -1,0 +1,81 @@
+"""Loader for libsnowb200.so (the CUDA library) with ctypes signatures of include/snow_b200.h.
+
+There is no fallback: if the library is missing or fails to load, import of the solver
+raises, so nothing silently runs on another path.
+"""
+import ctypes as C
+import os
+
+from .abi import ParticleDeviceData, CellData, SimParams, SceneParams
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsnowb200.so")
+
+
+class StepOptions(C.Structure):
+    _fields_ = [("quirks", C.c_int), ("substeps", C.c_int), ("stop_after", C.c_int),
+                ("use_graph", C.c_int), ("sync", C.c_int)]
+
+
+# Every symbol declared in include/snow_b200.h.
+EXPORTS = (
+    "snowb_allocate_array", "snowb_set_sim_params", "snowb_compute_grid_size", "snowb_calculate_hash",
+    "snowb_sort_particles", "snowb_reorder_data", "snowb_compute_boundary_volume", "snowb_integrate_pbd",
+    "snowb_connect_and_record", "snowb_snow_simulation", "snowb_snow_simulation_ex", "snowb_read_sizes",
+    "snowb_set_quirks", "snowb_set_stream", "snowb_synchronize", "snowb_energy_momentum", "snowb_release",
+    "snowb_last_error", "snowb_last_error_string",
+)
+
+_lib = None
+
+
+class SnowError(RuntimeError):
+    pass
+
+
+def load(path=LIB_PATH):
+    """Load the CUDA library once; raise if it is absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise SnowError("libsnowb200.so not built (run snowsimulation_b200/build.py): %s" % path)
+    lib = C.CDLL(path)
+    PD, PPD, CD = ParticleDeviceData, C.POINTER(ParticleDeviceData), CellData
+    u32, pu32, i, f = C.c_uint32, C.POINTER(C.c_uint32), C.c_int, C.c_float
+    sig = {
+        "snowb_allocate_array": [C.POINTER(C.c_void_p), C.c_size_t],
+        "snowb_set_sim_params": [C.POINTER(SimParams)],
+        "snowb_compute_grid_size": [u32, u32, pu32, pu32],
+        "snowb_calculate_hash": [CD, C.c_void_p, u32],
+        "snowb_sort_particles": [CD, u32],
+        "snowb_reorder_data": [CD, C.c_void_p, u32, u32],
+        "snowb_compute_boundary_volume": [CD, C.c_void_p, C.c_void_p, u32],
+        "snowb_integrate_pbd": [PPD, f, u32, i],
+        "snowb_connect_and_record": [PPD, u32, CD, i],
+        "snowb_snow_simulation": [PPD, pu32, PPD, pu32, PPD, u32, u32, PPD, CD, CD, CD,
+                                  C.POINTER(SceneParams), f, i] + [i] * 11 + [f],
+        "snowb_read_sizes": [pu32, pu32],
+        "snowb_set_quirks": [i],
+        "snowb_set_stream": [C.c_void_p],
+        "snowb_synchronize": [],
+        "snowb_energy_momentum": [PPD, u32, PPD, u32, C.POINTER(C.c_double)],
+        "snowb_release": [],
+        "snowb_last_error": [],
+    }
+    sig["snowb_snow_simulation_ex"] = sig["snowb_snow_simulation"] + [C.POINTER(StepOptions)]
+    for name, args in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = C.c_int
+    lib.snowb_last_error_string.argtypes = []
+    lib.snowb_last_error_string.restype = C.c_char_p
+    _lib = lib
+    return lib
+
+
+def check(rc):
+    if rc != 0:
+        msg = _lib.snowb_last_error_string().decode() if _lib is not None else ""
+        raise SnowError("libsnowb200 error %d: %s" % (rc, msg))
+    return rc

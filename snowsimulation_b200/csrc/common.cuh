@@ -1,0 +1,182 @@
+// common.cuh -- shared device definitions for libsnowb200 (sm_100a).
+//
+// Arithmetic contract (identical in the CPU oracle, so results are bit-exact):
+//   dot(a,b) = fma(a.z,b.z, fma(a.y,b.y, a.x*b.x)), length = sqrt(dot); sqrt and '/'
+//   correctly rounded; no other fused operation (the library is built with
+//   -fmad=false, so only the explicit __fmaf_rn calls below fuse).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "../../include/snow_b200.h"
+
+#define SNOWB_EMPTY 0xFFFFFFFFu
+#define SNOWB_UMAX 0xFFFFFFFFu
+
+namespace snowb {
+
+// Derived solver constants, passed by value to every kernel.
+struct DevParams {
+    float h, r, two_r, poly6, poly6_G, spiky_G, visc_lap, keps, pbd_eps;
+    float rho0, inv_rho0, eps, scorr_coeff, scorr_div, W0;
+    float gx, gy, gz, damping, max_speed, min_speed, b_damping, mu_s, mu_k, k_stretch;
+    float k_water, k_snow, C_water, C_snow, Tf, blending, sor, sph_visc, dem_visc;
+    float Th, k_ref, brk;
+    float ox, oy, oz, csx, csy, csz;
+    uint32_t gsx, gsy, gsz, ncells, maxc;
+    // Exact squared-distance cut-offs: d < h  <=>  d2 < h2_lt, d < 2r <=> d2 < r2_lt,
+    // d <= 2r <=> d2 < r2_le, where d = sqrt_rn(d2) (sqrt_rn is monotone).
+    float h2_lt, r2_lt, r2_le;
+    int quirks;
+};
+
+// Device-resident counters, one block per library context.
+struct DevState {
+    uint32_t n_sph, n_dem, n_b;     // current set sizes
+    uint32_t n0_sph, n0_dem;        // sizes at the start of the substep (launch sizes)
+    uint32_t n_freeze, n_melt;      // particles changing phase in this substep
+    uint32_t changed;               // n_freeze + n_melt > 0
+    uint32_t new_sph, new_dem;      // sizes after compaction
+    uint32_t err;                   // error bits (SNOWB_DEVERR_*)
+    uint32_t tail_dirty;            // a link pass wrote slots beyond the snow set (stale cell range)
+    uint32_t pad[4];
+};
+#define SNOWB_DEVERR_SCATTER 1u
+
+// ---------------------------------------------------------------- float3 helpers
+__device__ __forceinline__ float3 f3(float x, float y, float z) { return make_float3(x, y, z); }
+__device__ __forceinline__ float3 add3(float3 a, float3 b) { return f3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ float3 sub3(float3 a, float3 b) { return f3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 sc3(float s, float3 a) { return f3(s * a.x, s * a.y, s * a.z); }
+__device__ __forceinline__ float3 div3(float3 a, float s) { return f3(a.x / s, a.y / s, a.z / s); }
+__device__ __forceinline__ float dot3(float3 a, float3 b) { return __fmaf_rn(a.z, b.z, __fmaf_rn(a.y, b.y, a.x * b.x)); }
+__device__ __forceinline__ float len3(float3 a) { return sqrtf(dot3(a, a)); }
+__device__ __forceinline__ bool nan3(float3 a) { return isnan(a.x) || isnan(a.y) || isnan(a.z); }
+__device__ __forceinline__ bool inf3(float3 a) { return isinf(a.x) || isinf(a.y) || isinf(a.z); }
+__device__ __forceinline__ float3 xyz(float4 a) { return f3(a.x, a.y, a.z); }
+__device__ __forceinline__ float3 ld3(const snowb_float3* p, uint32_t i)
+{
+    const float* q = reinterpret_cast<const float*>(p) + 3ull * i;
+    return f3(__ldg(q), __ldg(q + 1), __ldg(q + 2));
+}
+__device__ __forceinline__ float3 ldv3(const snowb_float3* p, uint32_t i)   // plain (non-nc) load
+{
+    const float* q = reinterpret_cast<const float*>(p) + 3ull * i;
+    return f3(q[0], q[1], q[2]);
+}
+__device__ __forceinline__ void st3(snowb_float3* p, uint32_t i, float3 v)
+{
+    float* q = reinterpret_cast<float*>(p) + 3ull * i;
+    q[0] = v.x; q[1] = v.y; q[2] = v.z;
+}
+
+// ------------------------------------------------------------- SPH kernels :30-137
+__device__ __forceinline__ float W_poly6(const DevParams& P, float d)
+{
+    if (d >= 0.f && d < P.h) {
+        float h2 = P.h * P.h, d2 = d * d, q = h2 - d2;
+        float q3 = q * q * q;
+        return P.poly6 * q3;
+    }
+    return 0.f;
+}
+__device__ __forceinline__ float3 G_poly6(const DevParams& P, float3 v, float d)
+{
+    if (d >= 0.f && d < P.h) {
+        float h2 = P.h * P.h, d2 = d * d, q = h2 - d2, q2 = q * q;
+        return sc3(P.poly6_G * q2, v);
+    }
+    return f3(0.f, 0.f, 0.f);
+}
+__device__ __forceinline__ float3 G_spiky(const DevParams& P, float3 v, float d)
+{
+    if (d >= 0.f && d < P.h) {
+        float q = P.h - d, q2 = q * q;
+        return sc3(P.spiky_G * (q2 / (d + P.keps)), v);
+    }
+    return f3(0.f, 0.f, 0.f);
+}
+__device__ __forceinline__ float L_visc(const DevParams& P, float d)
+{
+    if (d >= 0.f && d < P.h) return P.visc_lap * (P.h - d);
+    return 0.f;
+}
+__device__ __forceinline__ float scorr_of(const DevParams& P, float d, float dt)
+{
+    float x = W_poly6(P, d) / P.scorr_div;
+    float x4 = (x * x) * (x * x);
+    return ((-P.scorr_coeff * x4) * dt) * dt;
+}
+
+// ------------------------------------------------------------------ grid :141-157
+__device__ __forceinline__ int3 grid_pos(const DevParams& P, float3 p)
+{
+    int3 g;
+    g.x = __float2int_rz(floorf((p.x - P.ox) / P.csx));
+    g.y = __float2int_rz(floorf((p.y - P.oy) / P.csy));
+    g.z = __float2int_rz(floorf((p.z - P.oz) / P.csz));
+    return g;
+}
+__device__ __forceinline__ uint32_t grid_hash(const DevParams& P, int3 g, int dx, int dy, int dz)
+{
+    uint32_t x = ((uint32_t)g.x + (uint32_t)dx) & (P.gsx - 1u);
+    uint32_t y = ((uint32_t)g.y + (uint32_t)dy) & (P.gsy - 1u);
+    uint32_t z = ((uint32_t)g.z + (uint32_t)dz) & (P.gsz - 1u);
+    return (z * P.gsy) * P.gsx + y * P.gsx + x;
+}
+
+// launch coverage of the reference's compute_grid_size(n, 512) (:348-357)
+__device__ __host__ __forceinline__ uint32_t coverage(uint32_t n)
+{
+    if (n == 0) return 0;
+    uint32_t t = n < 512u ? n : 512u;
+    uint32_t b = (n % t) ? n / t + 1 : n / t;
+    return b * t;
+}
+__device__ __host__ __forceinline__ uint32_t umin32(uint32_t a, uint32_t b) { return a < b ? a : b; }
+
+// Sorted view of one particle set for the 27-cell neighbor loops.  Entries j < n come
+// from the compact float4 copy written at the last sort; a stale cell range (cells the
+// reference leaves uncleared) may reach j >= n, which reads the caller's arrays exactly
+// as the reference does.
+struct SetView {
+    const uint32_t* cs;     // cell_start
+    const uint32_t* ce;     // cell_end
+    const uint32_t* gi;     // grid_index (sorted -> original)
+    const float4* p4;       // sorted (x, y, z, w) with w = mass (fluid/snow) or volume (boundary)
+    const snowb_float3* sp; // caller's sorted_pos (float3)
+    const float* wsrc;      // original-order source of the .w attribute (stale path)
+    uint32_t n;
+
+    __device__ __forceinline__ float4 pw(uint32_t j) const
+    {
+        if (j < n) return __ldg(p4 + j);
+        float3 q = ld3(sp, j);
+        return make_float4(q.x, q.y, q.z, wsrc[gi[j]]);
+    }
+    __device__ __forceinline__ float3 pos(uint32_t j) const
+    {
+        if (j < n) { float4 t = __ldg(p4 + j); return f3(t.x, t.y, t.z); }
+        return ld3(sp, j);
+    }
+    // attribute kept in a sorted copy (valid for j < n) with its original-order source
+    __device__ __forceinline__ float attr(const float* sorted, const float* orig, uint32_t j) const
+    {
+        return j < n ? __ldg(sorted + j) : orig[gi[j]];
+    }
+    __device__ __forceinline__ bool range(const DevParams& P, int3 g, int ox, int oy, int oz,
+                                          uint32_t& s, uint32_t& e) const
+    {
+        uint32_t h = grid_hash(P, g, ox, oy, oz);
+        s = __ldg(cs + h);
+        if (s == SNOWB_EMPTY) return false;
+        e = __ldg(ce + h);
+        return true;
+    }
+};
+
+#define FOR27 _Pragma("unroll 1") for (int oz = -1; oz <= 1; ++oz) _Pragma("unroll 1") for (int oy = -1; oy <= 1; ++oy) _Pragma("unroll 1") for (int ox = -1; ox <= 1; ++ox)
+
+// grid-stride loop over [0, n)
+#define GRID_LOOP(i, n) for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += gridDim.x * blockDim.x)
+
+}  // namespace snowb

@@ -1,0 +1,328 @@
+// phase.cuh -- freezing/melting with compaction (cuda_simulation.cu:3974-4125, :4387-4622)
+// and interlink formation (:4127-4292, :4768-4816).
+//
+// Phase change.  The reference claims target slots with atomicAdd, so their order is
+// scheduling dependent (Q8); here a particle's target is its rank among the particles
+// changing phase (ascending index).  Compaction always runs in the reference; when no
+// particle changed phase it is an identity, so every compaction kernel returns early
+// unless DevState::changed is set (no host round trip is needed).
+//
+// Interlink formation.  The reference lets every snow particle claim slots with atomics
+// while others read the same slots (Q10), so the topology depends on scheduling.  Here
+// the pass is the sequential reference procedure applied in one fixed order: hash cells
+// are grouped into 2x2x2 super-cells, each super-cell gets a colour 0..7 from the parity
+// of its coordinates, colours run in turn, and inside a colour each super-cell walks its
+// particles in ascending sorted index.  A particle only edits its own slots and those of
+// neighbours within h, i.e. in adjacent cells; same-coloured super-cells are at least
+// three cells apart, so they never touch the same particle and run in parallel, one
+// thread per super-cell.  A prefilter marks the particles that can change anything:
+// links are never removed during the pass and counts only grow, so a particle whose
+// count already reaches its cap, or whose candidates are all linked already, is a no-op.
+#pragma once
+#include "common.cuh"
+#include "sort.cuh"
+
+namespace snowb {
+
+// copy_particle_info (:3974-4002)
+__device__ __forceinline__ void copy_info(const snowb_particle_data& s, const snowb_particle_data& d, uint32_t i,
+                                          uint32_t t, uint32_t M)
+{
+    st3(d.positions, t, ldv3(s.positions, i));
+    st3(d.predict_positions, t, ldv3(s.predict_positions, i));
+    st3(d.new_positions, t, ldv3(s.new_positions, i));
+    st3(d.velocity, t, ldv3(s.velocity, i));
+    st3(d.force, t, ldv3(s.force, i));
+    st3(d.correction, t, ldv3(s.correction, i));
+    d.mass[t] = s.mass[i];
+    d.massInv[t] = s.massInv[i];
+    d.contrib[t] = s.contrib[i];
+    d.density[t] = s.density[i];
+    d.C[t] = s.C[i];
+    d.lambda[t] = s.lambda[i];
+    d.T[t] = s.T[i];
+    d.new_T[t] = s.new_T[i];
+    d.trackId[t] = s.trackId[i];
+    for (uint32_t c = 0; c < M; ++c) {
+        d.connect_record[t * M + c] = s.connect_record[i * M + c];
+        d.connect_length[t * M + c] = s.connect_length[i * M + c];
+    }
+    d.iter_end[t] = s.iter_end[i];
+}
+__device__ __forceinline__ void reset_records(const snowb_particle_data& d, uint32_t t, uint32_t M)
+{
+    for (uint32_t c = 0; c < M; ++c) {
+        d.connect_record[t * M + c] = SNOWB_UMAX;
+        d.connect_length[t * M + c] = 0.f;
+    }
+    d.iter_end[t] = M * t;
+}
+
+// freeze / melt predicates (:4425, :4396)
+__global__ void k_phase_flags(DevParams P, const DevState* __restrict__ S, snowb_particle_data sph,
+                              snowb_particle_data dem, int freeze, int melt, uint32_t* __restrict__ fl_s,
+                              uint32_t* __restrict__ fl_d)
+{
+    const uint32_t ns = S->n_sph, nd = S->n_dem;
+    GRID_LOOP(t, ns + nd) {
+        if (t < ns) fl_s[t] = (freeze && sph.T[t] <= P.Tf && sph.contrib[t] >= 0.99f) ? 1u : 0u;
+        else {
+            const uint32_t i = t - ns;
+            fl_d[i] = (melt && dem.T[i] > P.Tf && dem.contrib[i] >= 0.99f) ? 1u : 0u;
+        }
+    }
+}
+__global__ void k_phase_count(DevState* S)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) S->changed = (S->n_freeze + S->n_melt) != 0u;
+}
+// freezing (:4416-4449) and melting (:4387-4414) with ranked targets
+__global__ void k_phase_move(DevParams P, const DevState* __restrict__ S, snowb_particle_data sph,
+                             snowb_particle_data dem, const uint32_t* __restrict__ fl_s,
+                             const uint32_t* __restrict__ rk_s, const uint32_t* __restrict__ fl_d,
+                             const uint32_t* __restrict__ rk_d)
+{
+    if (S->changed == 0) return;
+    const uint32_t ns = S->n_sph, nd = S->n_dem, M = P.maxc;
+    GRID_LOOP(t, ns + nd) {
+        if (t < ns) {
+            if (!fl_s[t]) continue;
+            const uint32_t i = t, tg = nd + rk_s[i];
+            sph.contrib[i] = 0.f;
+            copy_info(sph, dem, i, tg, M);
+            sph.predicate[i] = 0; sph.trackId[i] = 0;
+            dem.predicate[tg] = 1;
+            reset_records(dem, tg, M);
+        } else {
+            const uint32_t i = t - ns;
+            if (!fl_d[i]) continue;
+            const uint32_t tg = ns + rk_d[i];
+            dem.contrib[i] = 0.f;
+            copy_info(dem, sph, i, tg, M);
+            dem.predicate[i] = 0; dem.trackId[i] = 0;
+            sph.predicate[tg] = 1;
+        }
+    }
+}
+// shuffle_useless_record (:4068-4111): drop links to particles that left the snow set
+__global__ void k_shuffle_records(DevParams P, const DevState* __restrict__ S, snowb_particle_data dem)
+{
+    if (S->changed == 0) return;
+    const uint32_t nd = S->n_dem, M = P.maxc;
+    GRID_LOOP(i, nd) {
+        for (uint32_t s = M * i; s < (i + 1) * M; ++s) {
+            const uint32_t r = dem.connect_record[s];
+            if (r < nd && dem.predicate[r] == 0) {
+                dem.connect_record[s] = SNOWB_UMAX;
+                dem.connect_length[s] = 0.f;
+                dem.iter_end[i]--;
+            }
+        }
+    }
+}
+// copy_to_target (:4451-4460) into the caller's phase-change buffer
+__global__ void k_copy_to_buffer(DevParams P, const DevState* __restrict__ S, snowb_particle_data d,
+                                 snowb_particle_data buf, uint32_t full)
+{
+    if (S->changed == 0) return;
+    GRID_LOOP(i, full) copy_info(d, buf, i, i, P.maxc);
+}
+// scatter (:4462-4480)
+__global__ void k_scatter_set(DevParams P, DevState* S, snowb_particle_data d, snowb_particle_data buf, uint32_t full)
+{
+    if (S->changed == 0) return;
+    GRID_LOOP(i, full) {
+        if (d.predicate[i] == 1) {
+            const uint32_t t = d.scan_index[i];
+            if (t >= full) { atomicOr(&S->err, SNOWB_DEVERR_SCATTER); continue; }
+            copy_info(buf, d, i, t, P.maxc);
+            d.new_index[i] = t;
+        } else d.new_index[i] = SNOWB_UMAX;
+    }
+}
+// setSize / new_end (:4545-4551), predicate fill (:4555-4556), clean_tail (:4482-4493).
+// The reference compacts every substep; without a phase change that is an identity except
+// that it zeroes scan_index in the tail and, if a link pass wrote into tail slots, resets
+// them (`full_clean`), which is what this kernel does in that case.
+__global__ void k_compact_finish(DevParams P, DevState* S, snowb_particle_data sph, snowb_particle_data dem,
+                                 uint32_t full)
+{
+    const bool full_clean = S->changed || S->tail_dirty;
+    const uint32_t sn = S->new_sph, dn = S->new_dem, M = P.maxc;
+    GRID_LOOP(t, 2 * full) {
+        const bool w = t < full;
+        const uint32_t i = w ? t : t - full;
+        const snowb_particle_data& d = w ? sph : dem;
+        const uint32_t n = w ? sn : dn;
+        if (i < n) {
+            if (full_clean) d.predicate[i] = 1;
+        } else {
+            d.scan_index[i] = 0;
+            if (full_clean) {
+                d.predicate[i] = 0; d.trackId[i] = 0;
+                reset_records(d, i, M);
+            }
+        }
+        if (i == 0 && full_clean) *d.new_end = n;
+    }
+}
+__global__ void k_commit_sizes(DevState* S)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0 && S->changed) { S->n_sph = S->new_sph; S->n_dem = S->new_dem; }
+}
+__global__ void k_clear_tail_flag(DevState* S)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) S->tail_dirty = 0;
+}
+// update_record_index (:4114-4125)
+__global__ void k_update_records(DevParams P, const DevState* __restrict__ S, snowb_particle_data dem)
+{
+    if (S->changed == 0 && S->tail_dirty == 0) return;
+    // without a phase change the reference's new_index is the identity below n, empty above
+    const bool moved = S->changed != 0;
+    const uint32_t nd = S->n_dem, total = P.maxc * nd;
+    GRID_LOOP(s, total) {
+        const uint32_t r = dem.connect_record[s];
+        if (r != SNOWB_UMAX) dem.connect_record[s] = moved ? dem.new_index[r] : (r < nd ? r : SNOWB_UMAX);
+    }
+}
+
+// ======================================================================= links
+__device__ __forceinline__ uint32_t link_tolerance(const DevParams& P, float T, int dynamic)
+{
+    uint32_t tol = dynamic ? __float2uint_rz(((T - P.Tf) / (P.Th - P.Tf)) * (float)P.maxc) : P.maxc;
+    return tol < P.maxc ? tol : P.maxc;
+}
+// prefilter: can particle (sorted) i add any link in this pass?
+__global__ void __launch_bounds__(128) k_link_filter(DevParams P, const DevState* __restrict__ S, SetView vd,
+                                                     snowb_particle_data dem, int dynamic,
+                                                     uint8_t* __restrict__ active)
+{
+    const uint32_t nd = S->n_dem, M = P.maxc;
+    vd.n = nd;
+    GRID_LOOP(i, nd) {
+        const uint32_t o = vd.gi[i];
+        const float3 p = vd.pos(i);
+        const uint32_t count = dem.iter_end[o] - o * M;
+        uint8_t act = 0;
+        if (count < link_tolerance(P, dem.T[o], dynamic)) {
+            const int3 g = grid_pos(P, p);
+            FOR27 {
+                uint32_t s, e;
+                if (!vd.range(P, g, ox, oy, oz, s, e)) continue;
+                for (uint32_t j = s; j < e && !act; ++j) {
+                    if (j == i) continue;
+                    float3 dv = sub3(p, vd.pos(j));
+                    if (dot3(dv, dv) < P.h2_lt) {
+                        const uint32_t o1 = vd.gi[j];
+                        bool found = false;
+                        for (uint32_t q = M * o; q < M * (o + 1); ++q)
+                            if (dem.connect_record[q] == o1) { found = true; break; }
+                        if (!found) act = 1;
+                    }
+                }
+                if (act) break;
+            }
+        }
+        active[i] = act;
+    }
+}
+// connect_and_record_cell (:4127-4252) + connect_and_record_d (:4255-4284) for one particle
+__device__ void link_particle(const DevParams& P, const SetView& vd, const snowb_particle_data& d, uint32_t i,
+                              int dynamic, uint32_t* tail_flag)
+{
+    const uint32_t M = P.maxc;
+    const float3 p = vd.pos(i);
+    const uint32_t o = vd.gi[i];
+    const int3 g = grid_pos(P, p);
+    const float T = d.T[o];
+    FOR27 {
+        uint32_t s, e;
+        if (!vd.range(P, g, ox, oy, oz, s, e)) continue;
+        for (uint32_t j = s; j < e; ++j) {
+            if (j == i) continue;
+            const uint32_t o1 = vd.gi[j];
+            const float dist = len3(sub3(p, vd.pos(j)));
+            const uint32_t count = d.iter_end[o] - o * M;
+            const uint32_t tol = link_tolerance(P, T, dynamic);
+            if (dist < P.h && count < tol) {
+                bool dup = false;
+                for (uint32_t q = M * o; q < M * (o + 1); ++q)
+                    if (d.connect_record[q] == o1) { dup = true; break; }
+                if (dup) break;   // the reference returns from the cell helper
+                for (uint32_t q = M * o; q < M * (o + 1); ++q) {
+                    if (d.connect_record[q] == SNOWB_UMAX) {
+                        d.connect_record[q] = o1;
+                        bool valid = false;
+                        if (d.iter_end[o1] < (o1 + 1) * M)
+                            for (uint32_t r = o1 * M; r < (o1 + 1) * M; ++r)
+                                if (d.connect_record[r] == SNOWB_UMAX) {
+                                    d.connect_record[r] = o;
+                                    d.connect_length[r] = dist;
+                                    d.iter_end[o1]++;
+                                    if (o1 >= vd.n) atomicOr(tail_flag, 1u);
+                                    valid = true;
+                                    break;
+                                }
+                        if (valid) { d.connect_length[q] = dist; d.iter_end[o]++; }
+                        else d.connect_record[q] = SNOWB_UMAX;
+                        break;
+                    }
+                }
+            }
+        }
+    }
+}
+// one colour: one thread per super-cell of that colour; fs/fe give each hash cell's
+// current (non-stale) sorted range
+__global__ void k_link_colour(DevParams P, DevState* S, SetView vd, snowb_particle_data dem,
+                              const uint32_t* __restrict__ fs, const uint32_t* __restrict__ fe,
+                              const uint8_t* __restrict__ active, uint32_t colour, int dynamic)
+{
+    vd.n = S->n_dem;
+    const uint32_t qx = P.gsx >> 2, qy = P.gsy >> 2, qz = P.gsz >> 2;
+    const uint32_t total = qx * qy * qz;
+    GRID_LOOP(t, total) {
+        const uint32_t sx = 2u * (t % qx) + (colour & 1u);
+        const uint32_t sy = 2u * ((t / qx) % qy) + ((colour >> 1) & 1u);
+        const uint32_t sz = 2u * (t / (qx * qy)) + ((colour >> 2) & 1u);
+        for (uint32_t dz = 0; dz < 2; ++dz)
+            for (uint32_t dy = 0; dy < 2; ++dy)
+                for (uint32_t dx = 0; dx < 2; ++dx) {
+                    const uint32_t h = ((2u * sz + dz) * P.gsy + (2u * sy + dy)) * P.gsx + (2u * sx + dx);
+                    const uint32_t b = fs[h], e = fe[h];
+                    for (uint32_t i = b; i < e; ++i)
+                        if (active[i]) link_particle(P, vd, dem, i, dynamic, &S->tail_dirty);
+                }
+    }
+}
+// adjust_connections_d (:4768-4808) in ascending index order (single thread).  The
+// reference indexes the partner's slots with an empty record once the count exceeds the
+// cap (an out-of-bounds read); that partner loop is skipped here.
+__global__ void k_adjust_links(DevParams P, DevState* S, snowb_particle_data d, uint32_t full)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const uint32_t n = S->n_dem, M = P.maxc;
+    for (uint32_t i = 0; i < n; ++i) {
+        uint32_t cm = __float2uint_rz(((d.T[i] - P.Tf) / (P.Th - P.Tf)) * (float)M);
+        if (cm > M) cm = M;
+        uint32_t count = 0;
+        for (uint32_t s = M * i; s < M * (i + 1); ++s) {
+            count = d.connect_record[s] != SNOWB_UMAX ? count + 1 : count;
+            if (count > cm) {
+                const uint32_t j = d.connect_record[s];
+                d.connect_record[s] = SNOWB_UMAX;
+                d.connect_length[s] = 0.f;
+                d.iter_end[i]--;
+                if (j == SNOWB_UMAX || j >= full) continue;
+                if (j >= n) S->tail_dirty = 1u;
+                for (uint32_t q = M * j; q < M * (j + 1); ++q)
+                    if (d.connect_record[q] == i) {
+                        d.connect_record[q] = SNOWB_UMAX; d.connect_length[q] = 0.f; d.iter_end[j]--;
+                    }
+            }
+        }
+    }
+}
+
+}  // namespace snowb

@@ -1,0 +1,680 @@
+// snow_b200.cu -- host orchestration and C ABI of libsnowb200.so (see include/snow_b200.h).
+//
+// snow_simulation (cuda_simulation.cu:4861-5157) is restated as a sequence of fused
+// kernels on one stream.  Set sizes live on the device (DevState), so a substep needs no
+// host round trip; the host reads them back once per call to honour the reference's
+// contract (ParticleSet::setSize).  Sorting follows the reference's sort points exactly,
+// but a set whose predicted positions have not changed since its last sort is not
+// sorted again (the result would be identical).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "sort.cuh"
+#include "solver.cuh"
+#include "phase.cuh"
+
+namespace snowb {
+
+// ------------------------------------------------------------------ error state
+static thread_local int g_err = SNOWB_OK;
+static thread_local std::string g_msg;
+
+static int fail(int code, const std::string& msg)
+{
+    g_err = code;
+    g_msg = msg;
+    return code;
+}
+#define CUDA_TRY(x)                                                                          \
+    do {                                                                                     \
+        cudaError_t _e = (x);                                                                \
+        if (_e != cudaSuccess)                                                               \
+            return fail(SNOWB_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(_e));    \
+    } while (0)
+#define TRY(x)                      \
+    do {                            \
+        int _r = (x);               \
+        if (_r != SNOWB_OK) return _r; \
+    } while (0)
+
+// ------------------------------------------------------------------ global state
+static std::mutex g_mu;
+static bool g_have_params = false;
+static snowb_sim_params g_sim;
+static DevParams g_P;
+static int g_quirks = SNOWB_QUIRKS_REFERENCE;
+static cudaStream_t g_stream = 0;
+static int g_max_blocks = 148 * 16;
+
+static float smallest_with_sqrt_ge(float t)   // min x: sqrtf(x) >= t
+{
+    float x = t * t;
+    while (x > 0.f && std::sqrt(x) >= t) x = std::nextafter(x, 0.f);
+    while (std::sqrt(x) < t) x = std::nextafter(x, INFINITY);
+    return x;
+}
+static float smallest_with_sqrt_gt(float t)   // min x: sqrtf(x) > t
+{
+    float x = t * t;
+    while (x > 0.f && std::sqrt(x) > t) x = std::nextafter(x, 0.f);
+    while (!(std::sqrt(x) > t)) x = std::nextafter(x, INFINITY);
+    return x;
+}
+
+static DevParams derive(const snowb_sim_params& s)
+{
+    DevParams P;
+    std::memset(&P, 0, sizeof(P));
+    P.h = s.effective_radius; P.r = s.particle_radius; P.two_r = 2.f * s.particle_radius;
+    P.poly6 = s.poly6; P.poly6_G = s.poly6_G; P.spiky_G = s.spiky_G; P.visc_lap = s.viscosity_laplacian;
+    P.keps = s.kernel_epsilon; P.pbd_eps = s.pbd_epsilon; P.rho0 = s.rest_density;
+    P.inv_rho0 = 1.f / s.rest_density; P.eps = s.epsilon; P.scorr_coeff = s.scorr_coeff;
+    P.scorr_div = s.scorr_divisor;
+    {   // W_poly6(0) evaluated as the kernel does
+        float h2 = P.h * P.h, d2 = 0.f * 0.f, q = h2 - d2;
+        float q3 = q * q;
+        q3 = q3 * q;
+        P.W0 = P.poly6 * q3;
+    }
+    P.gx = s.gravity[0]; P.gy = s.gravity[1]; P.gz = s.gravity[2];
+    P.damping = s.global_damping; P.max_speed = s.maximum_speed; P.min_speed = s.minimum_speed;
+    P.b_damping = s.boundary_damping; P.mu_s = s.static_friction; P.mu_k = s.kinematic_friction;
+    P.k_stretch = s.k_stretch; P.k_water = s.k_water; P.k_snow = s.k_snow; P.C_water = s.C_water;
+    P.C_snow = s.C_snow; P.Tf = s.freezing_point; P.blending = s.blending_speed; P.sor = s.sor_coeff;
+    P.sph_visc = s.sph_viscosity; P.dem_visc = s.dem_viscosity; P.Th = s.T_homogeneous;
+    P.k_ref = s.k_refreezing; P.brk = s.break_threshold;
+    P.ox = s.world_origin[0]; P.oy = s.world_origin[1]; P.oz = s.world_origin[2];
+    P.csx = s.cell_size[0]; P.csy = s.cell_size[1]; P.csz = s.cell_size[2];
+    P.gsx = s.grid_size[0]; P.gsy = s.grid_size[1]; P.gsz = s.grid_size[2];
+    P.ncells = s.num_cells; P.maxc = s.maximum_connection;
+    P.h2_lt = smallest_with_sqrt_ge(P.h);
+    P.r2_lt = smallest_with_sqrt_ge(P.two_r);
+    P.r2_le = smallest_with_sqrt_gt(P.two_r);
+    P.quirks = SNOWB_QUIRKS_REFERENCE;
+    return P;
+}
+
+// ------------------------------------------------------------------ context
+template <class T>
+static int dalloc(T** p, size_t count)
+{
+    *p = nullptr;
+    if (count == 0) count = 1;
+    CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(p), count * sizeof(T)));
+    return SNOWB_OK;
+}
+
+struct SetBufs {
+    uint32_t *key = nullptr, *slot = nullptr, *tmp = nullptr, *cnt = nullptr, *off = nullptr, *bsum = nullptr;
+    uint32_t* val = nullptr;
+    float4* p4 = nullptr;
+    float *invm = nullptr, *contrib = nullptr, *lambda = nullptr, *mass = nullptr;
+};
+
+struct Ctx {
+    int device = -1;
+    uint32_t cap = 0, bcap = 0, ncells = 0;
+    SetBufs s[2];          // 0 = water (SPH), 1 = snow (DEM)
+    SetBufs b;             // boundary
+    SetBufs gen;           // scratch for the standalone sort entry points
+    uint32_t gen_cap = 0;
+    uint32_t *fl_s = nullptr, *fl_d = nullptr, *rk_s = nullptr, *rk_d = nullptr, *sbsum = nullptr;
+    uint8_t* active = nullptr;
+    uint32_t *fs = nullptr, *fe = nullptr;
+    snowb_float3* tmp_vel = nullptr;
+    double* epart = nullptr;
+    double* eout = nullptr;
+    DevState* S = nullptr;
+    DevState* S_host = nullptr;
+    uint32_t* err_dev = nullptr;
+};
+static Ctx g_ctx;
+
+static void free_set(SetBufs& s)
+{
+    void* ptrs[] = {s.key, s.slot, s.tmp, s.cnt, s.off, s.bsum, s.val, s.p4, s.invm, s.contrib, s.lambda, s.mass};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    s = SetBufs();
+}
+static void free_ctx(Ctx& c)
+{
+    for (auto& s : c.s) free_set(s);
+    free_set(c.b);
+    free_set(c.gen);
+    void* ptrs[] = {c.fl_s, c.fl_d, c.rk_s, c.rk_d, c.sbsum, c.active, c.fs, c.fe, c.tmp_vel, c.epart, c.eout,
+                    c.S, c.err_dev};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (c.S_host) cudaFreeHost(c.S_host);
+    c = Ctx();
+}
+static int alloc_sort(SetBufs& s, uint32_t cap, uint32_t ncells, bool attrs)
+{
+    TRY(dalloc(&s.key, cap)); TRY(dalloc(&s.slot, cap)); TRY(dalloc(&s.tmp, cap)); TRY(dalloc(&s.val, cap));
+    TRY(dalloc(&s.cnt, ncells)); TRY(dalloc(&s.off, ncells + 1));
+    TRY(dalloc(&s.bsum, ncells / SCAN_CHUNK + 2));
+    CUDA_TRY(cudaMemset(s.cnt, 0, sizeof(uint32_t) * ncells));
+    if (attrs) {
+        TRY(dalloc(&s.p4, cap)); TRY(dalloc(&s.invm, cap)); TRY(dalloc(&s.contrib, cap)); TRY(dalloc(&s.lambda, cap));
+    }
+    return SNOWB_OK;
+}
+// (Re)create the context for the current device with room for `full` particles per set,
+// `nb` boundary particles and `ncells` cells.
+static int ensure_ctx(uint32_t full, uint32_t nb, uint32_t ncells)
+{
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    Ctx& c = g_ctx;
+    if (c.device == dev && c.cap >= full && c.bcap >= nb && c.ncells == ncells) return SNOWB_OK;
+    free_ctx(c);
+    c.device = dev;
+    c.cap = full > 0 ? full : 1;
+    c.bcap = nb > 0 ? nb : 1;
+    c.ncells = ncells;
+    for (auto& s : c.s) TRY(alloc_sort(s, c.cap, ncells, true));
+    TRY(dalloc(&c.b.p4, c.bcap)); TRY(dalloc(&c.b.invm, c.bcap)); TRY(dalloc(&c.b.mass, c.bcap));
+    TRY(dalloc(&c.b.lambda, c.bcap));
+    TRY(dalloc(&c.fl_s, c.cap)); TRY(dalloc(&c.fl_d, c.cap)); TRY(dalloc(&c.rk_s, c.cap)); TRY(dalloc(&c.rk_d, c.cap));
+    TRY(dalloc(&c.sbsum, 4 * (c.cap / SCAN_CHUNK + 2)));
+    TRY(dalloc(&c.active, c.cap));
+    TRY(dalloc(&c.fs, ncells)); TRY(dalloc(&c.fe, ncells));
+    TRY(dalloc(&c.tmp_vel, c.cap));
+    TRY(dalloc(&c.epart, 4 * 1024)); TRY(dalloc(&c.eout, 4));
+    TRY(dalloc(&c.S, 1)); TRY(dalloc(&c.err_dev, 1));
+    CUDA_TRY(cudaMemset(c.S, 0, sizeof(DevState)));
+    CUDA_TRY(cudaMemset(c.err_dev, 0, sizeof(uint32_t)));
+    CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&c.S_host), sizeof(DevState)));
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    g_max_blocks = sms * 16;
+    return SNOWB_OK;
+}
+static int ensure_gen(uint32_t n, uint32_t ncells)
+{
+    Ctx& c = g_ctx;
+    if (c.gen.key && c.gen_cap >= n && c.ncells == ncells) return SNOWB_OK;
+    free_set(c.gen);
+    c.gen_cap = n > 0 ? n : 1;
+    return alloc_sort(c.gen, c.gen_cap, ncells, false);
+}
+
+// ------------------------------------------------------------------ launch helpers
+static inline unsigned blocks_for(uint64_t work, int tpb)
+{
+    uint64_t b = (work + tpb - 1) / tpb;
+    if (b < 1) b = 1;
+    if (b > (uint64_t)g_max_blocks) b = g_max_blocks;
+    return (unsigned)b;
+}
+#define LAUNCH(kernel, work, tpb, ...)                                                     \
+    do {                                                                                   \
+        kernel<<<blocks_for((work), (tpb)), (tpb), 0, g_stream>>>(__VA_ARGS__);            \
+        cudaError_t _e = cudaGetLastError();                                               \
+        if (_e != cudaSuccess)                                                             \
+            return fail(SNOWB_ERR_CUDA, std::string(#kernel) + ": " + cudaGetErrorString(_e)); \
+    } while (0)
+#define LAUNCH1(kernel, ...) LAUNCH(kernel, 1, 32, __VA_ARGS__)
+
+static inline unsigned scan_blocks(uint32_t n) { return (n + SCAN_CHUNK - 1) / SCAN_CHUNK + (n == 0); }
+
+// exclusive scan of in[0, n) (n from the device when n_ptr is set; `cap` bounds it)
+static int scan(const uint32_t* in, const uint32_t* n_ptr, uint32_t n_fixed, uint32_t cap, uint32_t* bsum,
+                uint32_t* out, uint32_t* total, const uint32_t* cond)
+{
+    const uint32_t nb = scan_blocks(n_ptr ? cap : n_fixed);
+    k_scan_sums<<<nb, SCAN_TPB, 0, g_stream>>>(in, n_ptr, n_fixed, bsum, cond);
+    k_scan_apply<<<nb, SCAN_TPB, 0, g_stream>>>(in, n_ptr, n_fixed, bsum, out, total, cond);
+    CUDA_TRY(cudaGetLastError());
+    return SNOWB_OK;
+}
+
+// hash + stable sort + reorder of one set (sort_and_reorder :398-420), writing the
+// caller's cell data and the compact sorted copies.  cond: skip unless *cond != 0.
+static int sort_set(const DevParams& P, SetBufs& B, const snowb_particle_data& D, const snowb_cell_data& cd,
+                    const uint32_t* n_ptr, uint32_t cap, const uint32_t* cond, bool clear_all)
+{
+    const uint32_t nc = P.ncells;
+    LAUNCH(k_hash_count, cap, 256, P, D.predict_positions, n_ptr, 0u, B.key, B.slot, B.cnt, cond);
+    const unsigned nb = (nc + SCAN_CHUNK - 1) / SCAN_CHUNK;
+    k_block_sums<<<nb, SCAN_TPB, 0, g_stream>>>(B.cnt, nc, B.bsum, cond);
+    k_cell_scan<<<nb, SCAN_TPB, 0, g_stream>>>(B.cnt, B.bsum, nc, B.off, cd.cell_start, n_ptr, 0u, clear_all ? 1 : 0,
+                                               cond);
+    CUDA_TRY(cudaGetLastError());
+    LAUNCH(k_scatter, cap, 256, B.key, B.slot, B.off, B.tmp, n_ptr, 0u, cond);
+    LAUNCH(k_rank_reorder, cap, 256, B.key, B.off, B.tmp, D.predict_positions, D.mass, D.massInv, D.contrib, cd, B.p4,
+           B.invm, B.contrib, n_ptr, 0u, cond);
+    return SNOWB_OK;
+}
+
+static SetView make_view(const snowb_cell_data& cd, const float4* p4, const float* wsrc)
+{
+    SetView v;
+    v.cs = cd.cell_start; v.ce = cd.cell_end; v.gi = cd.grid_index; v.p4 = p4; v.sp = cd.sorted_pos;
+    v.wsrc = wsrc; v.n = 0;
+    return v;
+}
+
+struct StepArgs {
+    snowb_particle_data *sph, *dem, *bnd, *buf;
+    uint32_t nb, full;
+    snowb_cell_data scd, dcd, bcd;
+    float dt;
+    int iterations;
+    int correct_dem, sph_sph, friction, temperature, change_phase, freezing, melting, dem_visc, interlink,
+        dynamic, cd_on;
+    float dTe;
+    int stop_after;
+};
+
+// One substep (cuda_simulation.cu:4861-5157) given step flags derived from the scene time.
+// Returns SNOWB_OK; stops early after stage `stop_after` (0 = complete).
+static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool step_dem)
+{
+    Ctx& c = g_ctx;
+    DevState* S = c.S;
+    const uint32_t full = a.full, cap = g_ctx.cap;
+    const bool ref = P.quirks == SNOWB_QUIRKS_REFERENCE;
+    Sets X{*a.sph, *a.dem, *a.bnd};
+    SetView vs = make_view(a.scd, c.s[0].p4, a.sph->mass);
+    SetView vd = make_view(a.dcd, c.s[1].p4, a.dem->mass);
+    SetView vb = make_view(a.bcd, c.b.p4, a.bnd->volume);
+    Sorted ss{c.s[0].invm, c.s[0].contrib, c.s[0].lambda, nullptr};
+    Sorted sd{c.s[1].invm, c.s[1].contrib, c.s[1].lambda, nullptr};
+    Sorted sb{c.b.invm, nullptr, c.b.lambda, c.b.mass};
+    StageFlags F{a.correct_dem, a.sph_sph, a.interlink, step_sph ? 1 : 0, step_dem ? 1 : 0};
+    const uint32_t* n_s = &S->n_sph;
+    const uint32_t* n_d = &S->n_dem;
+    const uint32_t work3 = 2 * full + a.nb;
+    bool dirty_s = true, dirty_d = true;
+    auto sort_if = [&](int set, const uint32_t* cond) -> int {
+        bool& dirty = set ? dirty_d : dirty_s;
+        if (!dirty && !cond) return SNOWB_OK;
+        TRY(sort_set(P, c.s[set], set ? *a.dem : *a.sph, set ? a.dcd : a.scd, set ? n_d : n_s, cap, cond,
+                     !ref));
+        if (!cond) dirty = false;
+        return SNOWB_OK;
+    };
+#define STOP(k) do { if (a.stop_after == (k)) return SNOWB_OK; } while (0)
+
+    LAUNCH1(k_begin_substep, S);
+    TRY(sort_if(1, nullptr));
+    TRY(sort_if(0, nullptr));
+    STOP(1);
+    LAUNCH(k_density, work3, 128, P, S, vs, vd, vb, X);
+    STOP(2);
+    if (a.temperature) {
+        LAUNCH(k_heat, 2 * full, 128, P, S, vs, vd, X, a.dt);
+        LAUNCH(k_heat_commit, 2 * full, 256, S, X, a.dTe, step_sph ? 1 : 0, step_dem ? 1 : 0);
+    }
+    STOP(3);
+    if (a.change_phase) {
+        LAUNCH(k_phase_flags, 2 * full, 256, P, S, *a.sph, *a.dem, a.freezing, a.melting, c.fl_s, c.fl_d);
+        const uint32_t sb_stride = cap / SCAN_CHUNK + 2;
+        TRY(scan(c.fl_s, n_s, 0, cap, c.sbsum, c.rk_s, &S->n_freeze, nullptr));
+        TRY(scan(c.fl_d, n_d, 0, cap, c.sbsum + sb_stride, c.rk_d, &S->n_melt, nullptr));
+        LAUNCH1(k_phase_count, S);
+        LAUNCH(k_phase_move, 2 * full, 256, P, S, *a.sph, *a.dem, c.fl_s, c.rk_s, c.fl_d, c.rk_d);
+        // compact_and_clean (:4495-4589): predicate scans run every substep (they define
+        // scan_index), the data movement only after a phase change.
+        TRY(scan(a.sph->predicate, nullptr, full, full, c.sbsum, a.sph->scan_index, &S->new_sph, nullptr));
+        TRY(scan(a.dem->predicate, nullptr, full, full, c.sbsum + sb_stride, a.dem->scan_index, &S->new_dem, nullptr));
+        LAUNCH(k_shuffle_records, full, 256, P, S, *a.dem);
+        LAUNCH(k_copy_to_buffer, full, 256, P, S, *a.sph, *a.buf, full);
+        LAUNCH(k_scatter_set, full, 256, P, S, *a.sph, *a.buf, full);
+        LAUNCH(k_copy_to_buffer, full, 256, P, S, *a.dem, *a.buf, full);
+        LAUNCH(k_scatter_set, full, 256, P, S, *a.dem, *a.buf, full);
+        LAUNCH(k_compact_finish, 2 * full, 256, P, S, *a.sph, *a.dem, full);
+        LAUNCH1(k_commit_sizes, S);
+        LAUNCH(k_update_records, (uint64_t)P.maxc * full, 256, P, S, *a.dem);
+        LAUNCH1(k_clear_tail_flag, S);
+    }
+    STOP(4);
+    if (a.change_phase) {   // the reference sorts again; only a phase change alters the result
+        TRY(sort_if(1, &S->changed));
+        TRY(sort_if(0, &S->changed));
+    }
+    STOP(5);
+    if (a.interlink) {
+        LAUNCH(k_link_filter, full, 128, P, S, vd, *a.dem, a.dynamic, c.active);
+        for (uint32_t col = 0; col < 8; ++col)
+            LAUNCH(k_link_colour, (P.gsx / 4) * (P.gsy / 4) * (P.gsz / 4), 64, P, S, vd, *a.dem, c.s[1].off,
+                   c.s[1].off + 1, c.active, col, a.dynamic);
+        if (a.dynamic) LAUNCH1(k_adjust_links, P, S, *a.dem, full);
+    }
+    STOP(6);
+    if (step_sph || step_dem) {
+        LAUNCH(k_integrate, 2 * full, 256, P, S, X, full, a.dt, a.cd_on, step_sph ? 1 : 0, step_dem ? 1 : 0);
+        if (step_sph) dirty_s = true;
+        if (step_dem) dirty_d = true;
+    }
+    STOP(7);
+    for (int it = 0; it < a.iterations; ++it) {
+        const int base = 10 + 10 * it;
+        TRY(sort_if(1, nullptr));
+        TRY(sort_if(0, nullptr));
+        STOP(base + 0);
+        LAUNCH(k_density, work3, 128, P, S, vs, vd, vb, X);
+        STOP(base + 1);
+        LAUNCH(k_lambda, work3, 128, P, S, vs, vd, vb, X, ss, sd, sb);
+        STOP(base + 2);
+        LAUNCH(k_pbf, 2 * full, 128, P, S, vs, vd, vb, X, ss, sd, sb, a.dt, F);
+        STOP(base + 3);
+        LAUNCH(k_dem_corr, full, 128, P, S, vs, vd, vb, X, ss, sd, sb, F);
+        STOP(base + 5);
+        if (step_sph || step_dem) {
+            LAUNCH(k_apply, 2 * full, 256, P, S, vs, vd, X, step_sph ? 1 : 0, step_dem ? 1 : 0);
+            if (step_sph) dirty_s = true;
+            if (step_dem) dirty_d = true;
+        }
+        STOP(base + 6);
+        if (a.friction && step_dem) {
+            TRY(sort_if(1, nullptr));
+            TRY(sort_if(0, nullptr));
+            LAUNCH(k_friction, full, 128, P, S, vd, vb, X, sd, sb);
+            LAUNCH(k_apply, full, 256, P, S, vs, vd, X, 0, 1);
+            dirty_d = true;
+        }
+        STOP(base + 7);
+    }
+    if (step_sph || step_dem)
+        LAUNCH(k_finalize, 2 * full, 256, P, S, X, a.dt, step_sph ? 1 : 0, step_dem ? 1 : 0);
+    STOP(90);
+    // apply_XSPH_viscosity (:3663-3711), Jacobi
+    if (step_sph) {
+        LAUNCH(k_xsph, full, 128, P, S, vs, vd, *a.sph, *a.dem, 1, P.sph_visc, c.tmp_vel);
+        LAUNCH(k_xsph_commit, full, 256, P, S, vs, 1, c.tmp_vel, a.sph->velocity);
+    }
+    if (a.dem_visc && step_dem) {
+        LAUNCH(k_xsph, full, 128, P, S, vd, vs, *a.dem, *a.sph, 0, P.dem_visc, c.tmp_vel);
+        LAUNCH(k_xsph_commit, full, 256, P, S, vd, 0, c.tmp_vel, a.dem->velocity);
+    }
+#undef STOP
+    return SNOWB_OK;
+}
+
+static int check_params()
+{
+    if (!g_have_params) return fail(SNOWB_ERR_NO_PARAMS, "snowb_set_sim_params has not been called");
+    return SNOWB_OK;
+}
+
+static int run_steps(snowb_particle_data* sph, uint32_t* sph_size, snowb_particle_data* dem, uint32_t* dem_size,
+                     snowb_particle_data* bnd, uint32_t nb, uint32_t full, snowb_particle_data* buf,
+                     snowb_cell_data scd, snowb_cell_data dcd, snowb_cell_data bcd, snowb_scene_params* scene,
+                     float dt, int iterations, const int* fl, float dTe, const snowb_step_options& opt)
+{
+    TRY(check_params());
+    if (!sph || !dem || !bnd || !buf || !sph_size || !dem_size || !scene)
+        return fail(SNOWB_ERR_INVALID, "null argument");
+    if (*sph_size > full || *dem_size > full) return fail(SNOWB_ERR_INVALID, "set size exceeds full_size");
+    if (opt.substeps < 1) return fail(SNOWB_ERR_INVALID, "substeps must be >= 1");
+    DevParams P = g_P;
+    P.quirks = opt.quirks;
+    if (P.gsx < 4 || P.gsy < 4 || P.gsz < 4) return fail(SNOWB_ERR_INVALID, "grid must be at least 4 cells per axis");
+    TRY(ensure_ctx(full, nb, P.ncells));
+    Ctx& c = g_ctx;
+    StepArgs a{sph, dem, bnd, buf, nb, full, scd, dcd, bcd, dt, iterations,
+               fl[0], fl[1], fl[2], fl[3], fl[4], fl[5], fl[6], fl[7], fl[8], fl[9], fl[10], dTe, opt.stop_after};
+    LAUNCH1(k_set_state, c.S, *sph_size, *dem_size, nb);
+    LAUNCH(k_boundary_prep, nb, 256, bcd, bnd->volume, bnd->massInv, bnd->mass, nb, c.b.p4, c.b.invm, c.b.mass);
+    for (int k = 0; k < opt.substeps; ++k) {
+        const bool step_sph = scene->current_time >= scene->fluid_start_time;
+        const bool step_dem = scene->current_time >= scene->solid_start_time;
+        TRY(substep(P, a, step_sph, step_dem));
+        if (opt.stop_after != 0) break;
+        scene->current_time += dt;
+    }
+    if (opt.sync) {
+        CUDA_TRY(cudaMemcpyAsync(c.S_host, c.S, sizeof(DevState), cudaMemcpyDeviceToHost, g_stream));
+        CUDA_TRY(cudaStreamSynchronize(g_stream));
+        *sph_size = c.S_host->n_sph;
+        *dem_size = c.S_host->n_dem;
+        if (c.S_host->err) return fail(SNOWB_ERR_DEVICE, "device error flag " + std::to_string(c.S_host->err));
+    }
+    return SNOWB_OK;
+}
+
+}  // namespace snowb
+
+using namespace snowb;
+
+// =========================================================================== C ABI
+extern "C" {
+
+int snowb_last_error(void) { return g_err; }
+const char* snowb_last_error_string(void) { return g_msg.c_str(); }
+
+int snowb_allocate_array(void** dev_ptr, size_t size)
+{
+    if (!dev_ptr) return fail(SNOWB_ERR_INVALID, "null pointer");
+    CUDA_TRY(cudaMalloc(dev_ptr, size));
+    return SNOWB_OK;
+}
+
+int snowb_set_sim_params(const snowb_sim_params* params)
+{
+    if (!params) return fail(SNOWB_ERR_INVALID, "null params");
+    for (int k = 0; k < 3; ++k) {
+        uint32_t g = params->grid_size[k];
+        if (g == 0 || (g & (g - 1))) return fail(SNOWB_ERR_INVALID, "grid sizes must be powers of two");
+    }
+    if ((uint64_t)params->grid_size[0] * params->grid_size[1] * params->grid_size[2] != params->num_cells)
+        return fail(SNOWB_ERR_INVALID, "num_cells must equal the grid volume");
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_sim = *params;
+    g_P = derive(g_sim);
+    g_have_params = true;
+    return SNOWB_OK;
+}
+
+int snowb_compute_grid_size(uint32_t n, uint32_t block_size, uint32_t* num_blocks, uint32_t* num_threads)
+{
+    if (!num_blocks || !num_threads) return fail(SNOWB_ERR_INVALID, "null pointer");
+    if (n == 0) { *num_blocks = 0; *num_threads = 0; return SNOWB_OK; }
+    if (block_size == 0) return fail(SNOWB_ERR_INVALID, "block_size must be > 0");
+    *num_threads = block_size < n ? block_size : n;
+    *num_blocks = (n % *num_threads != 0) ? (n / *num_threads + 1) : (n / *num_threads);
+    return SNOWB_OK;
+}
+
+int snowb_calculate_hash(snowb_cell_data cd, const snowb_float3* pos, uint32_t n)
+{
+    TRY(check_params());
+    if (n == 0) return SNOWB_OK;
+    if (!pos || !cd.grid_hash || !cd.grid_index) return fail(SNOWB_ERR_INVALID, "null pointer");
+    LAUNCH(k_calc_hash, n, 256, g_P, cd, pos, n);
+    return SNOWB_OK;
+}
+
+int snowb_sort_particles(snowb_cell_data cd, uint32_t n)
+{
+    TRY(check_params());
+    if (n < 2) return SNOWB_OK;
+    if (!cd.grid_hash || !cd.grid_index) return fail(SNOWB_ERR_INVALID, "null pointer");
+    const uint32_t nc = g_P.ncells;
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (g_ctx.device != dev || g_ctx.ncells != nc) TRY(ensure_ctx(1, 1, nc));
+    TRY(ensure_gen(n, nc));
+    SetBufs& B = g_ctx.gen;
+    CUDA_TRY(cudaMemsetAsync(g_ctx.err_dev, 0, sizeof(uint32_t), g_stream));
+    LAUNCH(k_key_count, n, 256, cd.grid_hash, cd.grid_index, n, nc, B.key, B.val, B.slot, B.cnt, g_ctx.err_dev);
+    const unsigned nb = (nc + SCAN_CHUNK - 1) / SCAN_CHUNK;
+    k_block_sums<<<nb, SCAN_TPB, 0, g_stream>>>(B.cnt, nc, B.bsum, nullptr);
+    // cell_start is not touched by a plain sort: clear nothing (clear_all = 0, n = 0)
+    k_cell_scan<<<nb, SCAN_TPB, 0, g_stream>>>(B.cnt, B.bsum, nc, B.off, nullptr, nullptr, 0u, 0, nullptr);
+    CUDA_TRY(cudaGetLastError());
+    LAUNCH(k_scatter, n, 256, B.key, B.slot, B.off, B.tmp, nullptr, n, nullptr);
+    LAUNCH(k_rank_pairs, n, 256, B.key, B.val, B.off, B.tmp, cd.grid_hash, cd.grid_index, n);
+    uint32_t err = 0;
+    CUDA_TRY(cudaMemcpyAsync(&err, g_ctx.err_dev, sizeof(uint32_t), cudaMemcpyDeviceToHost, g_stream));
+    CUDA_TRY(cudaStreamSynchronize(g_stream));
+    if (err) return fail(SNOWB_ERR_INVALID, "grid_hash holds keys >= num_cells");
+    return SNOWB_OK;
+}
+
+int snowb_reorder_data(snowb_cell_data cd, const snowb_float3* old_pos, uint32_t n, uint32_t num_cells)
+{
+    TRY(check_params());
+    if (!cd.cell_start || !cd.cell_end || !cd.grid_hash || !cd.grid_index || !cd.sorted_pos)
+        return fail(SNOWB_ERR_INVALID, "null pointer");
+    if (num_cells > g_P.ncells) return fail(SNOWB_ERR_INVALID, "num_cells exceeds the cell table");
+    if (num_cells) CUDA_TRY(cudaMemsetAsync(cd.cell_start, 0xff, sizeof(uint32_t) * num_cells, g_stream));
+    if (n == 0) return SNOWB_OK;
+    if (!old_pos) return fail(SNOWB_ERR_INVALID, "null pointer");
+    LAUNCH(k_reorder, n, 256, cd, old_pos, n);
+    return SNOWB_OK;
+}
+
+int snowb_compute_boundary_volume(snowb_cell_data cd, float* mass, float* volume, uint32_t n)
+{
+    TRY(check_params());
+    if (n == 0) return SNOWB_OK;
+    if (!mass || !volume) return fail(SNOWB_ERR_INVALID, "null pointer");
+    LAUNCH(k_boundary_volume, n, 128, g_P, cd, mass, volume, n);
+    return SNOWB_OK;
+}
+
+int snowb_integrate_pbd(snowb_particle_data* particles, float dt, uint32_t n, int cd_on)
+{
+    TRY(check_params());
+    if (!particles) return fail(SNOWB_ERR_INVALID, "null pointer");
+    if (n == 0) return SNOWB_OK;
+    TRY(ensure_ctx(g_ctx.cap ? g_ctx.cap : 1, g_ctx.bcap ? g_ctx.bcap : 1, g_P.ncells));
+    DevParams P = g_P;
+    P.quirks = SNOWB_QUIRKS_FIXED;   // exactly n particles (the caller owns the launch size)
+    LAUNCH1(k_set_state, g_ctx.S, n, 0u, 0u);
+    Sets X{*particles, *particles, *particles};
+    LAUNCH(k_integrate, n, 256, P, g_ctx.S, X, n, dt, cd_on, 1, 0);
+    return SNOWB_OK;
+}
+
+int snowb_connect_and_record(snowb_particle_data* dem, uint32_t n, snowb_cell_data dcd, int dynamic)
+{
+    TRY(check_params());
+    if (!dem) return fail(SNOWB_ERR_INVALID, "null pointer");
+    if (n == 0) return SNOWB_OK;
+    DevParams P = g_P;
+    if (P.gsx < 4 || P.gsy < 4 || P.gsz < 4) return fail(SNOWB_ERR_INVALID, "grid must be at least 4 cells per axis");
+    TRY(ensure_ctx(g_ctx.cap > n ? g_ctx.cap : n, g_ctx.bcap ? g_ctx.bcap : 1, P.ncells));
+    Ctx& c = g_ctx;
+    LAUNCH1(k_set_state, c.S, 0u, n, 0u);
+    CUDA_TRY(cudaMemsetAsync(c.fs, 0, sizeof(uint32_t) * P.ncells, g_stream));
+    CUDA_TRY(cudaMemsetAsync(c.fe, 0, sizeof(uint32_t) * P.ncells, g_stream));
+    LAUNCH(k_fresh_ranges, n, 256, dcd.grid_hash, n, c.fs, c.fe);
+    // this entry point reads positions from the caller's sorted_pos only
+    SetView vd = make_view(dcd, nullptr, dem->mass);
+    vd.p4 = nullptr;
+    // the view's compact copy is not available here: fill it from sorted_pos
+    LAUNCH(k_boundary_prep, n, 256, dcd, dem->mass, dem->massInv, dem->mass, n, c.s[1].p4, c.s[1].invm, c.s[1].lambda);
+    vd.p4 = c.s[1].p4;
+    LAUNCH(k_link_filter, n, 128, P, c.S, vd, *dem, dynamic, c.active);
+    for (uint32_t col = 0; col < 8; ++col)
+        LAUNCH(k_link_colour, (P.gsx / 4) * (P.gsy / 4) * (P.gsz / 4), 64, P, c.S, vd, *dem, c.fs, c.fe, c.active, col,
+               dynamic);
+    CUDA_TRY(cudaStreamSynchronize(g_stream));
+    return SNOWB_OK;
+}
+
+static snowb_step_options default_options()
+{
+    snowb_step_options o;
+    o.quirks = g_quirks; o.substeps = 1; o.stop_after = 0; o.use_graph = 0; o.sync = 1;
+    return o;
+}
+
+int snowb_snow_simulation(snowb_particle_data* sph, uint32_t* sph_size, snowb_particle_data* dem, uint32_t* dem_size,
+                          snowb_particle_data* boundary, uint32_t boundary_size, uint32_t full_size,
+                          snowb_particle_data* buffer, snowb_cell_data scd, snowb_cell_data dcd, snowb_cell_data bcd,
+                          snowb_scene_params* scene, float dt, int iterations, int sph_dem_correction,
+                          int sph_sph_correction, int dem_friction, int compute_temperature, int change_phase,
+                          int simulate_freezing, int simulate_melting, int dem_viscosity, int use_interlink,
+                          int dynamic_max_connections, int cd_on, float temperature_variation)
+{
+    const int fl[11] = {sph_dem_correction, sph_sph_correction, dem_friction, compute_temperature, change_phase,
+                        simulate_freezing, simulate_melting, dem_viscosity, use_interlink, dynamic_max_connections,
+                        cd_on};
+    snowb_step_options o = default_options();
+    return run_steps(sph, sph_size, dem, dem_size, boundary, boundary_size, full_size, buffer, scd, dcd, bcd, scene,
+                     dt, iterations, fl, temperature_variation, o);
+}
+
+int snowb_snow_simulation_ex(snowb_particle_data* sph, uint32_t* sph_size, snowb_particle_data* dem,
+                             uint32_t* dem_size, snowb_particle_data* boundary, uint32_t boundary_size,
+                             uint32_t full_size, snowb_particle_data* buffer, snowb_cell_data scd,
+                             snowb_cell_data dcd, snowb_cell_data bcd, snowb_scene_params* scene, float dt,
+                             int iterations, int sph_dem_correction, int sph_sph_correction, int dem_friction,
+                             int compute_temperature, int change_phase, int simulate_freezing, int simulate_melting,
+                             int dem_viscosity, int use_interlink, int dynamic_max_connections, int cd_on,
+                             float temperature_variation, const snowb_step_options* options)
+{
+    const int fl[11] = {sph_dem_correction, sph_sph_correction, dem_friction, compute_temperature, change_phase,
+                        simulate_freezing, simulate_melting, dem_viscosity, use_interlink, dynamic_max_connections,
+                        cd_on};
+    snowb_step_options o = options ? *options : default_options();
+    if (o.quirks != SNOWB_QUIRKS_REFERENCE && o.quirks != SNOWB_QUIRKS_FIXED)
+        return fail(SNOWB_ERR_INVALID, "unknown quirk mode");
+    return run_steps(sph, sph_size, dem, dem_size, boundary, boundary_size, full_size, buffer, scd, dcd, bcd, scene,
+                     dt, iterations, fl, temperature_variation, o);
+}
+
+int snowb_read_sizes(uint32_t* sph_size, uint32_t* dem_size)
+{
+    if (!g_ctx.S) return fail(SNOWB_ERR_INVALID, "no step has run");
+    CUDA_TRY(cudaMemcpyAsync(g_ctx.S_host, g_ctx.S, sizeof(DevState), cudaMemcpyDeviceToHost, g_stream));
+    CUDA_TRY(cudaStreamSynchronize(g_stream));
+    if (sph_size) *sph_size = g_ctx.S_host->n_sph;
+    if (dem_size) *dem_size = g_ctx.S_host->n_dem;
+    return SNOWB_OK;
+}
+
+int snowb_set_quirks(int mode)
+{
+    if (mode != SNOWB_QUIRKS_REFERENCE && mode != SNOWB_QUIRKS_FIXED) return fail(SNOWB_ERR_INVALID, "unknown quirk mode");
+    g_quirks = mode;
+    return SNOWB_OK;
+}
+
+int snowb_set_stream(void* stream)
+{
+    g_stream = reinterpret_cast<cudaStream_t>(stream);
+    return SNOWB_OK;
+}
+
+int snowb_synchronize(void)
+{
+    CUDA_TRY(cudaStreamSynchronize(g_stream));
+    return SNOWB_OK;
+}
+
+int snowb_energy_momentum(const snowb_particle_data* sph, uint32_t ns, const snowb_particle_data* dem, uint32_t nd,
+                          double out[4])
+{
+    TRY(check_params());
+    if (!sph || !dem || !out) return fail(SNOWB_ERR_INVALID, "null pointer");
+    TRY(ensure_ctx(g_ctx.cap ? g_ctx.cap : 1, g_ctx.bcap ? g_ctx.bcap : 1, g_P.ncells));
+    const int nb = 512;
+    k_energy_partial<<<nb, 256, 0, g_stream>>>(*sph, ns, *dem, nd, (double)g_sim.C_water, (double)g_sim.C_snow,
+                                               g_ctx.epart);
+    k_energy_final<<<1, 32, 0, g_stream>>>(g_ctx.epart, nb, g_ctx.eout);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(out, g_ctx.eout, 4 * sizeof(double), cudaMemcpyDeviceToHost, g_stream));
+    CUDA_TRY(cudaStreamSynchronize(g_stream));
+    return SNOWB_OK;
+}
+
+int snowb_release(void)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    free_ctx(g_ctx);
+    return SNOWB_OK;
+}
+
+}  // extern "C"

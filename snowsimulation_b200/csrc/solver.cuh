@@ -1,0 +1,799 @@
+// solver.cuh -- constraint and integration kernels of the substep.
+//
+// One thread per particle in sorted order (neighbouring threads share cells, so the
+// 27-cell gathers hit L1), fused across the particle sets of a stage, grid-stride over
+// the set sizes held on the device.  Each neighbor sum keeps the reference's structure
+// (per-cell partial sums added to the running total, cells z-y-x, particles ascending)
+// and skips only terms that are exactly zero: a term is evaluated when
+// d2 < cut-off, which is equivalent to the reference's distance test d < h (resp.
+// d < 2r, d <= 2r) because sqrt is correctly rounded and monotone.
+#pragma once
+#include "common.cuh"
+
+namespace snowb {
+
+struct Sets {
+    snowb_particle_data sph, dem, bnd;
+};
+// compact sorted attribute copies (valid for sorted index j < n of the last sort)
+struct Sorted {
+    float* invm;     // massInv
+    float* contrib;  // contrib
+    float* lambda;   // lambda (written by the lambda stage)
+    float* mass;     // boundary only: mass
+};
+
+// ------------------------------------------------------------ per-cell neighbour sums
+// sum of w_j * W(d): w = mass (fluid/snow view) or rho0*V (boundary view, vol=true)
+__device__ __forceinline__ float acc_W(const DevParams& P, float acc, const SetView& v, float3 p, int3 g,
+                                       uint32_t skip, bool vol)
+{
+    FOR27 {
+        float cs = 0.f;
+        uint32_t s, e;
+        if (v.range(P, g, ox, oy, oz, s, e))
+            for (uint32_t j = s; j < e; ++j) {
+                if (j == skip) continue;
+                float4 q = v.pw(j);
+                float3 dv = sub3(p, xyz(q));
+                float d2 = dot3(dv, dv);
+                if (d2 < P.h2_lt) {
+                    float w = vol ? P.rho0 * q.w : q.w;
+                    cs += w * W_poly6(P, sqrtf(d2));
+                }
+            }
+        acc += cs;
+    }
+    return acc;
+}
+// lambda denominator; mode 0: 1/rho0, 1: (1/rho0)*((rho0*V_j)/m_self), 2: ... / m_j
+__device__ __forceinline__ float acc_gradsq(const DevParams& P, float acc, const SetView& v, float3 p, int3 g,
+                                            uint32_t skip, int mode, float m_self, const float* mass_s,
+                                            const float* mass_o)
+{
+    FOR27 {
+        float cs = 0.f;
+        uint32_t s, e;
+        if (v.range(P, g, ox, oy, oz, s, e))
+            for (uint32_t j = s; j < e; ++j) {
+                if (j == skip) continue;
+                float4 q = v.pw(j);
+                float3 dv = sub3(p, xyz(q));
+                float d2 = dot3(dv, dv);
+                if (d2 < P.h2_lt) {
+                    float d = sqrtf(d2);
+                    float sc;
+                    if (mode == 0) sc = P.inv_rho0;
+                    else {
+                        float m = mode == 1 ? m_self : v.attr(mass_s, mass_o, j);
+                        sc = P.inv_rho0 * ((P.rho0 * q.w) / m);
+                    }
+                    float3 gc = sc3(sc, G_spiky(P, dv, d));
+                    cs += dot3(gc, gc);
+                }
+            }
+        acc += cs;
+    }
+    return acc;
+}
+// pbf_correction (:883-929)
+__device__ __forceinline__ float3 acc_pbf_own(const DevParams& P, float3 acc, const SetView& v, float3 p, int3 g,
+                                              uint32_t skip, float li, const float* lam_s, const float* lam_o,
+                                              const float* con_s, const float* con_o, float dt)
+{
+    FOR27 {
+        float3 cs = f3(0.f, 0.f, 0.f);
+        uint32_t s, e;
+        if (v.range(P, g, ox, oy, oz, s, e))
+            for (uint32_t j = s; j < e; ++j) {
+                if (j == skip) continue;
+                float3 dv = sub3(p, v.pos(j));
+                float d2 = dot3(dv, dv);
+                if (d2 < P.h2_lt) {
+                    float d = sqrtf(d2);
+                    float3 gr = G_spiky(P, dv, d);
+                    float sc = scorr_of(P, d, dt);
+                    float lj = v.attr(lam_s, lam_o, j), cj = v.attr(con_s, con_o, j);
+                    cs = add3(cs, sc3(cj * ((li + lj) + sc), gr));
+                }
+            }
+        acc = add3(acc, cs);
+    }
+    return acc;
+}
+// pbf_correction_boundary (:932-979)
+__device__ __forceinline__ float3 acc_pbf_bnd(const DevParams& P, float3 acc, const SetView& v, float3 p, int3 g,
+                                              float li, const float* lam_s, const float* lam_o, float dt)
+{
+    FOR27 {
+        float3 cs = f3(0.f, 0.f, 0.f);
+        uint32_t s, e;
+        if (v.range(P, g, ox, oy, oz, s, e))
+            for (uint32_t j = s; j < e; ++j) {
+                float3 dv = sub3(p, v.pos(j));
+                float d2 = dot3(dv, dv);
+                if (d2 < P.h2_lt) {
+                    float d = sqrtf(d2);
+                    float3 gr = G_spiky(P, dv, d);
+                    float sc = scorr_of(P, d, dt);
+                    cs = add3(cs, sc3((li + v.attr(lam_s, lam_o, j)) + sc, gr));
+                }
+            }
+        acc = add3(acc, cs);
+    }
+    return acc;
+}
+// pbf_correction_coupling (:982-1034); reference quirks: the self-skip compares indices of
+// two different sets, and s_corr is taken as 0 (it reads an uninitialised value times 0)
+__device__ __forceinline__ float3 acc_pbf_cpl(const DevParams& P, float3 acc, const SetView& v, float3 p, int3 g,
+                                              uint32_t skip, float li, const float* lam_s, const float* lam_o,
+                                              float dt)
+{
+    const bool ref = P.quirks == SNOWB_QUIRKS_REFERENCE;
+    FOR27 {
+        float3 cs = f3(0.f, 0.f, 0.f);
+        uint32_t s, e;
+        if (v.range(P, g, ox, oy, oz, s, e))
+            for (uint32_t j = s; j < e; ++j) {
+                if (ref && j == skip) continue;
+                float3 dv = sub3(p, v.pos(j));
+                float d2 = dot3(dv, dv);
+                if (d2 < P.r2_le) {
+                    float d = sqrtf(d2);
+                    float3 gr = G_poly6(P, dv, d);
+                    float x = W_poly6(P, d) / P.scorr_div;
+                    float x4 = (x * x) * (x * x);
+                    float sc = ref ? ((((-P.scorr_coeff) * 0.f) * x4) * dt) * dt
+                                   : ((-P.scorr_coeff * x4) * dt) * dt;
+                    cs = add3(cs, sc3((li + v.attr(lam_s, lam_o, j)) + sc, gr));
+                }
+            }
+        acc = add3(acc, cs);
+    }
+    return acc;
+}
+// non-penetration: pbd_distance_correction_contrib (:1470-1527, skip) and
+// pbd_distance_correction_coupling_contrib (:1648-1705, no skip)
+__device__ __forceinline__ float3 acc_contact(const DevParams& P, float3 acc, const SetView& v, float3 p, int3 g,
+                                              uint32_t skip, float w0, const float* invm_s, const float* invm_o)
+{
+    FOR27 {
+        float3 cs = f3(0.f, 0.f, 0.f);
+        uint32_t s, e;
+        if (v.range(P, g, ox, oy, oz, s, e))
+            for (uint32_t j = s; j < e; ++j) {
+                if (j == skip) continue;
+                float3 dv = sub3(p, v.pos(j));
+                float d2 = dot3(dv, dv);
+                if (d2 < P.r2_lt) {
+                    float d = sqrtf(d2);
+                    float w1 = v.attr(invm_s, invm_o, j);
+                    float ws = w0 + w1;
+                    float C = d - P.two_r;
+                    float3 n = div3(dv, d + P.pbd_eps);
+                    cs = add3(cs, sc3(((-w0) * (1.f / ws)) * C, n));
+                }
+            }
+        acc = add3(acc, cs);
+    }
+    return acc;
+}
+// pbd_sph_sph_distance_correction (:1586-1646)
+__device__ __forceinline__ float3 acc_contact_sph(const DevParams& P, float3 acc, const SetView& v, float3 p,
+                                                  int3 g, uint32_t skip, float w0, float contrib_i,
+                                                  const float* invm_s, const float* invm_o)
+{
+    if (!(contrib_i <= 0.99f)) return add3(acc, f3(0.f, 0.f, 0.f));
+    return acc_contact(P, acc, v, p, g, skip, w0, invm_s, invm_o);
+}
+
+// ======================================================================== density
+// compute_snow_{sph,dem_sph,boundary}_density_d (:2219-2528), fused over the 3 sets.
+__global__ void __launch_bounds__(128) k_density(DevParams P, const DevState* __restrict__ S, SetView vs, SetView vd,
+                                                 SetView vb, Sets X)
+{
+    const uint32_t ns = S->n_sph, nd = S->n_dem, nb = S->n_b;
+    vs.n = ns; vd.n = nd; vb.n = nb;
+    GRID_LOOP(t, ns + nd + nb) {
+        float rho;
+        float* dens; float* Cc; uint32_t o;
+        if (t < ns) {
+            const uint32_t i = t; o = vs.gi[i];
+            float3 p = xyz(vs.p4[i]); int3 g = grid_pos(P, p);
+            rho = X.sph.mass[o] * P.W0;
+            rho = acc_W(P, rho, vs, p, g, i, false);
+            rho = acc_W(P, rho, vd, p, g, SNOWB_UMAX, false);
+            rho = acc_W(P, rho, vb, p, g, SNOWB_UMAX, true);
+            dens = X.sph.density; Cc = X.sph.C;
+        } else if (t < ns + nd) {
+            const uint32_t i = t - ns; o = vd.gi[i];
+            float3 p = xyz(vd.p4[i]); int3 g = grid_pos(P, p);
+            rho = X.dem.mass[o] * P.W0;
+            rho = acc_W(P, rho, vd, p, g, i, false);
+            rho = acc_W(P, rho, vs, p, g, SNOWB_UMAX, false);
+            rho = acc_W(P, rho, vb, p, g, SNOWB_UMAX, true);
+            dens = X.dem.density; Cc = X.dem.C;
+        } else {
+            const uint32_t i = t - ns - nd; o = vb.gi[i];
+            float3 p = xyz(vb.p4[i]); int3 g = grid_pos(P, p);
+            rho = (P.rho0 * X.bnd.volume[o]) * P.W0;
+            rho = acc_W(P, rho, vb, p, g, i, true);
+            rho = acc_W(P, rho, vd, p, g, SNOWB_UMAX, false);
+            rho = acc_W(P, rho, vs, p, g, SNOWB_UMAX, false);
+            dens = X.bnd.density; Cc = X.bnd.C;
+        }
+        dens[o] = rho;
+        float c = (rho / P.rho0) - 1.f;
+        Cc[o] = c > 0.f ? c : 0.f;
+    }
+}
+
+// ======================================================================== lambda
+// compute_snow_sph_lambdas_d / compute_dem_sph_lambdas_d / compute_snow_boundary_lambdas_d
+// (:2598-2898).  Writes lambda (original order) and its sorted copy.
+__global__ void __launch_bounds__(128) k_lambda(DevParams P, const DevState* __restrict__ S, SetView vs, SetView vd,
+                                                SetView vb, Sets X, Sorted ss, Sorted sd, Sorted sb)
+{
+    const uint32_t ns = S->n_sph, nd = S->n_dem, nb = S->n_b;
+    vs.n = ns; vd.n = nd; vb.n = nb;
+    const float3 z = f3(0.f, 0.f, 0.f);
+    GRID_LOOP(t, ns + nd + nb) {
+        if (t < ns) {
+            const uint32_t i = t, o = vs.gi[i];
+            float3 p = xyz(vs.p4[i]); int3 g = grid_pos(P, p);
+            float lam = -X.sph.C[o];
+            float gs = dot3(z, z);
+            gs = acc_gradsq(P, gs, vs, p, g, i, 0, 0.f, nullptr, nullptr);
+            gs = acc_gradsq(P, gs, vd, p, g, SNOWB_UMAX, 0, 0.f, nullptr, nullptr);
+            gs = acc_gradsq(P, gs, vb, p, g, SNOWB_UMAX, 1, X.sph.mass[o], nullptr, nullptr);
+            lam = lam / (gs + P.eps);
+            X.sph.lambda[o] = lam; ss.lambda[i] = lam;
+        } else if (t < ns + nd) {
+            const uint32_t i = t - ns, o = vd.gi[i];
+            float3 p = xyz(vd.p4[i]); int3 g = grid_pos(P, p);
+            float lam = -X.dem.C[o];
+            float gs = dot3(z, z);
+            gs = acc_gradsq(P, gs, vd, p, g, i, 0, 0.f, nullptr, nullptr);
+            gs = acc_gradsq(P, gs, vs, p, g, SNOWB_UMAX, 0, 0.f, nullptr, nullptr);
+            gs = acc_gradsq(P, gs, vb, p, g, SNOWB_UMAX, 1, X.dem.mass[o], nullptr, nullptr);
+            lam = lam / (gs + P.eps);
+            X.dem.lambda[o] = lam; sd.lambda[i] = lam;
+        } else {
+            const uint32_t i = t - ns - nd, o = vb.gi[i];
+            float3 p = xyz(vb.p4[i]); int3 g = grid_pos(P, p);
+            float lam = -X.bnd.C[o];
+            float gs = dot3(z, z);
+            gs = acc_gradsq(P, gs, vb, p, g, i, 2, 0.f, sb.mass, X.bnd.mass);
+            gs = acc_gradsq(P, gs, vs, p, g, SNOWB_UMAX, 0, 0.f, nullptr, nullptr);
+            gs = acc_gradsq(P, gs, vd, p, g, SNOWB_UMAX, 0, 0.f, nullptr, nullptr);
+            lam = lam / (gs + P.eps);
+            X.bnd.lambda[o] = lam; sb.lambda[i] = lam;
+        }
+    }
+}
+
+// ==================================================== PBF + water-side contact corrections
+// compute_pbf_sph_correction (:3070-3184) fused with compute_sph_dem_distance_correction
+// (:2061-2110) and compute_sph_sph_distance_correction (:2164-2217) for water, and
+// compute_pbf_new_dem_correction (:3187-3304) for snow.  Each water particle adds its
+// terms to its correction in the reference's kernel order.
+struct StageFlags {
+    int correct_dem, sph_sph, interlink, step_sph, step_dem;
+};
+__global__ void __launch_bounds__(128) k_pbf(DevParams P, const DevState* __restrict__ S, SetView vs, SetView vd,
+                                             SetView vb, Sets X, Sorted ss, Sorted sd, Sorted sb, float dt,
+                                             StageFlags F)
+{
+    const uint32_t ns = S->n_sph, nd = S->n_dem, nb = S->n_b;
+    vs.n = ns; vd.n = nd; vb.n = nb;
+    const bool ref = P.quirks == SNOWB_QUIRKS_REFERENCE;
+    GRID_LOOP(t, ns + nd) {
+        if (t < ns) {
+            const uint32_t i = t, o = vs.gi[i];
+            float3 p = xyz(vs.p4[i]); int3 g = grid_pos(P, p);
+            const float li = ss.lambda[i];
+            float3 c = f3(0.f, 0.f, 0.f);
+            c = acc_pbf_own(P, c, vs, p, g, i, li, ss.lambda, X.sph.lambda, ss.contrib, X.sph.contrib, dt);
+            c = acc_pbf_cpl(P, c, vd, p, g, i, li, sd.lambda, X.dem.lambda, dt);
+            c = acc_pbf_bnd(P, c, vb, p, g, li, sb.lambda, X.bnd.lambda, dt);
+            c = sc3(P.inv_rho0, c);
+            const float ci = X.sph.contrib[o];
+            c = sc3(ci, c);
+            if (nan3(c)) c = f3(0.f, 0.f, 0.f);
+            float3 acc = add3(ldv3(X.sph.correction, o), c);
+            const float3 z = f3(0.f, 0.f, 0.f);
+            const float w0 = X.sph.massInv[o];
+            if (F.correct_dem) {     // compute_sph_dem_distance_correction
+                float3 d = acc_contact(P, z, vd, p, g, SNOWB_UMAX, w0, sd.invm, X.dem.massInv);
+                d = sc3(1.f - ci, d);
+                if (nan3(d)) d = z;
+                acc = add3(acc, sc3(P.k_stretch, d));
+            }
+            if (F.sph_sph) {         // compute_sph_sph_distance_correction
+                float3 d = acc_contact_sph(P, z, vs, p, g, i, w0, ci, ss.invm, X.sph.massInv);
+                d = sc3(1.f - ci, d);
+                if (nan3(d)) d = z;
+                acc = add3(acc, d);
+            }
+            st3(X.sph.correction, o, acc);
+        } else {
+            const uint32_t i = t - ns;
+            const uint32_t o = ref ? vs.gi[i] : vd.gi[i];   // Q3: SPH grid_index in the reference
+            float3 p = xyz(vd.p4[i]); int3 g = grid_pos(P, p);
+            const float li = X.dem.lambda[o];
+            float3 c = f3(0.f, 0.f, 0.f);
+            c = acc_pbf_cpl(P, c, vs, p, g, i, li, ss.lambda, X.sph.lambda, dt);
+            if (nan3(c)) c = f3(0.f, 0.f, 0.f);
+            c = acc_pbf_own(P, c, vd, p, g, i, li, sd.lambda, X.dem.lambda, sd.contrib, X.dem.contrib, dt);
+            if (nan3(c)) c = f3(0.f, 0.f, 0.f);
+            c = acc_pbf_bnd(P, c, vb, p, g, li, sb.lambda, X.bnd.lambda, dt);
+            if (nan3(c)) c = f3(0.f, 0.f, 0.f);
+            c = sc3(P.inv_rho0, c);
+            c = sc3(1.f - X.dem.contrib[o], c);
+            if (nan3(c)) c = f3(0.f, 0.f, 0.f);
+            float* q = reinterpret_cast<float*>(X.dem.correction) + 3ull * o;
+            if (ref) {   // targets can repeat in the reference's indexing
+                atomicAdd(q, c.x); atomicAdd(q + 1, c.y); atomicAdd(q + 2, c.z);
+            } else {
+                q[0] += c.x; q[1] += c.y; q[2] += c.z;
+            }
+        }
+    }
+    (void)nb;
+}
+
+// ============================================================ snow-side corrections
+// delete_record (:4624-4658): remove the link from both particles' slot lists.
+__device__ __forceinline__ void delete_record(const snowb_particle_data& D, uint32_t M, uint32_t i0, uint32_t i1)
+{
+    for (uint32_t s = i0 * M; s < (i0 + 1) * M; ++s)
+        if (atomicCAS(D.connect_record + s, i1, SNOWB_UMAX) == i1) { atomicExch(D.connect_length + s, 0.f); break; }
+    for (uint32_t s = i1 * M; s < (i1 + 1) * M; ++s)
+        if (atomicCAS(D.connect_record + s, i0, SNOWB_UMAX) == i0) { atomicExch(D.connect_length + s, 0.f); break; }
+}
+// compute_interlink_correction (:4661-4739).  Both ends of a link hold the same length
+// and see the same distance, so whichever end breaks it first, neither adds a correction.
+__device__ __forceinline__ float3 link_corr(const DevParams& P, const snowb_particle_data& D, uint32_t i0,
+                                            uint32_t i1, float L, uint32_t n)
+{
+    const float3 z = f3(0.f, 0.f, 0.f);
+    if (i0 == i1 || i0 >= n || i1 >= n || L == 0.f) return z;
+    float3 v = sub3(ldv3(D.predict_positions, i0), ldv3(D.predict_positions, i1));
+    float dist = len3(v);
+    if (dist > P.brk * L) { delete_record(D, P.maxc, i0, i1); return z; }
+    if (dist > P.h) { delete_record(D, P.maxc, i0, i1); return z; }
+    float w0 = D.massInv[i0], w1 = D.massInv[i1];
+    float ws = w0 + w1, C = dist - L;
+    float3 n3 = div3(v, dist + P.pbd_eps);
+    float3 r = sc3(((P.k_ref * -w0) * (1.f / ws)) * C, n3);
+    if (len3(r) > 1.f) return z;
+    if (nan3(r)) return z;
+    if (inf3(r)) return z;
+    return r;
+}
+// compute_dem_sph_distance_correction (:2112-2162), compute_dem_distance_correction
+// (:1765-1834) and solve_snow_interlink_constraint_d (:4742-4765) for snow particle o,
+// added to its correction in the reference's kernel order (after the PBF pass).
+__global__ void __launch_bounds__(128) k_dem_corr(DevParams P, const DevState* __restrict__ S, SetView vs, SetView vd,
+                                                  SetView vb, Sets X, Sorted ss, Sorted sd, Sorted sb, StageFlags F)
+{
+    const uint32_t ns = S->n_sph, nd = S->n_dem, nb = S->n_b;
+    vs.n = ns; vd.n = nd; vb.n = nb;
+    const float3 z = f3(0.f, 0.f, 0.f);
+    GRID_LOOP(i, nd) {
+        const uint32_t o = vd.gi[i];
+        float3 p = xyz(vd.p4[i]); int3 g = grid_pos(P, p);
+        const float w0 = X.dem.massInv[o], ci = X.dem.contrib[o];
+        float3 acc = ldv3(X.dem.correction, o);
+        if (F.correct_dem) {
+            float3 d = acc_contact(P, z, vs, p, g, SNOWB_UMAX, w0, ss.invm, X.sph.massInv);
+            d = sc3(P.k_stretch * ci, d);
+            if (nan3(d)) d = z;
+            acc = add3(acc, d);
+        }
+        {
+            float3 d = acc_contact(P, z, vd, p, g, i, w0, sd.invm, X.dem.massInv);
+            d = acc_contact(P, d, vb, p, g, SNOWB_UMAX, w0, sb.invm, X.bnd.massInv);
+            d = sc3(ci, d);
+            if (nan3(d)) d = z;
+            acc = add3(acc, d);
+        }
+        if (F.interlink) {
+            const uint32_t M = P.maxc;
+            volatile const uint32_t* rec = X.dem.connect_record;
+            volatile const float* len = X.dem.connect_length;
+            float3 d = z;
+            for (uint32_t s = M * o; s < M * (o + 1); ++s) {
+                const uint32_t j = rec[s];
+                if (j != SNOWB_UMAX) d = add3(d, link_corr(P, X.dem, o, j, len[s], nd));
+            }
+            if (nan3(d)) d = z;
+            acc = add3(acc, d);
+        }
+        st3(X.dem.correction, o, acc);
+    }
+    (void)ns; (void)nb;
+}
+
+// ======================================================================= apply
+// apply_correction (:1342-1380); limits carry the reference's launch sizes (Q12).
+__device__ __forceinline__ uint32_t launch_limit(const DevParams& P, uint32_t n0, uint32_t n)
+{
+    return P.quirks == SNOWB_QUIRKS_REFERENCE ? umin32(coverage(n0), n) : n;
+}
+__global__ void k_apply(DevParams P, const DevState* __restrict__ S, SetView vs, SetView vd, Sets X, int do_sph,
+                        int do_dem)
+{
+    const uint32_t ls = do_sph ? launch_limit(P, S->n0_sph, S->n_sph) : 0u;
+    const uint32_t ld = do_dem ? launch_limit(P, S->n0_dem, S->n_dem) : 0u;
+    GRID_LOOP(t, ls + ld) {
+        const bool w = t < ls;
+        const uint32_t i = w ? t : t - ls;
+        const SetView& v = w ? vs : vd;
+        const snowb_particle_data& D = w ? X.sph : X.dem;
+        const uint32_t o = v.gi[i];
+        float3 np = add3(xyz(v.p4[i]), sc3(P.sor, ldv3(D.correction, o)));
+        st3(D.new_positions, o, np);
+        st3(D.predict_positions, o, np);
+        st3(D.correction, o, f3(0.f, 0.f, 0.f));
+    }
+}
+
+// ==================================================================== friction
+// compute_friction_correction (:1989-2059) with pbd_friction_correction{,_boundary}
+// (:1836-1987); overwrites the correction.
+__device__ __forceinline__ float3 friction_term(const DevParams& P, float3 dx, float w0, float w1, float d, float3 v)
+{
+    float ws = w0 + w1;
+    float3 n = div3(v, d + P.pbd_eps);
+    float pen = P.two_r - d;
+    float3 dxt = sub3(dx, sc3(dot3(dx, n), n));
+    float thr = P.mu_s * pen;
+    float len = len3(dxt);
+    if (len3(dxt) > thr) {
+        float c = fminf((P.mu_k * pen) / (len + 0.000001f), 1.f);
+        dxt = sc3(c, dxt);
+    }
+    return sc3(-(w0 / ws), dxt);
+}
+__global__ void __launch_bounds__(128) k_friction(DevParams P, const DevState* __restrict__ S, SetView vd, SetView vb,
+                                                  Sets X, Sorted sd, Sorted sb)
+{
+    vd.n = S->n_dem; vb.n = S->n_b;
+    const uint32_t ld = launch_limit(P, S->n0_dem, S->n_dem);
+    GRID_LOOP(i, ld) {
+        const uint32_t o = vd.gi[i];
+        float3 p = xyz(vd.p4[i]);
+        float3 op0 = ldv3(X.dem.positions, o);
+        const float w0 = X.dem.massInv[o];
+        int3 g = grid_pos(P, p);
+        float3 c = f3(0.f, 0.f, 0.f);
+        FOR27 {
+            float3 cs = f3(0.f, 0.f, 0.f);
+            uint32_t s, e;
+            if (vd.range(P, g, ox, oy, oz, s, e))
+                for (uint32_t j = s; j < e; ++j) {
+                    if (j == i) continue;
+                    float3 pp1 = vd.pos(j);
+                    float3 v = sub3(p, pp1);
+                    float d2 = dot3(v, v);
+                    if (d2 < P.r2_le) {
+                        const uint32_t oj = vd.gi[j];
+                        float3 op1 = ldv3(X.dem.positions, oj);
+                        float3 dx = add3(sub3(p, op0), sub3(pp1, op1));
+                        cs = add3(cs, friction_term(P, dx, w0, vd.attr(sd.invm, X.dem.massInv, j), sqrtf(d2), v));
+                    }
+                }
+            c = add3(c, cs);
+        }
+        FOR27 {
+            float3 cs = f3(0.f, 0.f, 0.f);
+            uint32_t s, e;
+            if (vb.range(P, g, ox, oy, oz, s, e))
+                for (uint32_t j = s; j < e; ++j) {
+                    float3 v = sub3(p, vb.pos(j));
+                    float d2 = dot3(v, v);
+                    if (d2 < P.r2_le)
+                        cs = add3(cs, friction_term(P, sub3(p, op0), w0, vb.attr(sb.invm, X.bnd.massInv, j), sqrtf(d2), v));
+                }
+            c = add3(c, cs);
+        }
+        if (nan3(c)) c = f3(0.f, 0.f, 0.f);
+        st3(X.dem.correction, o, c);
+    }
+}
+
+// =================================================================== integrate
+// integrate_pbd_cd_d (:467-540) / integrate_pbd_d (:447-465).  The reference kernel has no
+// bounds check, so it runs over its whole launch (clamped to the allocation here).
+__device__ __forceinline__ void integrate_one(const DevParams& P, const snowb_particle_data& D, uint32_t i, float dt,
+                                              int cd_on)
+{
+    float3 tv = add3(ldv3(D.velocity, i), f3(dt * P.gx, dt * P.gy, dt * P.gz));
+    tv = f3(tv.x * P.damping, tv.y * P.damping, tv.z * P.damping);
+    float3 pos = ldv3(D.positions, i);
+    if (!cd_on) {
+        float3 pp = add3(pos, sc3(dt, tv));
+        st3(D.predict_positions, i, pp);
+        st3(D.velocity, i, tv);
+        st3(D.new_positions, i, pp);
+        return;
+    }
+    float3 tp = add3(pos, sc3(dt, tv));
+    if (tp.x + P.r >= 1.0f) { tv.x = -fabsf(tv.x); tv = sc3(P.b_damping, tv); }
+    if (tp.x - P.r <= -1.0f) { tv.x = fabsf(tv.x); tv = sc3(P.b_damping, tv); }
+    if (tp.z + P.r >= 1.0f) { tv.z = -fabsf(tv.z); tv = sc3(P.b_damping, tv); }
+    if (tp.z - P.r <= -1.0f) { tv.z = fabsf(tv.z); tv = sc3(P.b_damping, tv); }
+    if (pos.y - P.r <= 0.f) {
+        pos.y = P.r;
+        reinterpret_cast<float*>(D.positions)[3ull * i + 1] = P.r;
+        tv.y = fabsf(tv.y);
+        tv = sc3(P.b_damping, tv);
+    }
+    if (len3(tv) > P.max_speed) tv = sc3(P.max_speed / len3(tv), tv);
+    float3 pp = add3(pos, sc3(dt, tv));
+    st3(D.predict_positions, i, pp);
+    st3(D.velocity, i, tv);
+    st3(D.new_positions, i, pp);
+    float c = D.contrib[i];
+    if (c < 0.99f) c += P.blending;
+    if (c >= 0.99f) c = 1.f;
+    D.contrib[i] = c;
+}
+__global__ void k_integrate(DevParams P, const DevState* __restrict__ S, Sets X, uint32_t full, float dt, int cd_on,
+                            int do_sph, int do_dem)
+{
+    const bool ref = P.quirks == SNOWB_QUIRKS_REFERENCE;
+    const uint32_t ls = do_sph ? (ref ? umin32(coverage(S->n_sph), full) : S->n_sph) : 0u;
+    const uint32_t ld = do_dem ? (ref ? umin32(coverage(S->n_dem), full) : S->n_dem) : 0u;
+    GRID_LOOP(t, ls + ld) {
+        if (t < ls) integrate_one(P, X.sph, t, dt, cd_on);
+        else integrate_one(P, X.dem, t - ls, dt, cd_on);
+    }
+}
+
+// ==================================================================== finalize
+// finalize_correction (:1383-1408)
+__global__ void k_finalize(DevParams P, const DevState* __restrict__ S, Sets X, float dt, int do_sph, int do_dem)
+{
+    const uint32_t ls = do_sph ? launch_limit(P, S->n0_sph, S->n_sph) : 0u;
+    const uint32_t ld = do_dem ? launch_limit(P, S->n0_dem, S->n_dem) : 0u;
+    GRID_LOOP(t, ls + ld) {
+        const bool w = t < ls;
+        const uint32_t i = w ? t : t - ls;
+        const snowb_particle_data& D = w ? X.sph : X.dem;
+        float3 np = ldv3(D.new_positions, i);
+        float3 diff = sub3(np, ldv3(D.positions, i));
+        float3 tv = len3(diff) >= P.min_speed ? div3(diff, dt) : f3(0.f, 0.f, 0.f);
+        st3(D.velocity, i, tv);
+        st3(D.positions, i, np);
+    }
+}
+
+// ======================================================================== heat
+// heat_transfer_cell (:3764-3810) over one cell
+__device__ __forceinline__ float heat_cell(const DevParams& P, const SetView& v, const snowb_particle_data& O,
+                                           int3 g, int ox, int oy, int oz, uint32_t skip, float3 p, float Ti,
+                                           float kk)
+{
+    float res = 0.f;
+    uint32_t s, e;
+    if (v.range(P, g, ox, oy, oz, s, e))
+        for (uint32_t j = s; j < e; ++j) {
+            if (j == skip) continue;
+            float3 dv = sub3(p, v.pos(j));
+            float d2 = dot3(dv, dv);
+            if (d2 < P.h2_lt) {
+                const uint32_t oj = v.gi[j];
+                res += (((O.mass[oj] / O.density[oj]) * kk) * (O.T[oj] - Ti)) * L_visc(P, sqrtf(d2));
+            }
+        }
+    return res;
+}
+__device__ __forceinline__ float heat_sum(const DevParams& P, float dT, const SetView& v, const snowb_particle_data& O,
+                                          int3 g, uint32_t skip, float3 p, float Ti, float kk)
+{
+    if (P.quirks == SNOWB_QUIRKS_REFERENCE) {
+        // Q7: the reference passes the particle's own cell to all 27 calls
+        const float s = heat_cell(P, v, O, g, 0, 0, 0, skip, p, Ti, kk);
+        for (int k = 0; k < 27; ++k) dT += s;
+        return dT;
+    }
+    FOR27 dT += heat_cell(P, v, O, g, ox, oy, oz, skip, p, Ti, kk);
+    return dT;
+}
+// transfer_heat_sph / transfer_heat_dem (:3812-3937): new_T from T
+__global__ void __launch_bounds__(128) k_heat(DevParams P, const DevState* __restrict__ S, SetView vs, SetView vd,
+                                              Sets X, float dt)
+{
+    const uint32_t ns = S->n_sph, nd = S->n_dem;
+    vs.n = ns; vd.n = nd;
+    const float kww = ((4.f * P.k_water) * P.k_water) / (P.k_water + P.k_water);
+    const float kss = ((4.f * P.k_snow) * P.k_snow) / (P.k_snow + P.k_snow);
+    const float kws = ((4.f * P.k_water) * P.k_snow) / (P.k_water + P.k_snow);
+    const float ksw = ((4.f * P.k_snow) * P.k_water) / (P.k_snow + P.k_water);
+    GRID_LOOP(t, ns + nd) {
+        const bool w = t < ns;
+        const uint32_t i = w ? t : t - ns;
+        const SetView& own = w ? vs : vd;
+        const SetView& oth = w ? vd : vs;
+        const snowb_particle_data& A = w ? X.sph : X.dem;
+        const snowb_particle_data& B = w ? X.dem : X.sph;
+        const uint32_t o = own.gi[i];
+        float3 p = xyz(own.p4[i]); int3 g = grid_pos(P, p);
+        const float Ti = A.T[o];
+        float dT = 0.f;
+        dT = heat_sum(P, dT, own, A, g, i, p, Ti, w ? kww : kss);
+        dT = heat_sum(P, dT, oth, B, g, SNOWB_UMAX, p, Ti, w ? kws : ksw);
+        dT = dT / ((w ? P.C_water : P.C_snow) * A.density[o]);
+        A.new_T[o] = Ti + dT * dt;
+    }
+}
+// thrust::copy new_T -> T (:3968-3969) then environmental_heat_transfer (:4847-4859)
+__global__ void k_heat_commit(const DevState* __restrict__ S, Sets X, float dTe, int env_sph, int env_dem)
+{
+    const uint32_t ns = S->n_sph, nd = S->n_dem;
+    GRID_LOOP(t, ns + nd) {
+        const bool w = t < ns;
+        const uint32_t i = w ? t : t - ns;
+        const snowb_particle_data& D = w ? X.sph : X.dem;
+        float T = D.new_T[i];
+        if (w ? env_sph : env_dem) T += dTe;
+        D.T[i] = T;
+    }
+}
+
+// ======================================================================== XSPH
+// xsph_viscosity_cell{,_coupling} (:3419-3502): sum of (m_j/rho_j) (v_j - v_i) W
+__device__ __forceinline__ float3 acc_xsph(const DevParams& P, float3 acc, const SetView& v,
+                                           const snowb_particle_data& O, const snowb_float3* vel, float3 p,
+                                           int3 g, uint32_t skip, float3 vi)
+{
+    FOR27 {
+        float3 cs = f3(0.f, 0.f, 0.f);
+        uint32_t s, e;
+        if (v.range(P, g, ox, oy, oz, s, e))
+            for (uint32_t j = s; j < e; ++j) {
+                if (j == skip) continue;
+                float3 dv = sub3(p, v.pos(j));
+                float d2 = dot3(dv, dv);
+                if (d2 < P.h2_lt) {
+                    const uint32_t oj = v.gi[j];
+                    float3 vij = sub3(ldv3(vel, oj), vi);
+                    float a = O.mass[oj] / O.density[oj];
+                    float wgt = W_poly6(P, sqrtf(d2));
+                    cs = add3(cs, f3((a * vij.x) * wgt, (a * vij.y) * wgt, (a * vij.z) * wgt));
+                }
+            }
+        acc = add3(acc, cs);
+    }
+    return acc;
+}
+// xsph_sph_viscosity / xsph_dem_viscosity (:3504-3660), Jacobi: results go to out_vel.
+// `limit` is the number of sorted particles processed (Q6 for the snow set).
+__global__ void __launch_bounds__(128) k_xsph(DevParams P, const DevState* __restrict__ S, SetView vown, SetView voth,
+                                              snowb_particle_data A, snowb_particle_data B, int own_is_sph,
+                                              float visc, snowb_float3* __restrict__ out_vel)
+{
+    const uint32_t ns = S->n_sph, nd = S->n_dem;
+    vown.n = own_is_sph ? ns : nd;
+    voth.n = own_is_sph ? nd : ns;
+    const uint32_t limit = own_is_sph ? ns
+                         : (P.quirks == SNOWB_QUIRKS_REFERENCE ? umin32(coverage(ns), nd) : nd);
+    GRID_LOOP(i, limit) {
+        const uint32_t o = vown.gi[i];
+        float3 p = xyz(vown.p4[i]); int3 g = grid_pos(P, p);
+        float3 vi = ldv3(A.velocity, o);
+        float3 c = f3(0.f, 0.f, 0.f);
+        c = acc_xsph(P, c, vown, A, A.velocity, p, g, i, vi);
+        c = acc_xsph(P, c, voth, B, B.velocity, p, g, SNOWB_UMAX, vi);
+        c = sc3(visc, c);
+        st3(out_vel, o, add3(vi, c));
+    }
+}
+// write the Jacobi results back (only the processed particles)
+__global__ void k_xsph_commit(DevParams P, const DevState* __restrict__ S, SetView vown, int own_is_sph,
+                              const snowb_float3* __restrict__ in_vel, snowb_float3* __restrict__ vel)
+{
+    const uint32_t ns = S->n_sph, nd = S->n_dem;
+    const uint32_t limit = own_is_sph ? ns
+                         : (P.quirks == SNOWB_QUIRKS_REFERENCE ? umin32(coverage(ns), nd) : nd);
+    GRID_LOOP(i, limit) {
+        const uint32_t o = vown.gi[i];
+        st3(vel, o, ldv3(in_vel, o));
+    }
+}
+
+// ===================================================================== misc
+// compute_boundary_volume_d (:303-346) with sph_boundary_volume (:159-192); reads the
+// caller's sorted positions directly (one-time setup).
+__global__ void k_boundary_volume(DevParams P, snowb_cell_data cd, const float* __restrict__ mass,
+                                  float* __restrict__ volume, uint32_t n)
+{
+    GRID_LOOP(i, n) {
+        const uint32_t o = cd.grid_index[i];
+        float3 p = ldv3(cd.sorted_pos, i);
+        float rho = mass[o] * P.W0;
+        int3 g = grid_pos(P, p);
+        FOR27 {
+            float cs = 0.f;
+            uint32_t h = grid_hash(P, g, ox, oy, oz);
+            uint32_t s = cd.cell_start[h];
+            if (s != SNOWB_EMPTY) {
+                uint32_t e = cd.cell_end[h];
+                for (uint32_t j = s; j < e; ++j) {
+                    if (j == i) continue;
+                    float3 dv = sub3(p, ldv3(cd.sorted_pos, j));
+                    float d2 = dot3(dv, dv);
+                    if (d2 < P.h2_lt) cs += mass[cd.grid_index[j]] * W_poly6(P, sqrtf(d2));
+                }
+            }
+            rho += cs;
+        }
+        volume[o] = mass[o] / rho;
+    }
+}
+// compact sorted view of the boundary set: p4 = (pos, volume), invm/mass by sorted index
+__global__ void k_boundary_prep(snowb_cell_data cd, const float* __restrict__ volume, const float* __restrict__ invm,
+                                const float* __restrict__ mass, uint32_t n, float4* __restrict__ p4,
+                                float* __restrict__ invm_s, float* __restrict__ mass_s)
+{
+    GRID_LOOP(i, n) {
+        const uint32_t o = cd.grid_index[i];
+        float3 q = ldv3(cd.sorted_pos, i);
+        p4[i] = make_float4(q.x, q.y, q.z, volume[o]);
+        invm_s[i] = invm[o];
+        mass_s[i] = mass[o];
+    }
+}
+__global__ void k_set_state(DevState* S, uint32_t ns, uint32_t nd, uint32_t nb)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        S->n_sph = ns; S->n_dem = nd; S->n_b = nb;
+        S->n0_sph = ns; S->n0_dem = nd;
+        S->n_freeze = 0; S->n_melt = 0; S->changed = 0; S->new_sph = ns; S->new_dem = nd;
+    }
+}
+__global__ void k_begin_substep(DevState* S)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        S->n0_sph = S->n_sph; S->n0_dem = S->n_dem;
+        S->n_freeze = 0; S->n_melt = 0; S->changed = 0;
+    }
+}
+
+// FP64 heat-energy and momentum partial sums (deterministic two-level reduction)
+__global__ void k_energy_partial(const snowb_particle_data sph, uint32_t ns, const snowb_particle_data dem,
+                                 uint32_t nd, double Cw, double Cs, double* __restrict__ part)
+{
+    __shared__ double sm[4][256];
+    double a[4] = {0, 0, 0, 0};
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < ns + nd; t += gridDim.x * blockDim.x) {
+        const bool w = t < ns;
+        const uint32_t i = w ? t : t - ns;
+        const snowb_particle_data& D = w ? sph : dem;
+        double m = (double)D.mass[i];
+        float3 v = ldv3(D.velocity, i);
+        a[0] += m * (w ? Cw : Cs) * (double)D.T[i];
+        a[1] += m * (double)v.x; a[2] += m * (double)v.y; a[3] += m * (double)v.z;
+    }
+    for (int k = 0; k < 4; ++k) sm[k][threadIdx.x] = a[k];
+    __syncthreads();
+    for (int st = 128; st > 0; st >>= 1) {
+        if ((int)threadIdx.x < st)
+            for (int k = 0; k < 4; ++k) sm[k][threadIdx.x] += sm[k][threadIdx.x + st];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 4; ++k) part[4 * blockIdx.x + k] = sm[k][0];
+}
+__global__ void k_energy_final(const double* __restrict__ part, int nblocks, double* __restrict__ out)
+{
+    if (threadIdx.x < 4) {
+        double s = 0;
+        for (int b = 0; b < nblocks; ++b) s += part[4 * b + threadIdx.x];
+        out[threadIdx.x] = s;
+    }
+}
+
+}  // namespace snowb
