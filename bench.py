@@ -1,0 +1,312 @@
+"""Throughput benchmark of the snow/water substep (particle-substeps/s) on B200.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Workload: the README-scale scene (5,888 water + 147,928 snow particles, 52,016 boundary
+particles, seeded synthetic lattice), one step = one frame = 4 substeps of dt = 1/240 s
+with 3 solver iterations.  `value` is timed on the device with CUDA events around each
+frame (state resident in HBM, L2 flushed between frames); `e2e` goes through the C-ABI
+call with the per-frame host I/O of the reference (positions, velocities and temperatures
+of both sets copied from pinned host memory before the frame and back after it, the
+buffers the reference maps from GL each frame).  Multi-GPU runs are independent replicas
+(one scene per rank, no collective in the step); `value` is the sum over ranks divided by
+the slowest rank's time.
+
+--impl reference times the CPU restatement of the same substep (FP32, all host threads,
+one substep per step), the only CPU implementation of this path: the reference itself
+runs it only on a GPU.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-substeps/s @154k particles (config 1)"
+UNIT = "particle-substeps/s"
+SUBSTEPS = 4
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scene", default="config1")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-out", default="")
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# ----------------------------------------------------------------- clocks sampling
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                                       "-lms", "200", "-i", str(dev)], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        for line in open(self.f.name):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            j = json.load(f)
+        return float(j["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+# ----------------------------------------------------------------- CPU baseline
+def cpu_baseline(scene_name, max_seconds=25.0, max_substeps=None):
+    """FP32 oracle (project CPU restatement) on the same scene, all host threads."""
+    from snowsimulation_b200 import scene
+    from oracle.oracle import OracleWorld
+    w = getattr(scene, scene_name)()
+    cores = os.cpu_count() or 1
+    o = OracleWorld(w, 32, threads=cores).setup()
+    n = w.n_sph + w.n_dem
+    done, t0 = 0, time.perf_counter()
+    while True:
+        o.step()
+        done += 1
+        el = time.perf_counter() - t0
+        if el > max_seconds * 0.5 or (max_substeps and done >= max_substeps):
+            break
+    return {"value": n * done / el, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": "%d substep(s) of %s (%d particles), FP32 C oracle, OpenMP %d threads, %.1f s"
+                      % (done, scene_name, n, cores, el)}
+
+
+# ----------------------------------------------------------------- reference arm
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    from snowsimulation_b200 import scene
+    from oracle.oracle import OracleWorld
+    w = getattr(scene, args.scene)()
+    cores = os.cpu_count() or 1
+    o = OracleWorld(w, 32, threads=cores).setup()
+    n = w.n_sph + w.n_dem
+    warm = max(1, min(args.warmup, 1))
+    for _ in range(warm):
+        o.step()
+    budget = 150.0
+    t0 = time.perf_counter()
+    done = 0
+    while done < args.steps:
+        o.step()
+        done += 1
+        if time.perf_counter() - t0 > budget:
+            break
+    el = time.perf_counter() - t0
+    val = n * done / el
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": done, "warmup": warm, "ms_per_step": 1000.0 * el / done, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.scene + " (5888 water + 147928 snow + 52016 boundary), one substep per step",
+                       "substeps_per_step": 1, "iterations": 3, "l2": "n/a (CPU)"},
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": "%d substep(s), FP32 C restatement of the substep (oracle/), "
+                                       "OpenMP %d threads; the reference runs this path only on a GPU"
+                                       % (done, cores)},
+            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ----------------------------------------------------------------- our arm
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    import torch.distributed as dist
+    from snowsimulation_b200 import scene, bytes_model, _native
+    from snowsimulation_b200.world import Simulation
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    w = getattr(scene, args.scene)(seed=rank)
+    sim = Simulation(w, device=dev).setup()
+    lib = sim.lib
+    n_part = w.n_sph + w.n_dem
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)   # > 126 MB L2
+
+    def frame(sync=False):
+        sim.step(substeps=SUBSTEPS, sync=sync)
+
+    for _ in range(max(3, args.warmup)):
+        frame()
+    torch.cuda.synchronize(dev)
+
+    # ---- device-timed frames (inputs resident; L2 flushed between frames, outside the events)
+    clocks = Clocks(local)
+    cnt0 = C.c_uint64(0)
+    lib.snowb_launch_count(C.byref(cnt0))
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.zero_()
+        evs[k][0].record(stream)
+        frame()
+        evs[k][1].record(stream)
+    torch.cuda.synchronize(dev)
+    cnt1 = C.c_uint64(0)
+    lib.snowb_launch_count(C.byref(cnt1))
+    clk = clocks.stop()
+    ms = [a.elapsed_time(b) for a, b in evs]
+    tot_ms = sum(ms)
+    sim.read_sizes()
+    if ws > 1:
+        t = torch.tensor([tot_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tot_ms = float(t.item())
+    value = ws * n_part * SUBSTEPS * args.steps / (tot_ms / 1000.0)
+    ms_per_step = tot_ms / args.steps
+
+    # ---- end to end through the C-ABI call with host buffers
+    fields = ("positions", "velocity", "T")
+    host = {(s, f): torch.empty_like(getattr(sim, s).t[f], device="cpu").pin_memory()
+            for s in ("sph", "dem") for f in fields}
+    for (s, f), hb in host.items():
+        hb.copy_(getattr(sim, s).t[f])
+    h2d = sum(hb.numel() * hb.element_size() for hb in host.values())
+    d2h = h2d
+    e_ms = []
+    if ws > 1:
+        dist.barrier()
+    for k in range(args.steps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for (s, f), hb in host.items():
+            getattr(sim, s).t[f].copy_(hb, non_blocking=True)
+        frame(sync=True)                       # the reference contract: sizes back on the host
+        for (s, f), hb in host.items():
+            hb.copy_(getattr(sim, s).t[f], non_blocking=True)
+        b.record(stream)
+        b.synchronize()
+        e_ms.append(a.elapsed_time(b))
+    e_tot = sum(e_ms)
+    if ws > 1:
+        t = torch.tensor([e_tot], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e_tot = float(t.item())
+    e2e = ws * n_part * SUBSTEPS * args.steps / (e_tot / 1000.0)
+
+    # ---- per-kernel device time (CUDA events on the library's stream), 2 frames
+    lib.snowb_profile_begin()
+    for _ in range(2):
+        frame()
+    buf = C.create_string_buffer(1 << 16)
+    _native.check(lib.snowb_profile_end(buf, len(buf)))
+    prof = {}
+    for line in buf.value.decode().splitlines():
+        nm, c, t = line.split()
+        prof[nm] = (int(c), float(t))
+    if args.profile_out and rank == 0:
+        with open(args.profile_out, "w") as f:
+            tot = sum(t for _, t in prof.values())
+            for nm, (c, t) in sorted(prof.items(), key=lambda x: -x[1][1]):
+                f.write("%-22s launches %5d  total %9.3f ms  share %5.1f%%\n" % (nm, c, t, 100 * t / tot))
+    modeled = {nm: v for nm, v in prof.items()
+               if bytes_model.kernel_bytes(nm, sim.n_sph, sim.n_dem, sim.n_b) is not None}
+    top = max(modeled, key=lambda nm: modeled[nm][1])
+    c, t = modeled[top]
+    per_launch_s = t / c / 1000.0
+    kb = bytes_model.kernel_bytes(top, sim.n_sph, sim.n_dem, sim.n_b)
+    peak, peak_kind = peaks()
+    achieved = kb / per_launch_s / 1e9
+    sub_bytes = bytes_model.substep_bytes(sim.n_sph, sim.n_dem, sim.n_b, w.iterations)
+    sub_gbs = sub_bytes * SUBSTEPS / (ms_per_step / 1000.0) / 1e9
+
+    if rank != 0:
+        if ws > 1:
+            dist.destroy_process_group()
+        return 0
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "%s: %d water + %d snow + %d boundary particles, 1 step = 1 frame = %d substeps "
+                               "(dt 1/240 s, 3 iterations), seeded lattice" % (args.scene, w.n_sph, w.n_dem,
+                                                                               w.n_b, SUBSTEPS),
+                   "substeps_per_step": SUBSTEPS, "iterations": w.iterations,
+                   "quirks": "reference", "parallelism": "replicas" if ws > 1 else "single",
+                   "l2": "flushed between timed steps (256 MB write)"},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_per_step": e_tot / args.steps},
+        "gpu_launches": int(cnt1.value - cnt0.value),
+        "clocks": clk,
+        "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                     "algorithmic_bytes_per_launch": kb, "avg_launch_ms": per_launch_s * 1000.0,
+                     "launches_per_step": c / 2},
+        "substep_roofline": {"algorithmic_bytes": sub_bytes, "achieved_GBs": sub_gbs,
+                             "frac": sub_gbs / peak},
+        "kernel_ms_per_step": {nm: t / 2 for nm, (c, t) in sorted(prof.items(), key=lambda x: -x[1][1])},
+    }
+    if ws == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args.scene)
+    print(json.dumps(line))
+    if ws > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -189,6 +189,15 @@ int snowb_synchronize(void);
 int snowb_energy_momentum(const snowb_particle_data* sph, uint32_t sph_size,
                           const snowb_particle_data* dem, uint32_t dem_size, double out[4]);
 
+/* Number of kernels this library has launched since it was loaded. */
+int snowb_launch_count(uint64_t* count);
+
+/* Per-kernel timing: between snowb_profile_begin and snowb_profile_end every launch is
+ * bracketed by CUDA events on the library's stream; snowb_profile_end waits for the stream
+ * and writes one line per kernel, "name launches total_ms", into out (NUL-terminated). */
+int snowb_profile_begin(void);
+int snowb_profile_end(char* out, size_t cap);
+
 /* Release the library's internal device buffers (they are re-created on demand). */
 int snowb_release(void);
 

@@ -23,7 +23,8 @@ EXPORTS = (
     "snowb_sort_particles", "snowb_reorder_data", "snowb_compute_boundary_volume", "snowb_integrate_pbd",
     "snowb_connect_and_record", "snowb_snow_simulation", "snowb_snow_simulation_ex", "snowb_read_sizes",
     "snowb_set_quirks", "snowb_set_stream", "snowb_synchronize", "snowb_energy_momentum", "snowb_release",
-    "snowb_last_error", "snowb_last_error_string",
+    "snowb_last_error", "snowb_last_error_string", "snowb_launch_count", "snowb_profile_begin",
+    "snowb_profile_end",
 )
 
 _lib = None
@@ -62,6 +63,9 @@ def load(path=LIB_PATH):
         "snowb_energy_momentum": [PPD, u32, PPD, u32, C.POINTER(C.c_double)],
         "snowb_release": [],
         "snowb_last_error": [],
+        "snowb_launch_count": [C.POINTER(C.c_uint64)],
+        "snowb_profile_begin": [],
+        "snowb_profile_end": [C.c_char_p, C.c_size_t],
     }
     sig["snowb_snow_simulation_ex"] = sig["snowb_snow_simulation"] + [C.POINTER(StepOptions)]
     for name, args in sig.items():

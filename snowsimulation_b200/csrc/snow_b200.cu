@@ -206,6 +206,37 @@ static int ensure_gen(uint32_t n, uint32_t ncells)
 }
 
 // ------------------------------------------------------------------ launch helpers
+// Every kernel launch goes through KL: it counts launches and, while profiling is on,
+// brackets the launch with CUDA events on the library's stream.
+struct ProfRec {
+    const char* name;
+    cudaEvent_t a, b;
+};
+static bool g_prof = false;
+static uint64_t g_launches = 0;
+static std::vector<ProfRec> g_prof_pool;
+static size_t g_prof_used = 0;
+
+static void prof_begin(const char* name)
+{
+    ++g_launches;
+    if (!g_prof) return;
+    if (g_prof_used == g_prof_pool.size()) {
+        ProfRec r{name, nullptr, nullptr};
+        cudaEventCreate(&r.a);
+        cudaEventCreate(&r.b);
+        g_prof_pool.push_back(r);
+    }
+    g_prof_pool[g_prof_used].name = name;
+    cudaEventRecord(g_prof_pool[g_prof_used].a, g_stream);
+}
+static void prof_end()
+{
+    if (!g_prof) return;
+    cudaEventRecord(g_prof_pool[g_prof_used].b, g_stream);
+    ++g_prof_used;
+}
+
 static inline unsigned blocks_for(uint64_t work, int tpb)
 {
     uint64_t b = (work + tpb - 1) / tpb;
@@ -213,14 +244,17 @@ static inline unsigned blocks_for(uint64_t work, int tpb)
     if (b > (uint64_t)g_max_blocks) b = g_max_blocks;
     return (unsigned)b;
 }
-#define LAUNCH(kernel, work, tpb, ...)                                                     \
+#define KL(kernel, grid, tpb, ...)                                                         \
     do {                                                                                   \
-        kernel<<<blocks_for((work), (tpb)), (tpb), 0, g_stream>>>(__VA_ARGS__);            \
+        prof_begin(#kernel);                                                               \
+        kernel<<<(grid), (tpb), 0, g_stream>>>(__VA_ARGS__);                               \
+        prof_end();                                                                        \
         cudaError_t _e = cudaGetLastError();                                               \
         if (_e != cudaSuccess)                                                             \
             return fail(SNOWB_ERR_CUDA, std::string(#kernel) + ": " + cudaGetErrorString(_e)); \
     } while (0)
-#define LAUNCH1(kernel, ...) LAUNCH(kernel, 1, 32, __VA_ARGS__)
+#define LAUNCH(kernel, work, tpb, ...) KL(kernel, blocks_for((work), (tpb)), (tpb), __VA_ARGS__)
+#define LAUNCH1(kernel, ...) KL(kernel, 1, 32, __VA_ARGS__)
 
 static inline unsigned scan_blocks(uint32_t n) { return (n + SCAN_CHUNK - 1) / SCAN_CHUNK + (n == 0); }
 
@@ -229,9 +263,8 @@ static int scan(const uint32_t* in, const uint32_t* n_ptr, uint32_t n_fixed, uin
                 uint32_t* out, uint32_t* total, const uint32_t* cond)
 {
     const uint32_t nb = scan_blocks(n_ptr ? cap : n_fixed);
-    k_scan_sums<<<nb, SCAN_TPB, 0, g_stream>>>(in, n_ptr, n_fixed, bsum, cond);
-    k_scan_apply<<<nb, SCAN_TPB, 0, g_stream>>>(in, n_ptr, n_fixed, bsum, out, total, cond);
-    CUDA_TRY(cudaGetLastError());
+    KL(k_scan_sums, nb, SCAN_TPB, in, n_ptr, n_fixed, bsum, cond);
+    KL(k_scan_apply, nb, SCAN_TPB, in, n_ptr, n_fixed, bsum, out, total, cond);
     return SNOWB_OK;
 }
 
@@ -243,10 +276,8 @@ static int sort_set(const DevParams& P, SetBufs& B, const snowb_particle_data& D
     const uint32_t nc = P.ncells;
     LAUNCH(k_hash_count, cap, 256, P, D.predict_positions, n_ptr, 0u, B.key, B.slot, B.cnt, cond);
     const unsigned nb = (nc + SCAN_CHUNK - 1) / SCAN_CHUNK;
-    k_block_sums<<<nb, SCAN_TPB, 0, g_stream>>>(B.cnt, nc, B.bsum, cond);
-    k_cell_scan<<<nb, SCAN_TPB, 0, g_stream>>>(B.cnt, B.bsum, nc, B.off, cd.cell_start, n_ptr, 0u, clear_all ? 1 : 0,
-                                               cond);
-    CUDA_TRY(cudaGetLastError());
+    KL(k_block_sums, nb, SCAN_TPB, B.cnt, nc, B.bsum, cond);
+    KL(k_cell_scan, nb, SCAN_TPB, B.cnt, B.bsum, nc, B.off, cd.cell_start, n_ptr, 0u, clear_all ? 1 : 0, cond);
     LAUNCH(k_scatter, cap, 256, B.key, B.slot, B.off, B.tmp, n_ptr, 0u, cond);
     LAUNCH(k_rank_reorder, cap, 256, B.key, B.off, B.tmp, D.predict_positions, D.mass, D.massInv, D.contrib, cd, B.p4,
            B.invm, B.contrib, n_ptr, 0u, cond);
@@ -507,10 +538,9 @@ int snowb_sort_particles(snowb_cell_data cd, uint32_t n)
     CUDA_TRY(cudaMemsetAsync(g_ctx.err_dev, 0, sizeof(uint32_t), g_stream));
     LAUNCH(k_key_count, n, 256, cd.grid_hash, cd.grid_index, n, nc, B.key, B.val, B.slot, B.cnt, g_ctx.err_dev);
     const unsigned nb = (nc + SCAN_CHUNK - 1) / SCAN_CHUNK;
-    k_block_sums<<<nb, SCAN_TPB, 0, g_stream>>>(B.cnt, nc, B.bsum, nullptr);
+    KL(k_block_sums, nb, SCAN_TPB, B.cnt, nc, B.bsum, nullptr);
     // cell_start is not touched by a plain sort: clear nothing (clear_all = 0, n = 0)
-    k_cell_scan<<<nb, SCAN_TPB, 0, g_stream>>>(B.cnt, B.bsum, nc, B.off, nullptr, nullptr, 0u, 0, nullptr);
-    CUDA_TRY(cudaGetLastError());
+    KL(k_cell_scan, nb, SCAN_TPB, B.cnt, B.bsum, nc, B.off, nullptr, nullptr, 0u, 0, nullptr);
     LAUNCH(k_scatter, n, 256, B.key, B.slot, B.off, B.tmp, nullptr, n, nullptr);
     LAUNCH(k_rank_pairs, n, 256, B.key, B.val, B.off, B.tmp, cd.grid_hash, cd.grid_index, n);
     uint32_t err = 0;
@@ -661,12 +691,54 @@ int snowb_energy_momentum(const snowb_particle_data* sph, uint32_t ns, const sno
     if (!sph || !dem || !out) return fail(SNOWB_ERR_INVALID, "null pointer");
     TRY(ensure_ctx(g_ctx.cap ? g_ctx.cap : 1, g_ctx.bcap ? g_ctx.bcap : 1, g_P.ncells));
     const int nb = 512;
-    k_energy_partial<<<nb, 256, 0, g_stream>>>(*sph, ns, *dem, nd, (double)g_sim.C_water, (double)g_sim.C_snow,
-                                               g_ctx.epart);
-    k_energy_final<<<1, 32, 0, g_stream>>>(g_ctx.epart, nb, g_ctx.eout);
-    CUDA_TRY(cudaGetLastError());
+    KL(k_energy_partial, nb, 256, *sph, ns, *dem, nd, (double)g_sim.C_water, (double)g_sim.C_snow, g_ctx.epart);
+    KL(k_energy_final, 1, 32, g_ctx.epart, nb, g_ctx.eout);
     CUDA_TRY(cudaMemcpyAsync(out, g_ctx.eout, 4 * sizeof(double), cudaMemcpyDeviceToHost, g_stream));
     CUDA_TRY(cudaStreamSynchronize(g_stream));
+    return SNOWB_OK;
+}
+
+int snowb_launch_count(uint64_t* count)
+{
+    if (!count) return fail(SNOWB_ERR_INVALID, "null pointer");
+    *count = g_launches;
+    return SNOWB_OK;
+}
+
+int snowb_profile_begin(void)
+{
+    g_prof = true;
+    g_prof_used = 0;
+    return SNOWB_OK;
+}
+
+int snowb_profile_end(char* out, size_t cap)
+{
+    CUDA_TRY(cudaStreamSynchronize(g_stream));
+    std::vector<std::string> names;
+    std::vector<double> total;
+    std::vector<uint64_t> count;
+    for (size_t k = 0; k < g_prof_used; ++k) {
+        float ms = 0.f;
+        CUDA_TRY(cudaEventElapsedTime(&ms, g_prof_pool[k].a, g_prof_pool[k].b));
+        const std::string nm = g_prof_pool[k].name;
+        size_t idx = 0;
+        while (idx < names.size() && names[idx] != nm) ++idx;
+        if (idx == names.size()) { names.push_back(nm); total.push_back(0.0); count.push_back(0); }
+        total[idx] += ms;
+        count[idx] += 1;
+    }
+    g_prof = false;
+    g_prof_used = 0;
+    std::string txt;
+    for (size_t i = 0; i < names.size(); ++i)
+        txt += names[i] + " " + std::to_string(count[i]) + " " + std::to_string(total[i]) + "\n";
+    if (out && cap) {
+        size_t n = txt.size() < cap - 1 ? txt.size() : cap - 1;
+        std::memcpy(out, txt.data(), n);
+        out[n] = 0;
+        if (txt.size() >= cap) return fail(SNOWB_ERR_INVALID, "profile buffer too small");
+    }
     return SNOWB_OK;
 }
 

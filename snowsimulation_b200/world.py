@@ -64,9 +64,12 @@ class Simulation:
 
     def __init__(self, world: HostWorld, device="cuda", quirks=QUIRKS_REFERENCE):
         self.lib = _native.load()
-        self.device = torch.device(device)
-        if self.device.type != "cuda":
+        dev = torch.device(device)
+        if dev.type != "cuda":
             raise _native.SnowError("the solver runs on a CUDA device only")
+        if dev.index is None:
+            dev = torch.device("cuda", torch.cuda.current_device())
+        self.device = dev
         torch.cuda.set_device(self.device)
         self.w = world
         self.quirks = quirks
