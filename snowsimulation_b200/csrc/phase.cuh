@@ -193,7 +193,18 @@ __device__ __forceinline__ uint32_t link_tolerance(const DevParams& P, float T, 
     uint32_t tol = dynamic ? __float2uint_rz(((T - P.Tf) / (P.Th - P.Tf)) * (float)P.maxc) : P.maxc;
     return tol < P.maxc ? tol : P.maxc;
 }
-// prefilter: can particle (sorted) i add any link in this pass?
+// Prefilter: can particle (sorted) i change any record in this pass?  During the pass
+// links are only added and counts only grow, so i is a no-op if its count already reaches
+// its cap, if it has no free slot, or if every candidate (d < h) is either linked to it
+// already or has no room (count at the cap or no free slot): an attempt on a full
+// partner claims a slot of i and releases it again.  A candidate that is i itself (a
+// stale cell range can hold it) keeps i active.
+__device__ __forceinline__ bool has_free_slot(const uint32_t* rec, uint32_t o, uint32_t M)
+{
+    for (uint32_t q = M * o; q < M * (o + 1); ++q)
+        if (rec[q] == SNOWB_UMAX) return true;
+    return false;
+}
 __global__ void __launch_bounds__(128) k_link_filter(DevParams P, const DevState* __restrict__ S, SetView vd,
                                                      snowb_particle_data dem, int dynamic,
                                                      uint8_t* __restrict__ active)
@@ -205,7 +216,7 @@ __global__ void __launch_bounds__(128) k_link_filter(DevParams P, const DevState
         const float3 p = vd.pos(i);
         const uint32_t count = dem.iter_end[o] - o * M;
         uint8_t act = 0;
-        if (count < link_tolerance(P, dem.T[o], dynamic)) {
+        if (count < link_tolerance(P, dem.T[o], dynamic) && has_free_slot(dem.connect_record, o, M)) {
             const int3 g = grid_pos(P, p);
             FOR27 {
                 uint32_t s, e;
@@ -215,10 +226,12 @@ __global__ void __launch_bounds__(128) k_link_filter(DevParams P, const DevState
                     float3 dv = sub3(p, vd.pos(j));
                     if (dot3(dv, dv) < P.h2_lt) {
                         const uint32_t o1 = vd.gi[j];
+                        if (o1 == o) { act = 1; break; }
                         bool found = false;
                         for (uint32_t q = M * o; q < M * (o + 1); ++q)
                             if (dem.connect_record[q] == o1) { found = true; break; }
-                        if (!found) act = 1;
+                        if (found) continue;
+                        if (dem.iter_end[o1] < (o1 + 1) * M && has_free_slot(dem.connect_record, o1, M)) act = 1;
                     }
                 }
                 if (act) break;

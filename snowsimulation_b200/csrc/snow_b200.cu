@@ -338,7 +338,7 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
     TRY(sort_if(1, nullptr));
     TRY(sort_if(0, nullptr));
     STOP(1);
-    LAUNCH(k_density, work3, 128, P, S, vs, vd, vb, X);
+    LAUNCH(k_density<false>, work3, 128, P, S, vs, vd, vb, X, ss, sd, sb);
     STOP(2);
     if (a.temperature) {
         LAUNCH(k_heat, 2 * full, 128, P, S, vs, vd, X, a.dt);
@@ -391,9 +391,8 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
         TRY(sort_if(1, nullptr));
         TRY(sort_if(0, nullptr));
         STOP(base + 0);
-        LAUNCH(k_density, work3, 128, P, S, vs, vd, vb, X);
-        STOP(base + 1);
-        LAUNCH(k_lambda, work3, 128, P, S, vs, vd, vb, X, ss, sd, sb);
+        // density + lambda in one pass (stage boundaries base+1 and base+2 coincide)
+        LAUNCH(k_density<true>, work3, 128, P, S, vs, vd, vb, X, ss, sd, sb);
         STOP(base + 2);
         LAUNCH(k_pbf, 2 * full, 128, P, S, vs, vd, vb, X, ss, sd, sb, a.dt, F);
         STOP(base + 3);

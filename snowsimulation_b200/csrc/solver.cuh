@@ -24,58 +24,6 @@ struct Sorted {
 };
 
 // ------------------------------------------------------------ per-cell neighbour sums
-// sum of w_j * W(d): w = mass (fluid/snow view) or rho0*V (boundary view, vol=true)
-__device__ __forceinline__ float acc_W(const DevParams& P, float acc, const SetView& v, float3 p, int3 g,
-                                       uint32_t skip, bool vol)
-{
-    FOR27 {
-        float cs = 0.f;
-        uint32_t s, e;
-        if (v.range(P, g, ox, oy, oz, s, e))
-            for (uint32_t j = s; j < e; ++j) {
-                if (j == skip) continue;
-                float4 q = v.pw(j);
-                float3 dv = sub3(p, xyz(q));
-                float d2 = dot3(dv, dv);
-                if (d2 < P.h2_lt) {
-                    float w = vol ? P.rho0 * q.w : q.w;
-                    cs += w * W_poly6(P, sqrtf(d2));
-                }
-            }
-        acc += cs;
-    }
-    return acc;
-}
-// lambda denominator; mode 0: 1/rho0, 1: (1/rho0)*((rho0*V_j)/m_self), 2: ... / m_j
-__device__ __forceinline__ float acc_gradsq(const DevParams& P, float acc, const SetView& v, float3 p, int3 g,
-                                            uint32_t skip, int mode, float m_self, const float* mass_s,
-                                            const float* mass_o)
-{
-    FOR27 {
-        float cs = 0.f;
-        uint32_t s, e;
-        if (v.range(P, g, ox, oy, oz, s, e))
-            for (uint32_t j = s; j < e; ++j) {
-                if (j == skip) continue;
-                float4 q = v.pw(j);
-                float3 dv = sub3(p, xyz(q));
-                float d2 = dot3(dv, dv);
-                if (d2 < P.h2_lt) {
-                    float d = sqrtf(d2);
-                    float sc;
-                    if (mode == 0) sc = P.inv_rho0;
-                    else {
-                        float m = mode == 1 ? m_self : v.attr(mass_s, mass_o, j);
-                        sc = P.inv_rho0 * ((P.rho0 * q.w) / m);
-                    }
-                    float3 gc = sc3(sc, G_spiky(P, dv, d));
-                    cs += dot3(gc, gc);
-                }
-            }
-        acc += cs;
-    }
-    return acc;
-}
 // pbf_correction (:883-929)
 __device__ __forceinline__ float3 acc_pbf_own(const DevParams& P, float3 acc, const SetView& v, float3 p, int3 g,
                                               uint32_t skip, float li, const float* lam_s, const float* lam_o,
@@ -188,86 +136,97 @@ __device__ __forceinline__ float3 acc_contact_sph(const DevParams& P, float3 acc
 }
 
 // ======================================================================== density
-// compute_snow_{sph,dem_sph,boundary}_density_d (:2219-2528), fused over the 3 sets.
-__global__ void __launch_bounds__(128) k_density(DevParams P, const DevState* __restrict__ S, SetView vs, SetView vd,
-                                                 SetView vb, Sets X)
+// Density and W-weighted sums with an optional lambda gradient sum in the same pass.
+// compute_snow_{sph,dem_sph,boundary}_density_d (:2219-2528) and, when LAMBDA is set,
+// compute_snow_{sph,dem_sph,boundary}_lambdas_d (:2598-2898): lambda needs the particle's
+// own C and neighbour positions only, so both come out of one traversal.  Each quantity
+// keeps its own per-cell accumulation in the reference's loop order.
+template <bool LAMBDA>
+__device__ __forceinline__ void acc_WG(const DevParams& P, float& rho, float& gs, const SetView& v, float3 p, int3 g,
+                                       uint32_t skip, bool vol, int mode, float m_self, const float* mass_s,
+                                       const float* mass_o)
 {
-    const uint32_t ns = S->n_sph, nd = S->n_dem, nb = S->n_b;
-    vs.n = ns; vd.n = nd; vb.n = nb;
-    GRID_LOOP(t, ns + nd + nb) {
-        float rho;
-        float* dens; float* Cc; uint32_t o;
-        if (t < ns) {
-            const uint32_t i = t; o = vs.gi[i];
-            float3 p = xyz(vs.p4[i]); int3 g = grid_pos(P, p);
-            rho = X.sph.mass[o] * P.W0;
-            rho = acc_W(P, rho, vs, p, g, i, false);
-            rho = acc_W(P, rho, vd, p, g, SNOWB_UMAX, false);
-            rho = acc_W(P, rho, vb, p, g, SNOWB_UMAX, true);
-            dens = X.sph.density; Cc = X.sph.C;
-        } else if (t < ns + nd) {
-            const uint32_t i = t - ns; o = vd.gi[i];
-            float3 p = xyz(vd.p4[i]); int3 g = grid_pos(P, p);
-            rho = X.dem.mass[o] * P.W0;
-            rho = acc_W(P, rho, vd, p, g, i, false);
-            rho = acc_W(P, rho, vs, p, g, SNOWB_UMAX, false);
-            rho = acc_W(P, rho, vb, p, g, SNOWB_UMAX, true);
-            dens = X.dem.density; Cc = X.dem.C;
-        } else {
-            const uint32_t i = t - ns - nd; o = vb.gi[i];
-            float3 p = xyz(vb.p4[i]); int3 g = grid_pos(P, p);
-            rho = (P.rho0 * X.bnd.volume[o]) * P.W0;
-            rho = acc_W(P, rho, vb, p, g, i, true);
-            rho = acc_W(P, rho, vd, p, g, SNOWB_UMAX, false);
-            rho = acc_W(P, rho, vs, p, g, SNOWB_UMAX, false);
-            dens = X.bnd.density; Cc = X.bnd.C;
-        }
-        dens[o] = rho;
-        float c = (rho / P.rho0) - 1.f;
-        Cc[o] = c > 0.f ? c : 0.f;
+    FOR27 {
+        float cs = 0.f, cg = 0.f;
+        uint32_t s, e;
+        if (v.range(P, g, ox, oy, oz, s, e))
+            for (uint32_t j = s; j < e; ++j) {
+                if (j == skip) continue;
+                float4 q = v.pw(j);
+                float3 dv = sub3(p, xyz(q));
+                float d2 = dot3(dv, dv);
+                if (d2 < P.h2_lt) {
+                    float d = sqrtf(d2);
+                    float w = vol ? P.rho0 * q.w : q.w;
+                    cs += w * W_poly6(P, d);
+                    if (LAMBDA) {
+                        float sc;
+                        if (mode == 0) sc = P.inv_rho0;
+                        else {
+                            float m = mode == 1 ? m_self : v.attr(mass_s, mass_o, j);
+                            sc = P.inv_rho0 * ((P.rho0 * q.w) / m);
+                        }
+                        float3 gc = sc3(sc, G_spiky(P, dv, d));
+                        cg += dot3(gc, gc);
+                    }
+                }
+            }
+        rho += cs;
+        if (LAMBDA) gs += cg;
     }
 }
-
-// ======================================================================== lambda
-// compute_snow_sph_lambdas_d / compute_dem_sph_lambdas_d / compute_snow_boundary_lambdas_d
-// (:2598-2898).  Writes lambda (original order) and its sorted copy.
-__global__ void __launch_bounds__(128) k_lambda(DevParams P, const DevState* __restrict__ S, SetView vs, SetView vd,
-                                                SetView vb, Sets X, Sorted ss, Sorted sd, Sorted sb)
+template <bool LAMBDA>
+__global__ void __launch_bounds__(128) k_density(DevParams P, const DevState* __restrict__ S, SetView vs, SetView vd,
+                                                 SetView vb, Sets X, Sorted ss, Sorted sd, Sorted sb)
 {
     const uint32_t ns = S->n_sph, nd = S->n_dem, nb = S->n_b;
     vs.n = ns; vd.n = nd; vb.n = nb;
     const float3 z = f3(0.f, 0.f, 0.f);
     GRID_LOOP(t, ns + nd + nb) {
+        float rho, gs = dot3(z, z);
+        const snowb_particle_data* D;
+        float* lam_s;
+        uint32_t o, i;
         if (t < ns) {
-            const uint32_t i = t, o = vs.gi[i];
+            i = t; o = vs.gi[i];
             float3 p = xyz(vs.p4[i]); int3 g = grid_pos(P, p);
-            float lam = -X.sph.C[o];
-            float gs = dot3(z, z);
-            gs = acc_gradsq(P, gs, vs, p, g, i, 0, 0.f, nullptr, nullptr);
-            gs = acc_gradsq(P, gs, vd, p, g, SNOWB_UMAX, 0, 0.f, nullptr, nullptr);
-            gs = acc_gradsq(P, gs, vb, p, g, SNOWB_UMAX, 1, X.sph.mass[o], nullptr, nullptr);
-            lam = lam / (gs + P.eps);
-            X.sph.lambda[o] = lam; ss.lambda[i] = lam;
+            rho = X.sph.mass[o] * P.W0;
+            acc_WG<LAMBDA>(P, rho, gs, vs, p, g, i, false, 0, 0.f, nullptr, nullptr);
+            acc_WG<LAMBDA>(P, rho, gs, vd, p, g, SNOWB_UMAX, false, 0, 0.f, nullptr, nullptr);
+            acc_WG<LAMBDA>(P, rho, gs, vb, p, g, SNOWB_UMAX, true, 1, X.sph.mass[o], nullptr, nullptr);
+            D = &X.sph; lam_s = ss.lambda;
         } else if (t < ns + nd) {
-            const uint32_t i = t - ns, o = vd.gi[i];
+            i = t - ns; o = vd.gi[i];
             float3 p = xyz(vd.p4[i]); int3 g = grid_pos(P, p);
-            float lam = -X.dem.C[o];
-            float gs = dot3(z, z);
-            gs = acc_gradsq(P, gs, vd, p, g, i, 0, 0.f, nullptr, nullptr);
-            gs = acc_gradsq(P, gs, vs, p, g, SNOWB_UMAX, 0, 0.f, nullptr, nullptr);
-            gs = acc_gradsq(P, gs, vb, p, g, SNOWB_UMAX, 1, X.dem.mass[o], nullptr, nullptr);
-            lam = lam / (gs + P.eps);
-            X.dem.lambda[o] = lam; sd.lambda[i] = lam;
+            rho = X.dem.mass[o] * P.W0;
+            acc_WG<LAMBDA>(P, rho, gs, vd, p, g, i, false, 0, 0.f, nullptr, nullptr);
+            acc_WG<LAMBDA>(P, rho, gs, vs, p, g, SNOWB_UMAX, false, 0, 0.f, nullptr, nullptr);
+            acc_WG<LAMBDA>(P, rho, gs, vb, p, g, SNOWB_UMAX, true, 1, X.dem.mass[o], nullptr, nullptr);
+            D = &X.dem; lam_s = sd.lambda;
         } else {
-            const uint32_t i = t - ns - nd, o = vb.gi[i];
+            // boundary: density visits (b, snow, water), lambda (b, water, snow)
+            i = t - ns - nd; o = vb.gi[i];
             float3 p = xyz(vb.p4[i]); int3 g = grid_pos(P, p);
-            float lam = -X.bnd.C[o];
-            float gs = dot3(z, z);
-            gs = acc_gradsq(P, gs, vb, p, g, i, 2, 0.f, sb.mass, X.bnd.mass);
-            gs = acc_gradsq(P, gs, vs, p, g, SNOWB_UMAX, 0, 0.f, nullptr, nullptr);
-            gs = acc_gradsq(P, gs, vd, p, g, SNOWB_UMAX, 0, 0.f, nullptr, nullptr);
-            lam = lam / (gs + P.eps);
-            X.bnd.lambda[o] = lam; sb.lambda[i] = lam;
+            rho = (P.rho0 * X.bnd.volume[o]) * P.W0;
+            acc_WG<LAMBDA>(P, rho, gs, vb, p, g, i, true, 2, 0.f, sb.mass, X.bnd.mass);
+            float unused = 0.f;
+            acc_WG<false>(P, rho, unused, vd, p, g, SNOWB_UMAX, false, 0, 0.f, nullptr, nullptr);
+            acc_WG<false>(P, rho, unused, vs, p, g, SNOWB_UMAX, false, 0, 0.f, nullptr, nullptr);
+            if (LAMBDA) {
+                float r2 = 0.f;
+                acc_WG<true>(P, r2, gs, vs, p, g, SNOWB_UMAX, false, 0, 0.f, nullptr, nullptr);
+                acc_WG<true>(P, r2, gs, vd, p, g, SNOWB_UMAX, false, 0, 0.f, nullptr, nullptr);
+            }
+            D = &X.bnd; lam_s = sb.lambda;
+        }
+        D->density[o] = rho;
+        float c = (rho / P.rho0) - 1.f;
+        c = c > 0.f ? c : 0.f;
+        D->C[o] = c;
+        if (LAMBDA) {
+            float lam = (-c) / (gs + P.eps);
+            D->lambda[o] = lam;
+            lam_s[i] = lam;
         }
     }
 }

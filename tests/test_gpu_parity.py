@@ -14,9 +14,9 @@ from tests._util import diff_worlds, track_ids
 
 pytestmark = pytest.mark.gpu
 
-# stage boundaries shared by both implementations (iteration stages 3 and 4 are fused on
-# the GPU, so the comparison inside an iteration happens after 0, 1, 2, 5, 6, 7)
-STOPS = [1, 2, 3, 4, 5, 6, 7] + [10 * (1 + it) + k for it in range(3) for k in (0, 1, 2, 5, 6, 7)] + [90, 0]
+# stage boundaries shared by both implementations (the GPU fuses iteration stages 1-2
+# and 3-5, so the comparison inside an iteration happens after 0, 2, 5, 6, 7)
+STOPS = [1, 2, 3, 4, 5, 6, 7] + [10 * (1 + it) + k for it in range(3) for k in (0, 2, 5, 6, 7)] + [90, 0]
 
 
 def _pair(world, quirks):
