@@ -175,6 +175,12 @@ int snowb_snow_simulation_ex(snowb_particle_data* sph, uint32_t* sph_size,
 /* Set sizes kept on the device by the last call with options->sync = 0 (blocks). */
 int snowb_read_sizes(uint32_t* sph_size, uint32_t* dem_size);
 
+/* Device counters of the last substep, in this order: n_sph, n_dem, n_boundary, sizes at
+ * substep start (2), particles freezing, melting, phase-change flag, sizes after compaction
+ * (2), device error bits, tail-dirty flag, particles kept by the link prefilter, links added.
+ * Copies min(n, 16) values into out (blocks). */
+int snowb_device_counters(uint32_t* out, int n);
+
 /* Default quirk mode of snowb_snow_simulation (SNOWB_QUIRKS_REFERENCE initially). */
 int snowb_set_quirks(int mode);
 

@@ -24,7 +24,7 @@ EXPORTS = (
     "snowb_connect_and_record", "snowb_snow_simulation", "snowb_snow_simulation_ex", "snowb_read_sizes",
     "snowb_set_quirks", "snowb_set_stream", "snowb_synchronize", "snowb_energy_momentum", "snowb_release",
     "snowb_last_error", "snowb_last_error_string", "snowb_launch_count", "snowb_profile_begin",
-    "snowb_profile_end",
+    "snowb_profile_end", "snowb_device_counters",
 )
 
 _lib = None
@@ -66,6 +66,7 @@ def load(path=LIB_PATH):
         "snowb_launch_count": [C.POINTER(C.c_uint64)],
         "snowb_profile_begin": [],
         "snowb_profile_end": [C.c_char_p, C.c_size_t],
+        "snowb_device_counters": [C.POINTER(C.c_uint32), C.c_int],
     }
     sig["snowb_snow_simulation_ex"] = sig["snowb_snow_simulation"] + [C.POINTER(StepOptions)]
     for name, args in sig.items():

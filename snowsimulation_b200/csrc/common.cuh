@@ -38,7 +38,9 @@ struct DevState {
     uint32_t new_sph, new_dem;      // sizes after compaction
     uint32_t err;                   // error bits (SNOWB_DEVERR_*)
     uint32_t tail_dirty;            // a link pass wrote slots beyond the snow set (stale cell range)
-    uint32_t pad[4];
+    uint32_t n_active;              // particles the link prefilter kept for the last link pass
+    uint32_t n_links;               // links added by the last link pass
+    uint32_t pad[2];
 };
 #define SNOWB_DEVERR_SCATTER 1u
 

@@ -205,7 +205,7 @@ __device__ __forceinline__ bool has_free_slot(const uint32_t* rec, uint32_t o, u
         if (rec[q] == SNOWB_UMAX) return true;
     return false;
 }
-__global__ void __launch_bounds__(128) k_link_filter(DevParams P, const DevState* __restrict__ S, SetView vd,
+__global__ void __launch_bounds__(128) k_link_filter(DevParams P, DevState* S, SetView vd,
                                                      snowb_particle_data dem, int dynamic,
                                                      uint8_t* __restrict__ active)
 {
@@ -230,7 +230,9 @@ __global__ void __launch_bounds__(128) k_link_filter(DevParams P, const DevState
                         bool found = false;
                         for (uint32_t q = M * o; q < M * (o + 1); ++q)
                             if (dem.connect_record[q] == o1) { found = true; break; }
-                        if (found) continue;
+                        // a linked candidate ends the reference's scan of this cell, and it
+                        // stays linked, so nothing after it in the cell is reached
+                        if (found) break;
                         if (dem.iter_end[o1] < (o1 + 1) * M && has_free_slot(dem.connect_record, o1, M)) act = 1;
                     }
                 }
@@ -238,11 +240,85 @@ __global__ void __launch_bounds__(128) k_link_filter(DevParams P, const DevState
             }
         }
         active[i] = act;
+        if (act) atomicAdd(&S->n_active, 1u);
     }
 }
-// connect_and_record_cell (:4127-4252) + connect_and_record_d (:4255-4284) for one particle
+// connect_and_record_cell (:4127-4252) + connect_and_record_d (:4255-4284) for one particle.
+// Only this thread edits particle o and its neighbours during the colour phase, so o's
+// slots, count and tolerance are kept in registers (M <= SNOWB_MAXC_FAST); every record
+// write goes through to memory, where the partner search reads it.  Candidates are
+// screened with the exact squared-distance test (dist < h <=> d2 < h2_lt).
+#define SNOWB_MAXC_FAST 32
+__device__ void link_particle_fast(const DevParams& P, const SetView& vd, const snowb_particle_data& d, uint32_t i,
+                                   int dynamic, DevState* S)
+{
+    const uint32_t M = P.maxc;
+    const float3 p = vd.pos(i);
+    const uint32_t o = vd.gi[i];
+    const int3 g = grid_pos(P, p);
+    const uint32_t tol = link_tolerance(P, d.T[o], dynamic);
+    const uint32_t base = o * M;
+    uint32_t count = d.iter_end[o] - base;
+    uint32_t r[SNOWB_MAXC_FAST];
+#pragma unroll
+    for (int k = 0; k < SNOWB_MAXC_FAST; ++k) r[k] = (uint32_t)k < M ? d.connect_record[base + k] : 0u;
+    FOR27 {
+        uint32_t s, e;
+        if (!vd.range(P, g, ox, oy, oz, s, e)) continue;
+        for (uint32_t j = s; j < e; ++j) {
+            if (j == i) continue;
+            const float3 dv = sub3(p, vd.pos(j));
+            const float d2 = dot3(dv, dv);
+            if (!(d2 < P.h2_lt) || !(count < tol)) continue;
+            const uint32_t o1 = vd.gi[j];
+            const float dist = sqrtf(d2);
+            bool dup = false;
+            int free_k = -1;
+#pragma unroll
+            for (int k = 0; k < SNOWB_MAXC_FAST; ++k) {
+                if ((uint32_t)k < M) {
+                    dup |= r[k] == o1;
+                    if (free_k < 0 && r[k] == SNOWB_UMAX) free_k = k;
+                }
+            }
+            if (dup) break;               // the reference returns from the cell helper
+            if (free_k < 0) continue;     // no free slot: the claim loop finds nothing
+            d.connect_record[base + free_k] = o1;           // claim
+            bool valid = false;
+            const uint32_t b1 = o1 * M;
+            if (d.iter_end[o1] < b1 + M)
+                for (uint32_t q = b1; q < b1 + M; ++q)
+                    if (d.connect_record[q] == SNOWB_UMAX) {
+                        d.connect_record[q] = o;
+                        d.connect_length[q] = dist;
+                        d.iter_end[o1]++;
+                        if (o1 >= vd.n) atomicOr(&S->tail_dirty, 1u);
+                        if (o1 == o) {                       // self link (stale cell range)
+                            ++count;
+#pragma unroll
+                            for (int k = 0; k < SNOWB_MAXC_FAST; ++k)
+                                if ((uint32_t)k == q - base) r[k] = o;
+                        }
+                        valid = true;
+                        break;
+                    }
+            if (valid) {
+                d.connect_length[base + free_k] = dist;
+                ++count;
+                d.iter_end[o] = base + count;
+#pragma unroll
+                for (int k = 0; k < SNOWB_MAXC_FAST; ++k)
+                    if (k == free_k) r[k] = o1;
+                atomicAdd(&S->n_links, 1u);
+            } else {
+                d.connect_record[base + free_k] = SNOWB_UMAX;
+            }
+        }
+    }
+}
+// general maximum_connection: the plain restatement with every access in memory
 __device__ void link_particle(const DevParams& P, const SetView& vd, const snowb_particle_data& d, uint32_t i,
-                              int dynamic, uint32_t* tail_flag)
+                              int dynamic, DevState* S)
 {
     const uint32_t M = P.maxc;
     const float3 p = vd.pos(i);
@@ -273,11 +349,11 @@ __device__ void link_particle(const DevParams& P, const SetView& vd, const snowb
                                     d.connect_record[r] = o;
                                     d.connect_length[r] = dist;
                                     d.iter_end[o1]++;
-                                    if (o1 >= vd.n) atomicOr(tail_flag, 1u);
+                                    if (o1 >= vd.n) atomicOr(&S->tail_dirty, 1u);
                                     valid = true;
                                     break;
                                 }
-                        if (valid) { d.connect_length[q] = dist; d.iter_end[o]++; }
+                        if (valid) { d.connect_length[q] = dist; d.iter_end[o]++; atomicAdd(&S->n_links, 1u); }
                         else d.connect_record[q] = SNOWB_UMAX;
                         break;
                     }
@@ -305,7 +381,10 @@ __global__ void k_link_colour(DevParams P, DevState* S, SetView vd, snowb_partic
                     const uint32_t h = ((2u * sz + dz) * P.gsy + (2u * sy + dy)) * P.gsx + (2u * sx + dx);
                     const uint32_t b = fs[h], e = fe[h];
                     for (uint32_t i = b; i < e; ++i)
-                        if (active[i]) link_particle(P, vd, dem, i, dynamic, &S->tail_dirty);
+                        if (active[i]) {
+                            if (P.maxc <= SNOWB_MAXC_FAST) link_particle_fast(P, vd, dem, i, dynamic, S);
+                            else link_particle(P, vd, dem, i, dynamic, S);
+                        }
                 }
     }
 }

@@ -664,6 +664,18 @@ int snowb_read_sizes(uint32_t* sph_size, uint32_t* dem_size)
     return SNOWB_OK;
 }
 
+int snowb_device_counters(uint32_t* out, int n)
+{
+    if (!out || n <= 0) return fail(SNOWB_ERR_INVALID, "null pointer");
+    if (!g_ctx.S) return fail(SNOWB_ERR_INVALID, "no step has run");
+    CUDA_TRY(cudaMemcpyAsync(g_ctx.S_host, g_ctx.S, sizeof(DevState), cudaMemcpyDeviceToHost, g_stream));
+    CUDA_TRY(cudaStreamSynchronize(g_stream));
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(g_ctx.S_host);
+    const int m = (int)(sizeof(DevState) / sizeof(uint32_t));
+    for (int k = 0; k < n; ++k) out[k] = k < m ? src[k] : 0u;
+    return SNOWB_OK;
+}
+
 int snowb_set_quirks(int mode)
 {
     if (mode != SNOWB_QUIRKS_REFERENCE && mode != SNOWB_QUIRKS_FIXED) return fail(SNOWB_ERR_INVALID, "unknown quirk mode");

@@ -717,7 +717,7 @@ __global__ void k_begin_substep(DevState* S)
 {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         S->n0_sph = S->n_sph; S->n0_dem = S->n_dem;
-        S->n_freeze = 0; S->n_melt = 0; S->changed = 0;
+        S->n_freeze = 0; S->n_melt = 0; S->changed = 0; S->n_active = 0; S->n_links = 0;
     }
 }
 
