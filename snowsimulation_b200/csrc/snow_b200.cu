@@ -134,6 +134,7 @@ struct Ctx {
     uint32_t* err_dev = nullptr;
 };
 static Ctx g_ctx;
+static uint64_t g_ctx_gen = 0;   // bumped whenever the scratch buffers are (re)allocated
 
 static void free_set(SetBufs& s)
 {
@@ -174,6 +175,7 @@ static int ensure_ctx(uint32_t full, uint32_t nb, uint32_t ncells)
     Ctx& c = g_ctx;
     if (c.device == dev && c.cap >= full && c.bcap >= nb && c.ncells == ncells) return SNOWB_OK;
     free_ctx(c);
+    ++g_ctx_gen;
     c.device = dev;
     c.cap = full > 0 ? full : 1;
     c.bcap = nb > 0 ? nb : 1;
@@ -216,6 +218,8 @@ static bool g_prof = false;
 static uint64_t g_launches = 0;
 static std::vector<ProfRec> g_prof_pool;
 static size_t g_prof_used = 0;
+static uint64_t g_graph_nodes_per_substep = 0;
+static size_t g_graph_prof_pairs = 0;
 
 static void prof_begin(const char* name)
 {
@@ -235,6 +239,25 @@ static void prof_end()
     if (!g_prof) return;
     cudaEventRecord(g_prof_pool[g_prof_used].b, g_stream);
     ++g_prof_used;
+}
+// accumulated per-kernel times (name, launches, ms) of the current profiling window
+static std::vector<std::string> g_acc_name;
+static std::vector<uint64_t> g_acc_count;
+static std::vector<double> g_acc_ms;
+static int prof_accumulate(size_t first, size_t last)
+{
+    for (size_t k = first; k < last; ++k) {
+        float ms = 0.f;
+        cudaError_t e = cudaEventElapsedTime(&ms, g_prof_pool[k].a, g_prof_pool[k].b);
+        if (e != cudaSuccess) return -1;
+        const std::string nm = g_prof_pool[k].name;
+        size_t idx = 0;
+        while (idx < g_acc_name.size() && g_acc_name[idx] != nm) ++idx;
+        if (idx == g_acc_name.size()) { g_acc_name.push_back(nm); g_acc_count.push_back(0); g_acc_ms.push_back(0.0); }
+        g_acc_count[idx] += 1;
+        g_acc_ms[idx] += ms;
+    }
+    return 0;
 }
 
 static inline unsigned blocks_for(uint64_t work, int tpb)
@@ -435,6 +458,110 @@ static int check_params()
     return SNOWB_OK;
 }
 
+// ------------------------------------------------------------------ CUDA graph of a substep
+// One substep's launch sequence is fixed by its arguments (all sizes live on the device),
+// so it is captured once on a library-owned stream and replayed; the caller's stream and
+// the capture stream are ordered with events.
+struct GraphCache {
+    bool valid = false;
+    std::vector<unsigned char> key;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+    int device = -1;
+};
+static GraphCache g_graph;
+
+static void graph_reset()
+{
+    if (g_graph.exec) cudaGraphExecDestroy(g_graph.exec);
+    if (g_graph.graph) cudaGraphDestroy(g_graph.graph);
+    g_graph.exec = nullptr;
+    g_graph.graph = nullptr;
+    g_graph.valid = false;
+    g_graph.key.clear();
+}
+static void graph_free()
+{
+    graph_reset();
+    if (g_graph.stream) cudaStreamDestroy(g_graph.stream);
+    if (g_graph.ev_in) cudaEventDestroy(g_graph.ev_in);
+    if (g_graph.ev_out) cudaEventDestroy(g_graph.ev_out);
+    g_graph = GraphCache();
+}
+template <class T>
+static void key_add(std::vector<unsigned char>& k, const T& v)
+{
+    const unsigned char* p = reinterpret_cast<const unsigned char*>(&v);
+    k.insert(k.end(), p, p + sizeof(T));
+}
+
+// Run `count` substeps by replaying the captured graph (capturing it first if needed).
+static int graph_substeps(const DevParams& P, const StepArgs& a, bool step_sph, bool step_dem, int count)
+{
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (g_graph.device != dev) {
+        graph_free();
+        g_graph.device = dev;
+    }
+    if (!g_graph.stream) {
+        CUDA_TRY(cudaStreamCreateWithFlags(&g_graph.stream, cudaStreamNonBlocking));
+        CUDA_TRY(cudaEventCreateWithFlags(&g_graph.ev_in, cudaEventDisableTiming));
+        CUDA_TRY(cudaEventCreateWithFlags(&g_graph.ev_out, cudaEventDisableTiming));
+    }
+    std::vector<unsigned char> key;
+    key_add(key, P);
+    key_add(key, a);
+    key_add(key, *a.sph);
+    key_add(key, *a.dem);
+    key_add(key, *a.bnd);
+    key_add(key, *a.buf);
+    key_add(key, step_sph);
+    key_add(key, step_dem);
+    key_add(key, g_ctx.S);
+    key_add(key, g_ctx_gen);
+    key_add(key, g_prof);
+    const cudaStream_t user = g_stream;
+    if (!g_graph.valid || g_graph.key != key) {
+        graph_reset();
+        g_stream = g_graph.stream;
+        // with profiling on, the events recorded around each launch become event nodes of
+        // the graph, which time every kernel without host gaps between launches
+        g_prof_used = 0;
+        cudaError_t e0 = cudaStreamBeginCapture(g_graph.stream, cudaStreamCaptureModeThreadLocal);
+        const uint64_t before = g_launches;
+        int rc = e0 == cudaSuccess ? substep(P, a, step_sph, step_dem) : SNOWB_ERR_CUDA;
+        g_graph_nodes_per_substep = g_launches - before;
+        g_launches = before;
+        cudaGraph_t gr = nullptr;
+        cudaError_t e1 = cudaStreamEndCapture(g_graph.stream, &gr);
+        g_stream = user;
+        g_graph_prof_pairs = g_prof_used;
+        if (e0 != cudaSuccess) return fail(SNOWB_ERR_CUDA, std::string("cudaStreamBeginCapture: ") + cudaGetErrorString(e0));
+        if (rc != SNOWB_OK) { if (gr) cudaGraphDestroy(gr); return rc; }
+        if (e1 != cudaSuccess) return fail(SNOWB_ERR_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e1));
+        g_graph.graph = gr;
+        CUDA_TRY(cudaGraphInstantiate(&g_graph.exec, gr, 0));
+        g_graph.key = key;
+        g_graph.valid = true;
+    }
+    CUDA_TRY(cudaEventRecord(g_graph.ev_in, user));
+    CUDA_TRY(cudaStreamWaitEvent(g_graph.stream, g_graph.ev_in, 0));
+    for (int k = 0; k < count; ++k) {
+        CUDA_TRY(cudaGraphLaunch(g_graph.exec, g_graph.stream));
+        if (g_prof) {
+            CUDA_TRY(cudaStreamSynchronize(g_graph.stream));
+            if (prof_accumulate(0, g_graph_prof_pairs) != 0) return fail(SNOWB_ERR_CUDA, "profile events");
+        }
+    }
+    CUDA_TRY(cudaEventRecord(g_graph.ev_out, g_graph.stream));
+    CUDA_TRY(cudaStreamWaitEvent(user, g_graph.ev_out, 0));
+    g_launches += (uint64_t)count * (uint64_t)g_graph_nodes_per_substep;
+    return SNOWB_OK;
+}
+
 static int run_steps(snowb_particle_data* sph, uint32_t* sph_size, snowb_particle_data* dem, uint32_t* dem_size,
                      snowb_particle_data* bnd, uint32_t nb, uint32_t full, snowb_particle_data* buf,
                      snowb_cell_data scd, snowb_cell_data dcd, snowb_cell_data bcd, snowb_scene_params* scene,
@@ -454,12 +581,30 @@ static int run_steps(snowb_particle_data* sph, uint32_t* sph_size, snowb_particl
                fl[0], fl[1], fl[2], fl[3], fl[4], fl[5], fl[6], fl[7], fl[8], fl[9], fl[10], dTe, opt.stop_after};
     LAUNCH1(k_set_state, c.S, *sph_size, *dem_size, nb);
     LAUNCH(k_boundary_prep, nb, 256, bcd, bnd->volume, bnd->massInv, bnd->mass, nb, c.b.p4, c.b.invm, c.b.mass);
-    for (int k = 0; k < opt.substeps; ++k) {
+    int k = 0;
+    while (k < opt.substeps) {
         const bool step_sph = scene->current_time >= scene->fluid_start_time;
         const bool step_dem = scene->current_time >= scene->solid_start_time;
+        if (opt.use_graph && opt.stop_after == 0) {
+            // replay as many substeps as keep the same step flags
+            int run = 0;
+            float t = scene->current_time;
+            while (k + run < opt.substeps && (t >= scene->fluid_start_time) == step_sph &&
+                   (t >= scene->solid_start_time) == step_dem) {
+                ++run;
+                t += dt;
+            }
+            TRY(graph_substeps(P, a, step_sph, step_dem, run));
+            for (int r = 0; r < run; ++r) scene->current_time += dt;
+            k += run;
+            continue;
+        }
+        const uint64_t before = g_launches;
         TRY(substep(P, a, step_sph, step_dem));
+        g_graph_nodes_per_substep = g_launches - before;
         if (opt.stop_after != 0) break;
         scene->current_time += dt;
+        ++k;
     }
     if (opt.sync) {
         CUDA_TRY(cudaMemcpyAsync(c.S_host, c.S, sizeof(DevState), cudaMemcpyDeviceToHost, g_stream));
@@ -720,30 +865,24 @@ int snowb_profile_begin(void)
 {
     g_prof = true;
     g_prof_used = 0;
+    g_acc_name.clear(); g_acc_count.clear(); g_acc_ms.clear();
     return SNOWB_OK;
 }
 
 int snowb_profile_end(char* out, size_t cap)
 {
     CUDA_TRY(cudaStreamSynchronize(g_stream));
-    std::vector<std::string> names;
-    std::vector<double> total;
-    std::vector<uint64_t> count;
-    for (size_t k = 0; k < g_prof_used; ++k) {
-        float ms = 0.f;
-        CUDA_TRY(cudaEventElapsedTime(&ms, g_prof_pool[k].a, g_prof_pool[k].b));
-        const std::string nm = g_prof_pool[k].name;
-        size_t idx = 0;
-        while (idx < names.size() && names[idx] != nm) ++idx;
-        if (idx == names.size()) { names.push_back(nm); total.push_back(0.0); count.push_back(0); }
-        total[idx] += ms;
-        count[idx] += 1;
-    }
+    if (g_graph.stream) CUDA_TRY(cudaStreamSynchronize(g_graph.stream));
+    // launches issued directly (not through a graph) are still pending in the pool
+    if (!g_graph.valid || g_prof_used > g_graph_prof_pairs)
+        if (prof_accumulate(g_graph.valid ? g_graph_prof_pairs : 0, g_prof_used) != 0)
+            return fail(SNOWB_ERR_CUDA, "profile events");
     g_prof = false;
     g_prof_used = 0;
+    graph_reset();   // the profiling graph carries event nodes; recapture without them
     std::string txt;
-    for (size_t i = 0; i < names.size(); ++i)
-        txt += names[i] + " " + std::to_string(count[i]) + " " + std::to_string(total[i]) + "\n";
+    for (size_t i = 0; i < g_acc_name.size(); ++i)
+        txt += g_acc_name[i] + " " + std::to_string(g_acc_count[i]) + " " + std::to_string(g_acc_ms[i]) + "\n";
     if (out && cap) {
         size_t n = txt.size() < cap - 1 ? txt.size() : cap - 1;
         std::memcpy(out, txt.data(), n);
@@ -756,6 +895,7 @@ int snowb_profile_end(char* out, size_t cap)
 int snowb_release(void)
 {
     std::lock_guard<std::mutex> lk(g_mu);
+    graph_free();
     free_ctx(g_ctx);
     return SNOWB_OK;
 }

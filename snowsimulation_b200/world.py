@@ -113,10 +113,10 @@ class Simulation:
         return self
 
     # -- Simulation::StepCUDA (Simulation.cpp:174-299) without the GL map/unmap
-    def step(self, substeps=1, stop_after=0, sync=True, dt=None, iterations=None):
+    def step(self, substeps=1, stop_after=0, sync=True, dt=None, iterations=None, use_graph=False):
         w = self.w
         ns, nd = C.c_uint32(self.n_sph), C.c_uint32(self.n_dem)
-        opt = _native.StepOptions(self.quirks, substeps, stop_after, 0, 1 if sync else 0)
+        opt = _native.StepOptions(self.quirks, substeps, stop_after, 1 if use_graph else 0, 1 if sync else 0)
         flags = [int(bool(w.flags.get(n, False))) for n in FLAG_NAMES]
         S = self._s
         _native.check(self.lib.snowb_snow_simulation_ex(

@@ -100,3 +100,16 @@ def test_multi_substep_call_matches_single_calls(cuda):
     b.step(substeps=4)
     d = diff_worlds(a.to_host(), b.to_host())
     assert not d, d[:6]
+
+
+def test_graph_replay_matches_direct(cuda):
+    """Substeps replayed from a captured CUDA graph equal substeps issued directly."""
+    from snowsimulation_b200.world import Simulation
+    w = phase_scene(seed=6)
+    a = Simulation(w).setup()
+    b = Simulation(w).setup()
+    a.step(substeps=6)
+    b.step(substeps=3, use_graph=True)
+    b.step(substeps=3, use_graph=True)
+    d = diff_worlds(a.to_host(), b.to_host())
+    assert not d, d[:6]
