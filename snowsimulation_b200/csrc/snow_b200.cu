@@ -220,6 +220,7 @@ static std::vector<ProfRec> g_prof_pool;
 static size_t g_prof_used = 0;
 static uint64_t g_graph_nodes_per_substep = 0;
 static size_t g_graph_prof_pairs = 0;
+static bool g_capturing = false;
 
 static void prof_begin(const char* name)
 {
@@ -232,12 +233,13 @@ static void prof_begin(const char* name)
         g_prof_pool.push_back(r);
     }
     g_prof_pool[g_prof_used].name = name;
-    cudaEventRecord(g_prof_pool[g_prof_used].a, g_stream);
+    // inside a stream capture the record must become an event node of the graph
+    cudaEventRecordWithFlags(g_prof_pool[g_prof_used].a, g_stream, g_capturing ? cudaEventRecordExternal : 0);
 }
 static void prof_end()
 {
     if (!g_prof) return;
-    cudaEventRecord(g_prof_pool[g_prof_used].b, g_stream);
+    cudaEventRecordWithFlags(g_prof_pool[g_prof_used].b, g_stream, g_capturing ? cudaEventRecordExternal : 0);
     ++g_prof_used;
 }
 // accumulated per-kernel times (name, launches, ms) of the current profiling window
@@ -532,7 +534,9 @@ static int graph_substeps(const DevParams& P, const StepArgs& a, bool step_sph, 
         g_prof_used = 0;
         cudaError_t e0 = cudaStreamBeginCapture(g_graph.stream, cudaStreamCaptureModeThreadLocal);
         const uint64_t before = g_launches;
+        g_capturing = true;
         int rc = e0 == cudaSuccess ? substep(P, a, step_sph, step_dem) : SNOWB_ERR_CUDA;
+        g_capturing = false;
         g_graph_nodes_per_substep = g_launches - before;
         g_launches = before;
         cudaGraph_t gr = nullptr;
