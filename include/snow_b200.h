@@ -120,6 +120,16 @@ int snowb_calculate_hash(snowb_cell_data cell_data, const snowb_float3* pos, uin
 /* sort_particles (cuda_simulation.cu:1455-1468): stable sort of (grid_hash, grid_index) by hash. */
 int snowb_sort_particles(snowb_cell_data cell_data, uint32_t num_particles);
 
+/* No counterpart in the reference.  The stable sort of snowb_sort_particles for callers
+ * that cannot allocate device memory (a host capturing its frame into a CUDA graph, a loop
+ * that forbids allocation after start-up, a process under a fixed memory budget).  It
+ * allocates nothing: its scratch is a static device array of about 6 MB that every GPU
+ * loading the library holds until exit.  Limits: at most 262144 particles and 262144 cells
+ * (larger requests fail with SNOWB_ERR_INVALID).  The first call on a device looks up the
+ * array's address and should come before any stream capture.  Calls share the array, so
+ * calls that overlap on the GPU race; the caller serialises them.  Blocks until done. */
+int snowb_sort_particles_static(snowb_cell_data cell_data, uint32_t num_particles);
+
 /* reorder_data (cuda_simulation.cu:377-396 / reorderDataAndFindCellStartD :242-301):
  * clears cell_start[0, num_cells), writes cell_start/cell_end of occupied cells and
  * sorted_pos[i] = old_pos[grid_index[i]]. */

@@ -25,6 +25,7 @@ EXPORTS = (
     "snowb_set_quirks", "snowb_set_stream", "snowb_synchronize", "snowb_energy_momentum", "snowb_release",
     "snowb_last_error", "snowb_last_error_string", "snowb_launch_count", "snowb_profile_begin",
     "snowb_profile_end", "snowb_device_counters",
+    "snowb_sort_particles_static",
 )
 
 _lib = None
@@ -67,6 +68,7 @@ def load(path=LIB_PATH):
         "snowb_profile_begin": [],
         "snowb_profile_end": [C.c_char_p, C.c_size_t],
         "snowb_device_counters": [C.POINTER(C.c_uint32), C.c_int],
+        "snowb_sort_particles_static": [CD, u32],
     }
     sig["snowb_snow_simulation_ex"] = sig["snowb_snow_simulation"] + [C.POINTER(StepOptions)]
     for name, args in sig.items():

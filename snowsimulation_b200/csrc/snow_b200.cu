@@ -698,6 +698,88 @@ int snowb_sort_particles(snowb_cell_data cd, uint32_t n)
     return SNOWB_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Sort without allocation.  Some callers cannot call cudaMalloc: a host that captures
+// its whole frame into a CUDA graph (allocation is not capturable), a renderer or game
+// loop that forbids allocation after start-up, or a process running under a fixed
+// device-memory budget.  snowb_sort_particles_static does the same stable sort as
+// snowb_sort_particles, but all its scratch lives in the fixed array below, which the
+// module reserves once on every device that loads this library and keeps until exit.
+// In host code the array's name is only a host-side stand-in, so its device address is
+// taken with cudaGetSymbolAddress once per device (on the first call made with that
+// device current; that first call should come before any stream capture).  All calls
+// share the array: calls that overlap on the GPU (other streams, other host threads)
+// race and must be serialised by the caller.
+#define SNOWB_STATIC_SORT_MAX_PARTICLES (1u << 18)
+#define SNOWB_STATIC_SORT_MAX_CELLS (1u << 18)
+static constexpr size_t kStaticBsum = SNOWB_STATIC_SORT_MAX_CELLS / SCAN_CHUNK + 2;
+static constexpr size_t kStaticWords = 4ull * SNOWB_STATIC_SORT_MAX_PARTICLES + SNOWB_STATIC_SORT_MAX_CELLS +
+                                       (SNOWB_STATIC_SORT_MAX_CELLS + 1) + kStaticBsum + 1;
+static __device__ __align__(256) uint32_t g_static_sort_scratch[kStaticWords];
+static uint32_t* g_static_sort_ptr[64] = {};   // device address of the array, per device
+
+static int static_sort_scratch(uint32_t** out)
+{
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(SNOWB_ERR_INVALID, "device index out of range for the static scratch table");
+    if (!g_static_sort_ptr[dev]) {
+        void* p = nullptr;
+        CUDA_TRY(cudaGetSymbolAddress(&p, g_static_sort_scratch));
+        g_static_sort_ptr[dev] = static_cast<uint32_t*>(p);
+    }
+    *out = g_static_sort_ptr[dev];
+    return SNOWB_OK;
+}
+#define KL_PLAIN(kernel, grid, tpb, ...)                                                   \
+    do {                                                                                   \
+        kernel<<<(grid), (tpb), 0, g_stream>>>(__VA_ARGS__);                               \
+        cudaError_t _e = cudaGetLastError();                                               \
+        if (_e != cudaSuccess)                                                             \
+            return fail(SNOWB_ERR_CUDA, std::string(#kernel) + ": " + cudaGetErrorString(_e)); \
+    } while (0)
+
+int snowb_sort_particles_static(snowb_cell_data cd, uint32_t n)
+{
+    TRY(check_params());
+    if (n < 2) return SNOWB_OK;
+    if (!cd.grid_hash || !cd.grid_index) return fail(SNOWB_ERR_INVALID, "null pointer");
+    const uint32_t nc = g_P.ncells;
+    if (n > SNOWB_STATIC_SORT_MAX_PARTICLES)
+        return fail(SNOWB_ERR_INVALID, "snowb_sort_particles_static: " + std::to_string(n) +
+                                           " particles exceed the static scratch limit of " +
+                                           std::to_string(SNOWB_STATIC_SORT_MAX_PARTICLES));
+    if (nc > SNOWB_STATIC_SORT_MAX_CELLS)
+        return fail(SNOWB_ERR_INVALID, "snowb_sort_particles_static: " + std::to_string(nc) +
+                                           " cells exceed the static scratch limit of " +
+                                           std::to_string(SNOWB_STATIC_SORT_MAX_CELLS));
+    uint32_t* base = nullptr;
+    TRY(static_sort_scratch(&base));
+    const uint32_t M = SNOWB_STATIC_SORT_MAX_PARTICLES;
+    uint32_t* key = base;
+    uint32_t* val = key + M;
+    uint32_t* slot = val + M;
+    uint32_t* tmp = slot + M;
+    uint32_t* cnt = tmp + M;
+    uint32_t* off = cnt + SNOWB_STATIC_SORT_MAX_CELLS;
+    uint32_t* bsum = off + (SNOWB_STATIC_SORT_MAX_CELLS + 1);
+    uint32_t* err = bsum + kStaticBsum;
+    // the per-cell counters and the error word must start at zero on every call
+    CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(uint32_t) * nc, g_stream));
+    CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(uint32_t), g_stream));
+    const unsigned nb = (nc + SCAN_CHUNK - 1) / SCAN_CHUNK;
+    KL_PLAIN(k_key_count, blocks_for(n, 256), 256, cd.grid_hash, cd.grid_index, n, nc, key, val, slot, cnt, err);
+    KL_PLAIN(k_block_sums, nb, SCAN_TPB, cnt, nc, bsum, nullptr);
+    KL_PLAIN(k_cell_scan, nb, SCAN_TPB, cnt, bsum, nc, off, nullptr, nullptr, 0u, 0, nullptr);
+    KL_PLAIN(k_scatter, blocks_for(n, 256), 256, key, slot, off, tmp, nullptr, n, nullptr);
+    KL_PLAIN(k_rank_pairs, blocks_for(n, 256), 256, key, val, off, tmp, cd.grid_hash, cd.grid_index, n);
+    uint32_t herr = 0;
+    CUDA_TRY(cudaMemcpyAsync(&herr, err, sizeof(uint32_t), cudaMemcpyDeviceToHost, g_stream));
+    CUDA_TRY(cudaStreamSynchronize(g_stream));
+    if (herr) return fail(SNOWB_ERR_INVALID, "grid_hash holds keys >= num_cells");
+    return SNOWB_OK;
+}
+
 int snowb_reorder_data(snowb_cell_data cd, const snowb_float3* old_pos, uint32_t n, uint32_t num_cells)
 {
     TRY(check_params());
