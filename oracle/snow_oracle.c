@@ -6,9 +6,11 @@
  * restates (cuda_simulation.cu unless another file is named).
  *
  * Arithmetic contract shared with the CUDA kernels (so FP32 parity is bit-exact):
- *   - dot(a,b) = fma(a.z,b.z, fma(a.y,b.y, a.x*b.x)); length(v) = sqrt(dot(v,v));
- *   - sqrt and division are IEEE correctly rounded; no other contraction
+ *   - every expression is evaluated as the reference writes it, left to right, each
+ *     operation rounded separately (dot(a,b) = (a.x*b.x + a.y*b.y) + a.z*b.z as in
+ *     helper_math.h, length(v) = sqrt(dot(v,v))); no fused multiply-add anywhere
  *     (build with -ffp-contract=off, never -ffast-math);
+ *   - sqrt and division are IEEE correctly rounded;
  *   - every neighbor sum is accumulated per cell (cells in z,y,x order, particles
  *     in ascending sorted index) and the cell partial is added to the running total,
  *     exactly the structure of the reference's per-cell helper functions;
@@ -73,7 +75,7 @@ static inline r3 vadd(r3 a, r3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); 
 static inline r3 vsub(r3 a, r3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
 static inline r3 vsc(real s, r3 a) { return v3(s * a.x, s * a.y, s * a.z); }
 static inline r3 vdivs(r3 a, real s) { return v3(a.x / s, a.y / s, a.z / s); }
-static inline real vdot(r3 a, r3 b) { return RFMA(a.z, b.z, RFMA(a.y, b.y, a.x * b.x)); }
+static inline real vdot(r3 a, r3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 static inline real vlen(r3 a) { return RSQRT(vdot(a, a)); }
 static inline int vnan(r3 a) { return isnan(a.x) || isnan(a.y) || isnan(a.z); }
 static inline int vinf(r3 a) { return isinf(a.x) || isinf(a.y) || isinf(a.z); }

@@ -8,9 +8,10 @@
  *
  * The same source builds two libraries:
  *   liboracle32.so  (ORACLE_REAL=float)  -- performs exactly the IEEE FP32
- *                   operations that the CUDA kernels perform (explicit fmaf,
- *                   correctly rounded sqrt/div, identical per-cell summation
- *                   order), so CUDA-vs-oracle parity is bit-exact;
+ *                   operations that the CUDA kernels perform (the reference's
+ *                   expressions, no fused multiply-add, correctly rounded sqrt/div,
+ *                   identical per-cell summation order), so CUDA-vs-oracle parity
+ *                   is bit-exact;
  *   liboracle64.so  (ORACLE_REAL=double) -- the FP64 reference run used to
  *                   report the FP32 error.
  *

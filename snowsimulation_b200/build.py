@@ -1,8 +1,8 @@
 """Build libsnowb200.so in-tree for sm_100a with nvcc.
 
-Flags: -fmad=false keeps every multiply and add separately rounded (fused operations are
-written out explicitly in the sources), and fast math stays off so division and sqrt are
-correctly rounded -- the arithmetic contract shared with the CPU oracle.
+Flags: -fmad=false keeps every multiply and add separately rounded, and fast math stays off
+so division and sqrt are correctly rounded -- the arithmetic contract shared with the CPU
+oracle (and with the reference when it is built with the same IEEE settings).
 """
 import os
 import subprocess

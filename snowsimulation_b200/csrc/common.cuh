@@ -1,9 +1,10 @@
 // common.cuh -- shared device definitions for libsnowb200 (sm_100a).
 //
-// Arithmetic contract (identical in the CPU oracle, so results are bit-exact):
-//   dot(a,b) = fma(a.z,b.z, fma(a.y,b.y, a.x*b.x)), length = sqrt(dot); sqrt and '/'
-//   correctly rounded; no other fused operation (the library is built with
-//   -fmad=false, so only the explicit __fmaf_rn calls below fuse).
+// Arithmetic contract (identical in the CPU oracle, so results are bit-exact): every
+// expression is evaluated as the reference writes it, left to right, each operation
+// rounded separately -- dot(a,b) = (a.x*b.x + a.y*b.y) + a.z*b.z as in helper_math.h,
+// length = sqrt(dot) -- with correctly rounded sqrt and '/', and no fused multiply-add
+// (the library is built with -fmad=false).
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -50,7 +51,7 @@ __device__ __forceinline__ float3 add3(float3 a, float3 b) { return f3(a.x + b.x
 __device__ __forceinline__ float3 sub3(float3 a, float3 b) { return f3(a.x - b.x, a.y - b.y, a.z - b.z); }
 __device__ __forceinline__ float3 sc3(float s, float3 a) { return f3(s * a.x, s * a.y, s * a.z); }
 __device__ __forceinline__ float3 div3(float3 a, float s) { return f3(a.x / s, a.y / s, a.z / s); }
-__device__ __forceinline__ float dot3(float3 a, float3 b) { return __fmaf_rn(a.z, b.z, __fmaf_rn(a.y, b.y, a.x * b.x)); }
+__device__ __forceinline__ float dot3(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 __device__ __forceinline__ float len3(float3 a) { return sqrtf(dot3(a, a)); }
 __device__ __forceinline__ bool nan3(float3 a) { return isnan(a.x) || isnan(a.y) || isnan(a.z); }
 __device__ __forceinline__ bool inf3(float3 a) { return isinf(a.x) || isinf(a.y) || isinf(a.z); }
