@@ -264,12 +264,23 @@ def main():
             tot = sum(t for _, t in prof.values())
             for nm, (c, t) in sorted(prof.items(), key=lambda x: -x[1][1]):
                 f.write("%-22s launches %5d  total %9.3f ms  share %5.1f%%\n" % (nm, c, t, 100 * t / tot))
+    def base(nm):
+        return nm.split("<")[0]
     modeled = {nm: v for nm, v in prof.items()
-               if bytes_model.kernel_bytes(nm, sim.n_sph, sim.n_dem, sim.n_b) is not None}
+               if bytes_model.kernel_bytes(base(nm), sim.n_sph, sim.n_dem, sim.n_b) is not None}
     top = max(modeled, key=lambda nm: modeled[nm][1])
     c, t = modeled[top]
     per_launch_s = t / c / 1000.0
-    kb = bytes_model.kernel_bytes(top, sim.n_sph, sim.n_dem, sim.n_b)
+    kb = bytes_model.kernel_bytes(base(top), sim.n_sph, sim.n_dem, sim.n_b)
+    if base(top) == "k_density" and "true" in top:     # density + lambda in one pass
+        kb += bytes_model.PASS["L"] * (sim.n_sph + sim.n_dem + sim.n_b)
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "dram_traffic_config1.txt")
+    if os.path.exists(tfile):   # per-launch DRAM bytes of the kernel from an ncu capture
+        for line in open(tfile):
+            parts = line.split()
+            if len(parts) >= 2 and parts[0] == top:
+                traffic = float(parts[1])
     peak, peak_kind = peaks()
     achieved = kb / per_launch_s / 1e9
     sub_bytes = bytes_model.substep_bytes(sim.n_sph, sim.n_dem, sim.n_b, w.iterations)
@@ -294,7 +305,7 @@ def main():
         "gpu_launches": int(cnt1.value - cnt0.value),
         "clocks": clk,
         "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak,
-                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "algorithmic_bytes_per_launch": kb, "avg_launch_ms": per_launch_s * 1000.0,
                      "launches_per_step": c / 2},
         "substep_roofline": {"algorithmic_bytes": sub_bytes, "achieved_GBs": sub_gbs,
