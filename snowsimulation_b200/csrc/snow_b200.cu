@@ -127,6 +127,7 @@ struct Ctx {
     uint8_t* active = nullptr;
     uint32_t *fs = nullptr, *fe = nullptr;
     snowb_float3* tmp_vel = nullptr;
+    uint32_t *nl_e = nullptr, *nl_cnt = nullptr;
     double* epart = nullptr;
     double* eout = nullptr;
     DevState* S = nullptr;
@@ -149,7 +150,7 @@ static void free_ctx(Ctx& c)
     free_set(c.b);
     free_set(c.gen);
     void* ptrs[] = {c.fl_s, c.fl_d, c.rk_s, c.rk_d, c.sbsum, c.active, c.fs, c.fe, c.tmp_vel, c.epart, c.eout,
-                    c.S, c.err_dev};
+                    c.S, c.err_dev, c.nl_e, c.nl_cnt};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c.S_host) cudaFreeHost(c.S_host);
@@ -188,6 +189,8 @@ static int ensure_ctx(uint32_t full, uint32_t nb, uint32_t ncells)
     TRY(dalloc(&c.active, c.cap));
     TRY(dalloc(&c.fs, ncells)); TRY(dalloc(&c.fe, ncells));
     TRY(dalloc(&c.tmp_vel, c.cap));
+    TRY(dalloc(&c.nl_e, (size_t)NLIST_K * 2 * c.cap));
+    TRY(dalloc(&c.nl_cnt, 2 * (size_t)c.cap));
     TRY(dalloc(&c.epart, 4 * 1024)); TRY(dalloc(&c.eout, 4));
     TRY(dalloc(&c.S, 1)); TRY(dalloc(&c.err_dev, 1));
     CUDA_TRY(cudaMemset(c.S, 0, sizeof(DevState)));
@@ -345,6 +348,7 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
     Sorted sd{c.s[1].invm, c.s[1].contrib, c.s[1].lambda, nullptr};
     Sorted sb{c.b.invm, nullptr, c.b.lambda, c.b.mass};
     StageFlags F{a.correct_dem, a.sph_sph, a.interlink, step_sph ? 1 : 0, step_dem ? 1 : 0};
+    NList NL{c.nl_e, c.nl_cnt, 2 * cap, cap};
     const uint32_t* n_s = &S->n_sph;
     const uint32_t* n_d = &S->n_dem;
     const uint32_t work3 = 2 * full + a.nb;
@@ -363,7 +367,7 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
     TRY(sort_if(1, nullptr));
     TRY(sort_if(0, nullptr));
     STOP(1);
-    LAUNCH(k_density<false>, work3, 128, P, S, vs, vd, vb, X, ss, sd, sb);
+    LAUNCH(k_density<false>, work3, 128, P, S, vs, vd, vb, X, ss, sd, sb, NL);
     STOP(2);
     if (a.temperature) {
         LAUNCH(k_heat, 2 * full, 128, P, S, vs, vd, X, a.dt);
@@ -417,11 +421,11 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
         TRY(sort_if(0, nullptr));
         STOP(base + 0);
         // density + lambda in one pass (stage boundaries base+1 and base+2 coincide)
-        LAUNCH(k_density<true>, work3, 128, P, S, vs, vd, vb, X, ss, sd, sb);
+        LAUNCH(k_density<true>, work3, 128, P, S, vs, vd, vb, X, ss, sd, sb, NL);
         STOP(base + 2);
-        LAUNCH(k_pbf, 2 * full, 128, P, S, vs, vd, vb, X, ss, sd, sb, a.dt, F);
+        LAUNCH(k_pbf, 2 * full, 128, P, S, vs, vd, vb, X, ss, sd, sb, a.dt, F, NL);
         STOP(base + 3);
-        LAUNCH(k_dem_corr, full, 128, P, S, vs, vd, vb, X, ss, sd, sb, F);
+        LAUNCH(k_dem_corr, full, 128, P, S, vs, vd, vb, X, ss, sd, sb, F, NL);
         STOP(base + 5);
         if (step_sph || step_dem) {
             LAUNCH(k_apply, 2 * full, 256, P, S, vs, vd, X, step_sph ? 1 : 0, step_dem ? 1 : 0);
@@ -443,11 +447,11 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
     STOP(90);
     // apply_XSPH_viscosity (:3663-3711), Jacobi
     if (step_sph) {
-        LAUNCH(k_xsph, full, 128, P, S, vs, vd, *a.sph, *a.dem, 1, P.sph_visc, c.tmp_vel);
+        LAUNCH(k_xsph_warp, (uint64_t)full * 32, 128, P, S, vs, vd, *a.sph, *a.dem, 1, P.sph_visc, c.tmp_vel);
         LAUNCH(k_xsph_commit, full, 256, P, S, vs, 1, c.tmp_vel, a.sph->velocity);
     }
     if (a.dem_visc && step_dem) {
-        LAUNCH(k_xsph, full, 128, P, S, vd, vs, *a.dem, *a.sph, 0, P.dem_visc, c.tmp_vel);
+        LAUNCH(k_xsph_warp, (uint64_t)full * 32, 128, P, S, vd, vs, *a.dem, *a.sph, 0, P.dem_visc, c.tmp_vel);
         LAUNCH(k_xsph_commit, full, 256, P, S, vd, 0, c.tmp_vel, a.dem->velocity);
     }
 #undef STOP
@@ -579,6 +583,7 @@ static int run_steps(snowb_particle_data* sph, uint32_t* sph_size, snowb_particl
     DevParams P = g_P;
     P.quirks = opt.quirks;
     if (P.gsx < 4 || P.gsy < 4 || P.gsz < 4) return fail(SNOWB_ERR_INVALID, "grid must be at least 4 cells per axis");
+    if (full >= (1u << 25) || nb >= (1u << 25)) return fail(SNOWB_ERR_INVALID, "more than 2^25 particles per set");
     TRY(ensure_ctx(full, nb, P.ncells));
     Ctx& c = g_ctx;
     StepArgs a{sph, dem, bnd, buf, nb, full, scd, dcd, bcd, dt, iterations,

@@ -23,6 +23,32 @@ struct Sorted {
     float* mass;     // boundary only: mass
 };
 
+// Neighbour lists.  The density+lambda pass records, per water or snow particle, every
+// candidate that passed the support test (d < h), in traversal order, tagged with its
+// set and its cell (0..26).  The PBF and contact passes of the same sort replay the list
+// (their supports are d < h or smaller) instead of re-testing ~300 candidates over 81
+// cells, keeping the per-cell partial sums.  A particle with more than NLIST_K entries is
+// marked overflowed and its consumers traverse the cells as before.
+constexpr uint32_t NLIST_K = 96;
+constexpr uint32_t NL_J_MASK = (1u << 25) - 1u;
+constexpr uint32_t NL_OVF = 1u << 31;
+struct NList {
+    uint32_t* e;       // entry k of slot s at e[k * stride + s]: j | cell << 25 | set << 30
+    uint32_t* cnt;     // per slot: own | other << 10 | boundary << 20 (| NL_OVF)
+    uint32_t stride;   // 2 * capacity: water slots [0, cap), snow slots [cap, 2 cap)
+    uint32_t cap;
+};
+struct NLWriter {
+    uint32_t* e;
+    uint32_t stride, slot, n;
+    __device__ __forceinline__ void push(uint32_t j, int cell, int set)
+    {
+        if (n < NLIST_K) e[(size_t)n * stride + slot] = j | ((uint32_t)cell << 25) | ((uint32_t)set << 30);
+        ++n;
+    }
+};
+#define CELL27 ((oz + 1) * 9 + (oy + 1) * 3 + (ox + 1))
+
 // ------------------------------------------------------------ per-cell neighbour sums
 // pbf_correction (:883-929)
 __device__ __forceinline__ float3 acc_pbf_own(const DevParams& P, float3 acc, const SetView& v, float3 p, int3 g,
@@ -135,6 +161,108 @@ __device__ __forceinline__ float3 acc_contact_sph(const DevParams& P, float3 acc
     return acc_contact(P, acc, v, p, g, skip, w0, invm_s, invm_o);
 }
 
+// Replays of a recorded neighbour segment [k0, k1) of slot `slot`, per-cell partial sums
+// kept (entries of one cell are contiguous and in traversal order).
+struct Seg {
+    const uint32_t* e;
+    uint32_t stride, slot, k0, k1;
+    __device__ __forceinline__ uint32_t at(uint32_t k) const { return __ldg(e + (size_t)k * stride + slot); }
+};
+__device__ __forceinline__ float3 seg_pbf_own(const DevParams& P, float3 acc, const Seg& S, const SetView& v,
+                                              float3 p, float li, const float* lam_s, const float* lam_o,
+                                              const float* con_s, const float* con_o, float dt)
+{
+    float3 cs = f3(0.f, 0.f, 0.f);
+    uint32_t cur = 0xFFu;
+    for (uint32_t k = S.k0; k < S.k1; ++k) {
+        const uint32_t en = S.at(k), j = en & NL_J_MASK, cell = (en >> 25) & 31u;
+        if (cell != cur) { if (cur != 0xFFu) acc = add3(acc, cs); cs = f3(0.f, 0.f, 0.f); cur = cell; }
+        float3 dv = sub3(p, v.pos(j));
+        float d = sqrtf(dot3(dv, dv));
+        float3 gr = G_spiky(P, dv, d);
+        float sc = scorr_of(P, d, dt);
+        float lj = v.attr(lam_s, lam_o, j), cj = v.attr(con_s, con_o, j);
+        cs = add3(cs, sc3(cj * ((li + lj) + sc), gr));
+    }
+    if (cur != 0xFFu) acc = add3(acc, cs);
+    return acc;
+}
+__device__ __forceinline__ float3 seg_pbf_bnd(const DevParams& P, float3 acc, const Seg& S, const SetView& v,
+                                              float3 p, float li, const float* lam_s, const float* lam_o, float dt)
+{
+    float3 cs = f3(0.f, 0.f, 0.f);
+    uint32_t cur = 0xFFu;
+    for (uint32_t k = S.k0; k < S.k1; ++k) {
+        const uint32_t en = S.at(k), j = en & NL_J_MASK, cell = (en >> 25) & 31u;
+        if (cell != cur) { if (cur != 0xFFu) acc = add3(acc, cs); cs = f3(0.f, 0.f, 0.f); cur = cell; }
+        float3 dv = sub3(p, v.pos(j));
+        float d = sqrtf(dot3(dv, dv));
+        float3 gr = G_spiky(P, dv, d);
+        float sc = scorr_of(P, d, dt);
+        cs = add3(cs, sc3((li + v.attr(lam_s, lam_o, j)) + sc, gr));
+    }
+    if (cur != 0xFFu) acc = add3(acc, cs);
+    return acc;
+}
+__device__ __forceinline__ float3 seg_pbf_cpl(const DevParams& P, float3 acc, const Seg& S, const SetView& v,
+                                              float3 p, uint32_t skip, float li, const float* lam_s,
+                                              const float* lam_o, float dt)
+{
+    const bool ref = P.quirks == SNOWB_QUIRKS_REFERENCE;
+    float3 cs = f3(0.f, 0.f, 0.f);
+    uint32_t cur = 0xFFu;
+    for (uint32_t k = S.k0; k < S.k1; ++k) {
+        const uint32_t en = S.at(k), j = en & NL_J_MASK, cell = (en >> 25) & 31u;
+        if (cell != cur) { if (cur != 0xFFu) acc = add3(acc, cs); cs = f3(0.f, 0.f, 0.f); cur = cell; }
+        if (ref && j == skip) continue;
+        float3 dv = sub3(p, v.pos(j));
+        float d2 = dot3(dv, dv);
+        if (d2 < P.r2_le) {
+            float d = sqrtf(d2);
+            float3 gr = G_poly6(P, dv, d);
+            float x = W_poly6(P, d) / P.scorr_div;
+            float x4 = (x * x) * (x * x);
+            float sc = ref ? ((((-P.scorr_coeff) * 0.f) * x4) * dt) * dt : ((-P.scorr_coeff * x4) * dt) * dt;
+            cs = add3(cs, sc3((li + v.attr(lam_s, lam_o, j)) + sc, gr));
+        }
+    }
+    if (cur != 0xFFu) acc = add3(acc, cs);
+    return acc;
+}
+__device__ __forceinline__ float3 seg_contact(const DevParams& P, float3 acc, const Seg& S, const SetView& v,
+                                              float3 p, float w0, const float* invm_s, const float* invm_o)
+{
+    float3 cs = f3(0.f, 0.f, 0.f);
+    uint32_t cur = 0xFFu;
+    for (uint32_t k = S.k0; k < S.k1; ++k) {
+        const uint32_t en = S.at(k), j = en & NL_J_MASK, cell = (en >> 25) & 31u;
+        if (cell != cur) { if (cur != 0xFFu) acc = add3(acc, cs); cs = f3(0.f, 0.f, 0.f); cur = cell; }
+        float3 dv = sub3(p, v.pos(j));
+        float d2 = dot3(dv, dv);
+        if (d2 < P.r2_lt) {
+            float d = sqrtf(d2);
+            float w1 = v.attr(invm_s, invm_o, j);
+            float ws = w0 + w1;
+            float C = d - P.two_r;
+            float3 n = div3(dv, d + P.pbd_eps);
+            cs = add3(cs, sc3(((-w0) * (1.f / ws)) * C, n));
+        }
+    }
+    if (cur != 0xFFu) acc = add3(acc, cs);
+    return acc;
+}
+// segments of slot `slot`; false when the list overflowed (fall back to traversal)
+__device__ __forceinline__ bool segments(const NList& L, uint32_t slot, Seg& own, Seg& oth, Seg& bnd)
+{
+    const uint32_t c = L.cnt[slot];
+    if (c & NL_OVF) return false;
+    const uint32_t a = c & 1023u, b = (c >> 10) & 1023u, d = (c >> 20) & 1023u;
+    own = Seg{L.e, L.stride, slot, 0u, a};
+    oth = Seg{L.e, L.stride, slot, a, a + b};
+    bnd = Seg{L.e, L.stride, slot, a + b, a + b + d};
+    return true;
+}
+
 // ======================================================================== density
 // Density and W-weighted sums with an optional lambda gradient sum in the same pass.
 // compute_snow_{sph,dem_sph,boundary}_density_d (:2219-2528) and, when LAMBDA is set,
@@ -144,7 +272,7 @@ __device__ __forceinline__ float3 acc_contact_sph(const DevParams& P, float3 acc
 template <bool LAMBDA>
 __device__ __forceinline__ void acc_WG(const DevParams& P, float& rho, float& gs, const SetView& v, float3 p, int3 g,
                                        uint32_t skip, bool vol, int mode, float m_self, const float* mass_s,
-                                       const float* mass_o)
+                                       const float* mass_o, NLWriter* wr = nullptr, int set = 0)
 {
     FOR27 {
         float cs = 0.f, cg = 0.f;
@@ -156,6 +284,7 @@ __device__ __forceinline__ void acc_WG(const DevParams& P, float& rho, float& gs
                 float3 dv = sub3(p, xyz(q));
                 float d2 = dot3(dv, dv);
                 if (d2 < P.h2_lt) {
+                    if (wr) wr->push(j, CELL27, set);
                     float d = sqrtf(d2);
                     float w = vol ? P.rho0 * q.w : q.w;
                     cs += w * W_poly6(P, d);
@@ -177,7 +306,7 @@ __device__ __forceinline__ void acc_WG(const DevParams& P, float& rho, float& gs
 }
 template <bool LAMBDA>
 __global__ void __launch_bounds__(128) k_density(DevParams P, const DevState* __restrict__ S, SetView vs, SetView vd,
-                                                 SetView vb, Sets X, Sorted ss, Sorted sd, Sorted sb)
+                                                 SetView vb, Sets X, Sorted ss, Sorted sd, Sorted sb, NList L)
 {
     const uint32_t ns = S->n_sph, nd = S->n_dem, nb = S->n_b;
     vs.n = ns; vd.n = nd; vb.n = nb;
@@ -187,22 +316,27 @@ __global__ void __launch_bounds__(128) k_density(DevParams P, const DevState* __
         const snowb_particle_data* D;
         float* lam_s;
         uint32_t o, i;
-        if (t < ns) {
-            i = t; o = vs.gi[i];
-            float3 p = xyz(vs.p4[i]); int3 g = grid_pos(P, p);
-            rho = X.sph.mass[o] * P.W0;
-            acc_WG<LAMBDA>(P, rho, gs, vs, p, g, i, false, 0, 0.f, nullptr, nullptr);
-            acc_WG<LAMBDA>(P, rho, gs, vd, p, g, SNOWB_UMAX, false, 0, 0.f, nullptr, nullptr);
-            acc_WG<LAMBDA>(P, rho, gs, vb, p, g, SNOWB_UMAX, true, 1, X.sph.mass[o], nullptr, nullptr);
-            D = &X.sph; lam_s = ss.lambda;
-        } else if (t < ns + nd) {
-            i = t - ns; o = vd.gi[i];
-            float3 p = xyz(vd.p4[i]); int3 g = grid_pos(P, p);
-            rho = X.dem.mass[o] * P.W0;
-            acc_WG<LAMBDA>(P, rho, gs, vd, p, g, i, false, 0, 0.f, nullptr, nullptr);
-            acc_WG<LAMBDA>(P, rho, gs, vs, p, g, SNOWB_UMAX, false, 0, 0.f, nullptr, nullptr);
-            acc_WG<LAMBDA>(P, rho, gs, vb, p, g, SNOWB_UMAX, true, 1, X.dem.mass[o], nullptr, nullptr);
-            D = &X.dem; lam_s = sd.lambda;
+        if (t < ns + nd) {
+            const bool w = t < ns;
+            i = w ? t : t - ns;
+            const SetView& own = w ? vs : vd;
+            const SetView& oth = w ? vd : vs;
+            D = w ? &X.sph : &X.dem;
+            lam_s = w ? ss.lambda : sd.lambda;
+            o = own.gi[i];
+            float3 p = xyz(own.p4[i]); int3 g = grid_pos(P, p);
+            rho = D->mass[o] * P.W0;
+            NLWriter wr{L.e, L.stride, (w ? 0u : L.cap) + i, 0u};
+            NLWriter* pw = LAMBDA ? &wr : nullptr;
+            acc_WG<LAMBDA>(P, rho, gs, own, p, g, i, false, 0, 0.f, nullptr, nullptr, pw, 0);
+            const uint32_t n_own = wr.n;
+            acc_WG<LAMBDA>(P, rho, gs, oth, p, g, SNOWB_UMAX, false, 0, 0.f, nullptr, nullptr, pw, 1);
+            const uint32_t n_oth = wr.n - n_own;
+            acc_WG<LAMBDA>(P, rho, gs, vb, p, g, SNOWB_UMAX, true, 1, D->mass[o], nullptr, nullptr, pw, 2);
+            if (LAMBDA) {
+                const uint32_t n_bnd = wr.n - n_own - n_oth;
+                L.cnt[wr.slot] = wr.n > NLIST_K ? NL_OVF : (n_own | (n_oth << 10) | (n_bnd << 20));
+            }
         } else {
             // boundary: density visits (b, snow, water), lambda (b, water, snow)
             i = t - ns - nd; o = vb.gi[i];
@@ -241,7 +375,7 @@ struct StageFlags {
 };
 __global__ void __launch_bounds__(128) k_pbf(DevParams P, const DevState* __restrict__ S, SetView vs, SetView vd,
                                              SetView vb, Sets X, Sorted ss, Sorted sd, Sorted sb, float dt,
-                                             StageFlags F)
+                                             StageFlags F, NList L)
 {
     const uint32_t ns = S->n_sph, nd = S->n_dem, nb = S->n_b;
     vs.n = ns; vd.n = nd; vb.n = nb;
@@ -252,9 +386,17 @@ __global__ void __launch_bounds__(128) k_pbf(DevParams P, const DevState* __rest
             float3 p = xyz(vs.p4[i]); int3 g = grid_pos(P, p);
             const float li = ss.lambda[i];
             float3 c = f3(0.f, 0.f, 0.f);
-            c = acc_pbf_own(P, c, vs, p, g, i, li, ss.lambda, X.sph.lambda, ss.contrib, X.sph.contrib, dt);
-            c = acc_pbf_cpl(P, c, vd, p, g, i, li, sd.lambda, X.dem.lambda, dt);
-            c = acc_pbf_bnd(P, c, vb, p, g, li, sb.lambda, X.bnd.lambda, dt);
+            Seg so, sx, sbn;
+            const bool lst = segments(L, i, so, sx, sbn);
+            if (lst) {
+                c = seg_pbf_own(P, c, so, vs, p, li, ss.lambda, X.sph.lambda, ss.contrib, X.sph.contrib, dt);
+                c = seg_pbf_cpl(P, c, sx, vd, p, i, li, sd.lambda, X.dem.lambda, dt);
+                c = seg_pbf_bnd(P, c, sbn, vb, p, li, sb.lambda, X.bnd.lambda, dt);
+            } else {
+                c = acc_pbf_own(P, c, vs, p, g, i, li, ss.lambda, X.sph.lambda, ss.contrib, X.sph.contrib, dt);
+                c = acc_pbf_cpl(P, c, vd, p, g, i, li, sd.lambda, X.dem.lambda, dt);
+                c = acc_pbf_bnd(P, c, vb, p, g, li, sb.lambda, X.bnd.lambda, dt);
+            }
             c = sc3(P.inv_rho0, c);
             const float ci = X.sph.contrib[o];
             c = sc3(ci, c);
@@ -263,7 +405,8 @@ __global__ void __launch_bounds__(128) k_pbf(DevParams P, const DevState* __rest
             const float3 z = f3(0.f, 0.f, 0.f);
             const float w0 = X.sph.massInv[o];
             if (F.correct_dem) {     // compute_sph_dem_distance_correction
-                float3 d = acc_contact(P, z, vd, p, g, SNOWB_UMAX, w0, sd.invm, X.dem.massInv);
+                float3 d = lst ? seg_contact(P, z, sx, vd, p, w0, sd.invm, X.dem.massInv)
+                               : acc_contact(P, z, vd, p, g, SNOWB_UMAX, w0, sd.invm, X.dem.massInv);
                 d = sc3(1.f - ci, d);
                 if (nan3(d)) d = z;
                 acc = add3(acc, sc3(P.k_stretch, d));
@@ -281,11 +424,20 @@ __global__ void __launch_bounds__(128) k_pbf(DevParams P, const DevState* __rest
             float3 p = xyz(vd.p4[i]); int3 g = grid_pos(P, p);
             const float li = X.dem.lambda[o];
             float3 c = f3(0.f, 0.f, 0.f);
-            c = acc_pbf_cpl(P, c, vs, p, g, i, li, ss.lambda, X.sph.lambda, dt);
-            if (nan3(c)) c = f3(0.f, 0.f, 0.f);
-            c = acc_pbf_own(P, c, vd, p, g, i, li, sd.lambda, X.dem.lambda, sd.contrib, X.dem.contrib, dt);
-            if (nan3(c)) c = f3(0.f, 0.f, 0.f);
-            c = acc_pbf_bnd(P, c, vb, p, g, li, sb.lambda, X.bnd.lambda, dt);
+            Seg so, sx, sbn;
+            if (segments(L, L.cap + i, so, sx, sbn)) {
+                c = seg_pbf_cpl(P, c, sx, vs, p, i, li, ss.lambda, X.sph.lambda, dt);
+                if (nan3(c)) c = f3(0.f, 0.f, 0.f);
+                c = seg_pbf_own(P, c, so, vd, p, li, sd.lambda, X.dem.lambda, sd.contrib, X.dem.contrib, dt);
+                if (nan3(c)) c = f3(0.f, 0.f, 0.f);
+                c = seg_pbf_bnd(P, c, sbn, vb, p, li, sb.lambda, X.bnd.lambda, dt);
+            } else {
+                c = acc_pbf_cpl(P, c, vs, p, g, i, li, ss.lambda, X.sph.lambda, dt);
+                if (nan3(c)) c = f3(0.f, 0.f, 0.f);
+                c = acc_pbf_own(P, c, vd, p, g, i, li, sd.lambda, X.dem.lambda, sd.contrib, X.dem.contrib, dt);
+                if (nan3(c)) c = f3(0.f, 0.f, 0.f);
+                c = acc_pbf_bnd(P, c, vb, p, g, li, sb.lambda, X.bnd.lambda, dt);
+            }
             if (nan3(c)) c = f3(0.f, 0.f, 0.f);
             c = sc3(P.inv_rho0, c);
             c = sc3(1.f - X.dem.contrib[o], c);
@@ -334,7 +486,8 @@ __device__ __forceinline__ float3 link_corr(const DevParams& P, const snowb_part
 // (:1765-1834) and solve_snow_interlink_constraint_d (:4742-4765) for snow particle o,
 // added to its correction in the reference's kernel order (after the PBF pass).
 __global__ void __launch_bounds__(128) k_dem_corr(DevParams P, const DevState* __restrict__ S, SetView vs, SetView vd,
-                                                  SetView vb, Sets X, Sorted ss, Sorted sd, Sorted sb, StageFlags F)
+                                                  SetView vb, Sets X, Sorted ss, Sorted sd, Sorted sb, StageFlags F,
+                                                  NList L)
 {
     const uint32_t ns = S->n_sph, nd = S->n_dem, nb = S->n_b;
     vs.n = ns; vd.n = nd; vb.n = nb;
@@ -344,15 +497,20 @@ __global__ void __launch_bounds__(128) k_dem_corr(DevParams P, const DevState* _
         float3 p = xyz(vd.p4[i]); int3 g = grid_pos(P, p);
         const float w0 = X.dem.massInv[o], ci = X.dem.contrib[o];
         float3 acc = ldv3(X.dem.correction, o);
+        Seg so, sx, sbn;
+        const bool lst = segments(L, L.cap + i, so, sx, sbn);
         if (F.correct_dem) {
-            float3 d = acc_contact(P, z, vs, p, g, SNOWB_UMAX, w0, ss.invm, X.sph.massInv);
+            float3 d = lst ? seg_contact(P, z, sx, vs, p, w0, ss.invm, X.sph.massInv)
+                           : acc_contact(P, z, vs, p, g, SNOWB_UMAX, w0, ss.invm, X.sph.massInv);
             d = sc3(P.k_stretch * ci, d);
             if (nan3(d)) d = z;
             acc = add3(acc, d);
         }
         {
-            float3 d = acc_contact(P, z, vd, p, g, i, w0, sd.invm, X.dem.massInv);
-            d = acc_contact(P, d, vb, p, g, SNOWB_UMAX, w0, sb.invm, X.bnd.massInv);
+            float3 d = lst ? seg_contact(P, z, so, vd, p, w0, sd.invm, X.dem.massInv)
+                           : acc_contact(P, z, vd, p, g, i, w0, sd.invm, X.dem.massInv);
+            d = lst ? seg_contact(P, d, sbn, vb, p, w0, sb.invm, X.bnd.massInv)
+                    : acc_contact(P, d, vb, p, g, SNOWB_UMAX, w0, sb.invm, X.bnd.massInv);
             d = sc3(ci, d);
             if (nan3(d)) d = z;
             acc = add3(acc, d);
@@ -648,6 +806,70 @@ __global__ void __launch_bounds__(128) k_xsph(DevParams P, const DevState* __res
         c = acc_xsph(P, c, voth, B, B.velocity, p, g, SNOWB_UMAX, vi);
         c = sc3(visc, c);
         st3(out_vel, o, add3(vi, c));
+    }
+}
+// Warp-per-particle variant: lane k < 27 computes the partial sum of cell k (the
+// reference's per-cell helper), then the partials are added to the running total in cell
+// order with shuffles -- the same operations in the same order as one thread would do,
+// with 27-way parallelism for the small sets XSPH works on.
+__device__ __forceinline__ float3 warp_ordered_sum(float3 acc, float3 part)
+{
+#pragma unroll 1
+    for (int k = 0; k < 27; ++k) {
+        float3 v;
+        v.x = __shfl_sync(0xffffffffu, part.x, k);
+        v.y = __shfl_sync(0xffffffffu, part.y, k);
+        v.z = __shfl_sync(0xffffffffu, part.z, k);
+        acc = add3(acc, v);
+    }
+    return acc;
+}
+__device__ __forceinline__ float3 xsph_cell(const DevParams& P, const SetView& v, const snowb_particle_data& O,
+                                            const snowb_float3* vel, float3 p, int3 g, int ox, int oy, int oz,
+                                            uint32_t skip, float3 vi)
+{
+    float3 cs = f3(0.f, 0.f, 0.f);
+    uint32_t s, e;
+    if (v.range(P, g, ox, oy, oz, s, e))
+        for (uint32_t j = s; j < e; ++j) {
+            if (j == skip) continue;
+            float3 dv = sub3(p, v.pos(j));
+            float d2 = dot3(dv, dv);
+            if (d2 < P.h2_lt) {
+                const uint32_t oj = v.gi[j];
+                float3 vij = sub3(ldv3(vel, oj), vi);
+                float a = O.mass[oj] / O.density[oj];
+                float wgt = W_poly6(P, sqrtf(d2));
+                cs = add3(cs, f3((a * vij.x) * wgt, (a * vij.y) * wgt, (a * vij.z) * wgt));
+            }
+        }
+    return cs;
+}
+__global__ void __launch_bounds__(128) k_xsph_warp(DevParams P, const DevState* __restrict__ S, SetView vown,
+                                                   SetView voth, snowb_particle_data A, snowb_particle_data B,
+                                                   int own_is_sph, float visc, snowb_float3* __restrict__ out_vel)
+{
+    const uint32_t ns = S->n_sph, nd = S->n_dem;
+    vown.n = own_is_sph ? ns : nd;
+    voth.n = own_is_sph ? nd : ns;
+    const uint32_t limit = own_is_sph ? ns
+                         : (P.quirks == SNOWB_QUIRKS_REFERENCE ? umin32(coverage(ns), nd) : nd);
+    const int lane = threadIdx.x & 31;
+    const int ox = lane % 3 - 1, oy = (lane / 3) % 3 - 1, oz = lane / 9 - 1;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t i = warp; i < limit; i += nwarps) {
+        const uint32_t o = vown.gi[i];
+        const float3 p = xyz(vown.p4[i]);
+        const int3 g = grid_pos(P, p);
+        const float3 vi = ldv3(A.velocity, o);
+        const float3 z = f3(0.f, 0.f, 0.f);
+        float3 part = lane < 27 ? xsph_cell(P, vown, A, A.velocity, p, g, ox, oy, oz, i, vi) : z;
+        float3 c = warp_ordered_sum(z, part);
+        part = lane < 27 ? xsph_cell(P, voth, B, B.velocity, p, g, ox, oy, oz, SNOWB_UMAX, vi) : z;
+        c = warp_ordered_sum(c, part);
+        c = sc3(visc, c);
+        if (lane == 0) st3(out_vel, o, add3(vi, c));
     }
 }
 // write the Jacobi results back (only the processed particles)
