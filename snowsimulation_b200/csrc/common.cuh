@@ -27,6 +27,8 @@ struct DevParams {
     // Exact squared-distance cut-offs: d < h  <=>  d2 < h2_lt, d < 2r <=> d2 < r2_lt,
     // d <= 2r <=> d2 < r2_le, where d = sqrt_rn(d2) (sqrt_rn is monotone).
     float h2_lt, r2_lt, r2_le;
+    // box-culling thresholds: the cut-offs with a relative safety margin
+    float h2_cull, r2_cull;
     int quirks;
 };
 
@@ -145,6 +147,7 @@ struct SetView {
     const uint32_t* cs;     // cell_start
     const uint32_t* ce;     // cell_end
     const uint32_t* gi;     // grid_index (sorted -> original)
+    const uint32_t* gh;     // grid_hash (sorted)
     const float4* p4;       // sorted (x, y, z, w) with w = mass (fluid/snow) or volume (boundary)
     const snowb_float3* sp; // caller's sorted_pos (float3)
     const float* wsrc;      // original-order source of the .w attribute (stale path)
@@ -173,6 +176,32 @@ struct SetView {
         s = __ldg(cs + h);
         if (s == SNOWB_EMPTY) return false;
         e = __ldg(ce + h);
+        return true;
+    }
+    // As range(), but a cell that holds only current members (its first entry is in the
+    // current sort and carries its hash) and whose box lies at squared distance >= cut2
+    // from p is reported empty: every member is then beyond the support, so all its terms
+    // are exact zeros.  Stale ranges (members anywhere) are never culled.
+    __device__ __forceinline__ bool range_culled(const DevParams& P, int3 g, int ox, int oy, int oz, float3 p,
+                                                 float cut2, uint32_t& s, uint32_t& e) const
+    {
+        uint32_t h = grid_hash(P, g, ox, oy, oz);
+        s = __ldg(cs + h);
+        if (s == SNOWB_EMPTY) return false;
+        e = __ldg(ce + h);
+        if (ox | oy | oz) {
+            float gx = 0.f, gy = 0.f, gz = 0.f;
+            const float m = 1e-6f;   // covers the rounding of the face coordinates
+            if (ox < 0) gx = p.x - ((float)g.x * P.csx + P.ox);
+            if (ox > 0) gx = ((float)(g.x + 1) * P.csx + P.ox) - p.x;
+            if (oy < 0) gy = p.y - ((float)g.y * P.csy + P.oy);
+            if (oy > 0) gy = ((float)(g.y + 1) * P.csy + P.oy) - p.y;
+            if (oz < 0) gz = p.z - ((float)g.z * P.csz + P.oz);
+            if (oz > 0) gz = ((float)(g.z + 1) * P.csz + P.oz) - p.z;
+            gx = fmaxf(gx - m, 0.f); gy = fmaxf(gy - m, 0.f); gz = fmaxf(gz - m, 0.f);
+            const float b2 = gx * gx + gy * gy + gz * gz;
+            if (b2 >= cut2 && s < n && __ldg(gh + s) == h) return false;
+        }
         return true;
     }
 };

@@ -95,6 +95,8 @@ static DevParams derive(const snowb_sim_params& s)
     P.h2_lt = smallest_with_sqrt_ge(P.h);
     P.r2_lt = smallest_with_sqrt_ge(P.two_r);
     P.r2_le = smallest_with_sqrt_gt(P.two_r);
+    P.h2_cull = P.h2_lt * (1.f + 1e-5f);
+    P.r2_cull = P.r2_le * (1.f + 1e-5f);
     P.quirks = SNOWB_QUIRKS_REFERENCE;
     return P;
 }
@@ -315,7 +317,8 @@ static int sort_set(const DevParams& P, SetBufs& B, const snowb_particle_data& D
 static SetView make_view(const snowb_cell_data& cd, const float4* p4, const float* wsrc)
 {
     SetView v;
-    v.cs = cd.cell_start; v.ce = cd.cell_end; v.gi = cd.grid_index; v.p4 = p4; v.sp = cd.sorted_pos;
+    v.cs = cd.cell_start; v.ce = cd.cell_end; v.gi = cd.grid_index; v.gh = cd.grid_hash; v.p4 = p4;
+    v.sp = cd.sorted_pos;
     v.wsrc = wsrc; v.n = 0;
     return v;
 }
@@ -426,6 +429,7 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
         LAUNCH(k_pbf, 2 * full, 128, P, S, vs, vd, vb, X, ss, sd, sb, a.dt, F, NL);
         STOP(base + 3);
         LAUNCH(k_dem_corr, full, 128, P, S, vs, vd, vb, X, ss, sd, sb, F, NL);
+        if (a.interlink) LAUNCH(k_interlink, full, 128, P, S, *a.dem);
         STOP(base + 5);
         if (step_sph || step_dem) {
             LAUNCH(k_apply, 2 * full, 256, P, S, vs, vd, X, step_sph ? 1 : 0, step_dem ? 1 : 0);

@@ -134,7 +134,7 @@ __device__ __forceinline__ float3 acc_contact(const DevParams& P, float3 acc, co
     FOR27 {
         float3 cs = f3(0.f, 0.f, 0.f);
         uint32_t s, e;
-        if (v.range(P, g, ox, oy, oz, s, e))
+        if (v.range_culled(P, g, ox, oy, oz, p, P.r2_cull, s, e))
             for (uint32_t j = s; j < e; ++j) {
                 if (j == skip) continue;
                 float3 dv = sub3(p, v.pos(j));
@@ -277,7 +277,7 @@ __device__ __forceinline__ void acc_WG(const DevParams& P, float& rho, float& gs
     FOR27 {
         float cs = 0.f, cg = 0.f;
         uint32_t s, e;
-        if (v.range(P, g, ox, oy, oz, s, e))
+        if (v.range_culled(P, g, ox, oy, oz, p, P.h2_cull, s, e))
             for (uint32_t j = s; j < e; ++j) {
                 if (j == skip) continue;
                 float4 q = v.pw(j);
@@ -515,21 +515,28 @@ __global__ void __launch_bounds__(128) k_dem_corr(DevParams P, const DevState* _
             if (nan3(d)) d = z;
             acc = add3(acc, d);
         }
-        if (F.interlink) {
-            const uint32_t M = P.maxc;
-            volatile const uint32_t* rec = X.dem.connect_record;
-            volatile const float* len = X.dem.connect_length;
-            float3 d = z;
-            for (uint32_t s = M * o; s < M * (o + 1); ++s) {
-                const uint32_t j = rec[s];
-                if (j != SNOWB_UMAX) d = add3(d, link_corr(P, X.dem, o, j, len[s], nd));
-            }
-            if (nan3(d)) d = z;
-            acc = add3(acc, d);
-        }
         st3(X.dem.correction, o, acc);
     }
     (void)ns; (void)nb;
+}
+// solve_snow_interlink_constraint_d (:4742-4765), one thread per snow particle in original
+// order (consecutive threads read consecutive slot blocks; linked partners are near in
+// index), added to the correction after the contact terms as in the reference.
+__global__ void k_interlink(DevParams P, const DevState* __restrict__ S, snowb_particle_data dem)
+{
+    const uint32_t nd = S->n_dem, M = P.maxc;
+    const float3 z = f3(0.f, 0.f, 0.f);
+    GRID_LOOP(o, nd) {
+        volatile const uint32_t* rec = dem.connect_record;
+        volatile const float* len = dem.connect_length;
+        float3 d = z;
+        for (uint32_t s = M * o; s < M * (o + 1); ++s) {
+            const uint32_t j = rec[s];
+            if (j != SNOWB_UMAX) d = add3(d, link_corr(P, dem, o, j, len[s], nd));
+        }
+        if (nan3(d)) d = z;
+        st3(dem.correction, o, add3(ldv3(dem.correction, o), d));
+    }
 }
 
 // ======================================================================= apply
@@ -588,7 +595,7 @@ __global__ void __launch_bounds__(128) k_friction(DevParams P, const DevState* _
         FOR27 {
             float3 cs = f3(0.f, 0.f, 0.f);
             uint32_t s, e;
-            if (vd.range(P, g, ox, oy, oz, s, e))
+            if (vd.range_culled(P, g, ox, oy, oz, p, P.r2_cull, s, e))
                 for (uint32_t j = s; j < e; ++j) {
                     if (j == i) continue;
                     float3 pp1 = vd.pos(j);
@@ -606,7 +613,7 @@ __global__ void __launch_bounds__(128) k_friction(DevParams P, const DevState* _
         FOR27 {
             float3 cs = f3(0.f, 0.f, 0.f);
             uint32_t s, e;
-            if (vb.range(P, g, ox, oy, oz, s, e))
+            if (vb.range_culled(P, g, ox, oy, oz, p, P.r2_cull, s, e))
                 for (uint32_t j = s; j < e; ++j) {
                     float3 v = sub3(p, vb.pos(j));
                     float d2 = dot3(v, v);
