@@ -12,6 +12,10 @@ buffers the reference maps from GL each frame).  Multi-GPU runs are independent 
 (one scene per rank, no collective in the step); `value` is the sum over ranks divided by
 the slowest rank's time.
 
+The line also carries "batched": 64 scenes of uneven size (log-uniform 2k-40k particles)
+stepped as one batch, against the same scenes stepped one after another through the
+plain entry point (--no-batched skips it).
+
 --impl reference times the CPU restatement of the same substep (FP32, all host threads,
 one substep per step), the only CPU implementation of this path: the reference itself
 runs it only on a GPU.
@@ -42,6 +46,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scene", default="config1")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--profile-out", default="")
     return ap.parse_args()
 
@@ -158,6 +163,68 @@ def run_reference(args):
             "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
+
+
+# ----------------------------------------------------------------- batched vs plain
+def batched_compare(frames, dev, seed, flush):
+    """64 scenes of uneven size (log-uniform 2k-40k particles) stepped as one batch, and the
+    same scenes stepped one after another through the plain entry point (each with its
+    own cached substep graph).  Both in the fixed-quirks mode, in which the batch equals
+    the independent runs bit for bit.  Device time with CUDA events per frame."""
+    import torch
+    from snowsimulation_b200 import scene
+    from snowsimulation_b200.abi import QUIRKS_FIXED
+    from snowsimulation_b200.batch import BatchSimulation
+    from snowsimulation_b200.world import Simulation
+
+    worlds = scene.config2(seed=seed)
+    n_part = sum(w.n_sph + w.n_dem for w in worlds)
+    stream = torch.cuda.current_stream(dev)
+
+    def timed(fn):
+        ms = []
+        for _ in range(frames):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            torch.cuda.synchronize(dev)
+            ms.append(a.elapsed_time(b))
+        return sum(ms)
+
+    plain = [Simulation(w, device=dev, quirks=QUIRKS_FIXED).setup() for w in worlds]
+
+    def plain_frame():
+        for sim in plain:
+            sim.step(substeps=SUBSTEPS, sync=False, use_graph=True)
+
+    for _ in range(3):
+        plain_frame()
+    torch.cuda.synchronize(dev)
+    plain_ms = timed(plain_frame)
+    del plain
+    torch.cuda.empty_cache()
+
+    batch = BatchSimulation(worlds, device=dev).setup()
+
+    def batch_frame():
+        batch.step(substeps=SUBSTEPS, sync=False, use_graph=True)
+
+    for _ in range(3):
+        batch_frame()
+    torch.cuda.synchronize(dev)
+    batch_ms = timed(batch_frame)
+    batch.read_sizes()
+    n_b = batch.n_b
+    del batch
+    torch.cuda.empty_cache()
+    ps = n_part * SUBSTEPS * frames
+    return {"workload": "config2: %d scenes, %d water+snow particles (log-uniform 2k-40k per scene) + %d boundary, "
+                        "1 step = 1 frame = %d substeps, fixed quirks" % (len(worlds), n_part, n_b, SUBSTEPS),
+            "frames": frames, "value": ps / (batch_ms / 1000.0), "unit": UNIT, "ms_per_step": batch_ms / frames,
+            "plain_value": ps / (plain_ms / 1000.0), "plain_ms_per_step": plain_ms / frames,
+            "speedup_vs_plain": plain_ms / batch_ms}
 
 
 # ----------------------------------------------------------------- our arm
@@ -294,6 +361,20 @@ def main():
     sub_bytes = bytes_model.substep_bytes(sim.n_sph, sim.n_dem, sim.n_b, w.iterations)
     sub_gbs = sub_bytes * SUBSTEPS / (ms_per_step / 1000.0) / 1e9
 
+    del sim
+    batched_res = None
+    if not args.no_batched:
+        batched_res = batched_compare(min(args.steps, 5), dev, rank, flush)
+        if ws > 1:
+            t = torch.tensor([batched_res["ms_per_step"], batched_res["plain_ms_per_step"]], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            f = batched_res["frames"]
+            ps_rank = batched_res["value"] * batched_res["ms_per_step"] * f / 1000.0
+            batched_res["value"] = ws * ps_rank / (float(t[0]) * f / 1000.0)
+            batched_res["plain_value"] = ws * ps_rank / (float(t[1]) * f / 1000.0)
+            batched_res["ms_per_step"], batched_res["plain_ms_per_step"] = float(t[0]), float(t[1])
+            batched_res["speedup_vs_plain"] = float(t[1]) / float(t[0])
+
     if rank != 0:
         if ws > 1:
             dist.destroy_process_group()
@@ -320,6 +401,8 @@ def main():
                              "frac": sub_gbs / peak},
         "kernel_ms_per_step": {nm: t / prof_frames for nm, (c, t) in sorted(prof.items(), key=lambda x: -x[1][1])},
     }
+    if not args.no_batched:
+        line["batched"] = batched_res
     if ws == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.scene)
     print(json.dumps(line))

@@ -182,6 +182,65 @@ int snowb_snow_simulation_ex(snowb_particle_data* sph, uint32_t* sph_size,
                              int dynamic_max_connections, int cd_on, float temperature_variation,
                              const snowb_step_options* options);
 
+/* ---- batched scenes (no reference counterpart) ------------------------------------------
+ * Many independent scenes that share one snowb_sim_params (same grid, origin, cell size,
+ * constants) are stepped by one launch sequence.  The sets of all scenes are concatenated
+ * into one set per kind (water, snow, boundary); a scene-id array beside each set says
+ * which scene each slot belongs to.  Scene s owns its own copy of the reference's cell
+ * grid, at block (s % scenes_x, s / scenes_x) of a grid that is scenes_x times wider in x
+ * and scenes_z times deeper in z, and wraps inside that block as a lone scene wraps in its
+ * grid, so particles of different scenes never see each other.  With SNOWB_QUIRKS_FIXED
+ * (required: the reference's quirks depend on whole-set sizes) every scene's particles
+ * come out bit for bit as the same scene run alone, in the same relative order.
+ * Cell tables of batched sets hold snowb_batch_num_cells() entries. */
+typedef struct snowb_batch {
+    uint32_t scenes_x, scenes_z;  /* scene blocks along x and z, each a power of two */
+    uint32_t* scene_sph;          /* scene id per water slot (full_size); phase changes move the ids */
+    uint32_t* scene_dem;          /* scene id per snow slot (full_size) */
+    const uint32_t* scene_boundary; /* scene id per boundary particle */
+    uint32_t* scene_buffer;       /* scratch, full_size entries */
+} snowb_batch;
+
+/* Cells of the batched grid: num_cells x scenes_x x scenes_z. */
+int snowb_batch_num_cells(const snowb_batch* batch, uint32_t* num_cells);
+
+/* calculate_hash for a batched set; scene_of[i] is particle i's scene. */
+int snowb_batch_calculate_hash(const snowb_batch* batch, snowb_cell_data cell_data, const snowb_float3* pos,
+                               const uint32_t* scene_of, uint32_t num_particles);
+
+/* sort_particles over the batched grid. */
+int snowb_batch_sort_particles(const snowb_batch* batch, snowb_cell_data cell_data, uint32_t num_particles);
+
+/* reorder_data over the batched grid (clears all snowb_batch_num_cells() cell_start entries). */
+int snowb_batch_reorder_data(const snowb_batch* batch, snowb_cell_data cell_data, const snowb_float3* old_pos,
+                             uint32_t num_particles);
+
+/* compute_boundary_volume of the batched boundary set (scene ids: batch->scene_boundary). */
+int snowb_batch_compute_boundary_volume(const snowb_batch* batch, snowb_cell_data cell_data, float* mass,
+                                        float* volume, uint32_t num_particles);
+
+/* connect_and_record of the batched snow set (scene ids: batch->scene_dem). */
+int snowb_batch_connect_and_record(const snowb_batch* batch, snowb_particle_data* dem, uint32_t dem_size,
+                                   snowb_cell_data dem_cell_data, int dynamic_max_connections);
+
+/* snowb_snow_simulation_ex over all scenes of the batch; options->quirks must be
+ * SNOWB_QUIRKS_FIXED.  Sizes are those of the concatenated sets. */
+int snowb_batch_snow_simulation(const snowb_batch* batch,
+                                snowb_particle_data* sph, uint32_t* sph_size,
+                                snowb_particle_data* dem, uint32_t* dem_size,
+                                snowb_particle_data* boundary, uint32_t boundary_size,
+                                uint32_t full_size,
+                                snowb_particle_data* phase_change_buffer,
+                                snowb_cell_data sph_cell_data, snowb_cell_data dem_cell_data,
+                                snowb_cell_data b_cell_data,
+                                snowb_scene_params* scene_params,
+                                float dt, int iterations,
+                                int sph_dem_correction, int sph_sph_correction, int dem_friction,
+                                int compute_temperature, int change_phase, int simulate_freezing,
+                                int simulate_melting, int dem_viscosity, int use_interlink,
+                                int dynamic_max_connections, int cd_on, float temperature_variation,
+                                const snowb_step_options* options);
+
 /* Set sizes kept on the device by the last call with options->sync = 0 (blocks). */
 int snowb_read_sizes(uint32_t* sph_size, uint32_t* dem_size);
 

@@ -907,19 +907,22 @@ static void reset_records(const K* k, or_particles* d, uint32_t t)
     }
     d->iter_end[t] = k->maxc * t;
 }
-static void compact_set(const K* k, or_particles* d, or_particles* buf, uint32_t full)
+/* rebase = 1 (quirks=fixed, snow set): a moved particle keeps its link count, iter_end =
+   t*maxc + count; the reference copies iter_end verbatim (Q13). */
+static void compact_set(const K* k, or_particles* d, or_particles* buf, uint32_t full, int rebase)
 {
     for (uint32_t i = 0; i < full; i++) copy_info(k, d, buf, i, i);
     for (uint32_t i = 0; i < full; i++) {
         if (d->predicate[i] == 1) {
             uint32_t t = d->scan_index[i];
             copy_info(k, buf, d, i, t);
+            if (rebase) d->iter_end[t] = k->maxc * t + (buf->iter_end[i] - k->maxc * i);
             d->new_index[i] = t;
         } else d->new_index[i] = UMAX;
     }
 }
 static void stage_phase(const K* k, or_particles* sph, uint32_t* ns, or_particles* dem, uint32_t* nd,
-                        or_particles* buf, uint32_t full, int freeze, int melt)
+                        or_particles* buf, uint32_t full, int freeze, int melt, int fixed)
 {
     /* freezing :4416-4449 */
     if (freeze)
@@ -959,8 +962,8 @@ static void stage_phase(const K* k, or_particles* sph, uint32_t* ns, or_particle
                 dem->iter_end[i]--;
             }
         }
-    compact_set(k, sph, buf, full);
-    compact_set(k, dem, buf, full);
+    compact_set(k, sph, buf, full, 0);
+    compact_set(k, dem, buf, full, fixed);
     *ns = sn; *nd = dn;
     *sph->new_end = sn; *dem->new_end = dn;
     for (uint32_t i = 0; i < sn; i++) sph->predicate[i] = 1;
@@ -1158,7 +1161,7 @@ int or_snow_simulation(const or_params* P,
     STOP(3);
     if (flags & OR_CHANGE_PHASE)
         stage_phase(&k, sph, sph_size, dem, dem_size, buffer, full,
-                    (flags & OR_SIMULATE_FREEZING) != 0, (flags & OR_SIMULATE_MELTING) != 0);
+                    (flags & OR_SIMULATE_FREEZING) != 0, (flags & OR_SIMULATE_MELTING) != 0, fixed);
     STOP(4);
     sort_and_reorder(P, &k, dem->predict_positions, dcd, *dem_size, quirks);
     sort_and_reorder(P, &k, sph->predict_positions, scd, *sph_size, quirks);

@@ -6,7 +6,7 @@ raises, so nothing silently runs on another path.
 import ctypes as C
 import os
 
-from .abi import ParticleDeviceData, CellData, SimParams, SceneParams
+from .abi import ParticleDeviceData, CellData, SimParams, SceneParams, Batch
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libsnowb200.so")
@@ -26,6 +26,9 @@ EXPORTS = (
     "snowb_last_error", "snowb_last_error_string", "snowb_launch_count", "snowb_profile_begin",
     "snowb_profile_end", "snowb_device_counters",
     "snowb_sort_particles_static",
+    "snowb_batch_num_cells", "snowb_batch_calculate_hash", "snowb_batch_sort_particles",
+    "snowb_batch_reorder_data", "snowb_batch_compute_boundary_volume", "snowb_batch_connect_and_record",
+    "snowb_batch_snow_simulation",
 )
 
 _lib = None
@@ -71,6 +74,16 @@ def load(path=LIB_PATH):
         "snowb_sort_particles_static": [CD, u32],
     }
     sig["snowb_snow_simulation_ex"] = sig["snowb_snow_simulation"] + [C.POINTER(StepOptions)]
+    PB = C.POINTER(Batch)
+    sig.update({
+        "snowb_batch_num_cells": [PB, pu32],
+        "snowb_batch_calculate_hash": [PB, CD, C.c_void_p, C.c_void_p, u32],
+        "snowb_batch_sort_particles": [PB, CD, u32],
+        "snowb_batch_reorder_data": [PB, CD, C.c_void_p, u32],
+        "snowb_batch_compute_boundary_volume": [PB, CD, C.c_void_p, C.c_void_p, u32],
+        "snowb_batch_connect_and_record": [PB, PPD, u32, CD, i],
+        "snowb_batch_snow_simulation": [PB] + sig["snowb_snow_simulation_ex"],
+    })
     for name, args in sig.items():
         fn = getattr(lib, name)
         fn.argtypes = args

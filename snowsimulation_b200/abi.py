@@ -49,6 +49,12 @@ class SimParams(C.Structure):
     ]
 
 
+class Batch(C.Structure):
+    """snowb_batch: scene layout of a batched run and the scene-id array of each set."""
+    _fields_ = [("scenes_x", C.c_uint32), ("scenes_z", C.c_uint32), ("scene_sph", C.c_void_p),
+                ("scene_dem", C.c_void_p), ("scene_boundary", C.c_void_p), ("scene_buffer", C.c_void_p)]
+
+
 class SceneParams(C.Structure):
     _fields_ = [("fluid_start_time", C.c_float), ("solid_start_time", C.c_float),
                 ("current_time", C.c_float)]

@@ -24,6 +24,12 @@ struct DevParams {
     float Th, k_ref, brk;
     float ox, oy, oz, csx, csy, csz;
     uint32_t gsx, gsy, gsz, ncells, maxc;
+    // Batched scenes: scene s owns the block of sgx x gsy x sgz cells starting at
+    // x = (s % batch_nx) * sgx, z = (s / batch_nx) * sgz, and wraps inside it exactly as a
+    // single scene wraps in its own grid.  batch_nx = 0: one scene, sgx = gsx, sgz = gsz.
+    // batch_nx and the scene count are powers of two; ids are masked into range (an id out
+    // of range is reported by k_check_scenes).
+    uint32_t sgx, sgz, batch_nx, batch_shift, scene_mask;
     // Exact squared-distance cut-offs: d < h  <=>  d2 < h2_lt, d < 2r <=> d2 < r2_lt,
     // d <= 2r <=> d2 < r2_le, where d = sqrt_rn(d2) (sqrt_rn is monotone).
     float h2_lt, r2_lt, r2_le;
@@ -46,6 +52,7 @@ struct DevState {
     uint32_t pad[2];
 };
 #define SNOWB_DEVERR_SCATTER 1u
+#define SNOWB_DEVERR_SCENE 2u      // a batched scene id >= the scene count
 
 // ---------------------------------------------------------------- float3 helpers
 __device__ __forceinline__ float3 f3(float x, float y, float z) { return make_float3(x, y, z); }
@@ -113,19 +120,28 @@ __device__ __forceinline__ float scorr_of(const DevParams& P, float d, float dt)
 }
 
 // ------------------------------------------------------------------ grid :141-157
-__device__ __forceinline__ int3 grid_pos(const DevParams& P, float3 p)
+// grid cell of a particle: coordinates in its scene (unwrapped) and the scene block base
+struct GCell {
+    int x, y, z;
+    uint32_t bx, bz;
+};
+__device__ __forceinline__ GCell grid_pos(const DevParams& P, float3 p, uint32_t scene = 0u)
 {
-    int3 g;
+    GCell g;
     g.x = __float2int_rz(floorf((p.x - P.ox) / P.csx));
     g.y = __float2int_rz(floorf((p.y - P.oy) / P.csy));
     g.z = __float2int_rz(floorf((p.z - P.oz) / P.csz));
+    scene &= P.scene_mask;
+    g.bx = (scene & (P.batch_nx - 1u)) * P.sgx;
+    g.bz = (scene >> P.batch_shift) * P.sgz;
     return g;
 }
-__device__ __forceinline__ uint32_t grid_hash(const DevParams& P, int3 g, int dx, int dy, int dz)
+// hash of cell g + (dx,dy,dz), each axis wrapped in the scene's grid (calcGridHash :151-157)
+__device__ __forceinline__ uint32_t grid_hash(const DevParams& P, GCell g, int dx, int dy, int dz)
 {
-    uint32_t x = ((uint32_t)g.x + (uint32_t)dx) & (P.gsx - 1u);
+    uint32_t x = (((uint32_t)g.x + (uint32_t)dx) & (P.sgx - 1u)) + g.bx;
     uint32_t y = ((uint32_t)g.y + (uint32_t)dy) & (P.gsy - 1u);
-    uint32_t z = ((uint32_t)g.z + (uint32_t)dz) & (P.gsz - 1u);
+    uint32_t z = (((uint32_t)g.z + (uint32_t)dz) & (P.sgz - 1u)) + g.bz;
     return (z * P.gsy) * P.gsx + y * P.gsx + x;
 }
 
@@ -148,6 +164,7 @@ struct SetView {
     const uint32_t* ce;     // cell_end
     const uint32_t* gi;     // grid_index (sorted -> original)
     const uint32_t* gh;     // grid_hash (sorted)
+    const uint32_t* sid;    // scene id per sorted particle (batched runs only, else null)
     const float4* p4;       // sorted (x, y, z, w) with w = mass (fluid/snow) or volume (boundary)
     const snowb_float3* sp; // caller's sorted_pos (float3)
     const float* wsrc;      // original-order source of the .w attribute (stale path)
@@ -169,7 +186,8 @@ struct SetView {
     {
         return j < n ? __ldg(sorted + j) : orig[gi[j]];
     }
-    __device__ __forceinline__ bool range(const DevParams& P, int3 g, int ox, int oy, int oz,
+    __device__ __forceinline__ uint32_t scene(uint32_t i) const { return sid ? __ldg(sid + i) : 0u; }
+    __device__ __forceinline__ bool range(const DevParams& P, GCell g, int ox, int oy, int oz,
                                           uint32_t& s, uint32_t& e) const
     {
         uint32_t h = grid_hash(P, g, ox, oy, oz);
@@ -182,7 +200,7 @@ struct SetView {
     // current sort and carries its hash) and whose box lies at squared distance >= cut2
     // from p is reported empty: every member is then beyond the support, so all its terms
     // are exact zeros.  Stale ranges (members anywhere) are never culled.
-    __device__ __forceinline__ bool range_culled(const DevParams& P, int3 g, int ox, int oy, int oz, float3 p,
+    __device__ __forceinline__ bool range_culled(const DevParams& P, GCell g, int ox, int oy, int oz, float3 p,
                                                  float cut2, uint32_t& s, uint32_t& e) const
     {
         uint32_t h = grid_hash(P, g, ox, oy, oz);

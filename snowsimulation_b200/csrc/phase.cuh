@@ -77,10 +77,14 @@ __global__ void k_phase_count(DevState* S)
     if (blockIdx.x == 0 && threadIdx.x == 0) S->changed = (S->n_freeze + S->n_melt) != 0u;
 }
 // freezing (:4416-4449) and melting (:4387-4414) with ranked targets
+// scene ids of batched runs travel with the particles (null pointers: one scene)
+struct SceneIds {
+    uint32_t *sph, *dem, *buf;
+};
 __global__ void k_phase_move(DevParams P, const DevState* __restrict__ S, snowb_particle_data sph,
                              snowb_particle_data dem, const uint32_t* __restrict__ fl_s,
                              const uint32_t* __restrict__ rk_s, const uint32_t* __restrict__ fl_d,
-                             const uint32_t* __restrict__ rk_d)
+                             const uint32_t* __restrict__ rk_d, SceneIds sc)
 {
     if (S->changed == 0) return;
     const uint32_t ns = S->n_sph, nd = S->n_dem, M = P.maxc;
@@ -90,6 +94,7 @@ __global__ void k_phase_move(DevParams P, const DevState* __restrict__ S, snowb_
             const uint32_t i = t, tg = nd + rk_s[i];
             sph.contrib[i] = 0.f;
             copy_info(sph, dem, i, tg, M);
+            if (sc.sph) sc.dem[tg] = sc.sph[i];
             sph.predicate[i] = 0; sph.trackId[i] = 0;
             dem.predicate[tg] = 1;
             reset_records(dem, tg, M);
@@ -99,6 +104,7 @@ __global__ void k_phase_move(DevParams P, const DevState* __restrict__ S, snowb_
             const uint32_t tg = ns + rk_d[i];
             dem.contrib[i] = 0.f;
             copy_info(dem, sph, i, tg, M);
+            if (sc.sph) sc.sph[tg] = sc.dem[i];
             dem.predicate[i] = 0; dem.trackId[i] = 0;
             sph.predicate[tg] = 1;
         }
@@ -122,13 +128,19 @@ __global__ void k_shuffle_records(DevParams P, const DevState* __restrict__ S, s
 }
 // copy_to_target (:4451-4460) into the caller's phase-change buffer
 __global__ void k_copy_to_buffer(DevParams P, const DevState* __restrict__ S, snowb_particle_data d,
-                                 snowb_particle_data buf, uint32_t full)
+                                 snowb_particle_data buf, uint32_t full, const uint32_t* __restrict__ sid,
+                                 uint32_t* __restrict__ sid_buf)
 {
     if (S->changed == 0) return;
-    GRID_LOOP(i, full) copy_info(d, buf, i, i, P.maxc);
+    GRID_LOOP(i, full) {
+        copy_info(d, buf, i, i, P.maxc);
+        if (sid) sid_buf[i] = sid[i];
+    }
 }
-// scatter (:4462-4480)
-__global__ void k_scatter_set(DevParams P, DevState* S, snowb_particle_data d, snowb_particle_data buf, uint32_t full)
+// scatter (:4462-4480).  rebase (fixed quirks, snow set): a moved particle keeps its link
+// count, iter_end = t*M + count; the reference copies iter_end verbatim (Q13).
+__global__ void k_scatter_set(DevParams P, DevState* S, snowb_particle_data d, snowb_particle_data buf, uint32_t full,
+                              uint32_t* __restrict__ sid, const uint32_t* __restrict__ sid_buf, int rebase)
 {
     if (S->changed == 0) return;
     GRID_LOOP(i, full) {
@@ -136,6 +148,8 @@ __global__ void k_scatter_set(DevParams P, DevState* S, snowb_particle_data d, s
             const uint32_t t = d.scan_index[i];
             if (t >= full) { atomicOr(&S->err, SNOWB_DEVERR_SCATTER); continue; }
             copy_info(buf, d, i, t, P.maxc);
+            if (rebase) d.iter_end[t] = P.maxc * t + (buf.iter_end[i] - P.maxc * i);
+            if (sid) sid[t] = sid_buf[i];
             d.new_index[i] = t;
         } else d.new_index[i] = SNOWB_UMAX;
     }
@@ -217,7 +231,7 @@ __global__ void __launch_bounds__(128) k_link_filter(DevParams P, DevState* S, S
         const uint32_t count = dem.iter_end[o] - o * M;
         uint8_t act = 0;
         if (count < link_tolerance(P, dem.T[o], dynamic) && has_free_slot(dem.connect_record, o, M)) {
-            const int3 g = grid_pos(P, p);
+            const GCell g = grid_pos(P, p, vd.scene(i));
             FOR27 {
                 uint32_t s, e;
                 if (!vd.range(P, g, ox, oy, oz, s, e)) continue;
@@ -255,7 +269,7 @@ __device__ void link_particle_fast(const DevParams& P, const SetView& vd, const 
     const uint32_t M = P.maxc;
     const float3 p = vd.pos(i);
     const uint32_t o = vd.gi[i];
-    const int3 g = grid_pos(P, p);
+    const GCell g = grid_pos(P, p, vd.scene(i));
     const uint32_t tol = link_tolerance(P, d.T[o], dynamic);
     const uint32_t base = o * M;
     uint32_t count = d.iter_end[o] - base;
@@ -323,7 +337,7 @@ __device__ void link_particle(const DevParams& P, const SetView& vd, const snowb
     const uint32_t M = P.maxc;
     const float3 p = vd.pos(i);
     const uint32_t o = vd.gi[i];
-    const int3 g = grid_pos(P, p);
+    const GCell g = grid_pos(P, p, vd.scene(i));
     const float T = d.T[o];
     FOR27 {
         uint32_t s, e;

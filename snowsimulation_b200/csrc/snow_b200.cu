@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -92,6 +93,7 @@ static DevParams derive(const snowb_sim_params& s)
     P.csx = s.cell_size[0]; P.csy = s.cell_size[1]; P.csz = s.cell_size[2];
     P.gsx = s.grid_size[0]; P.gsy = s.grid_size[1]; P.gsz = s.grid_size[2];
     P.ncells = s.num_cells; P.maxc = s.maximum_connection;
+    P.sgx = P.gsx; P.sgz = P.gsz; P.batch_nx = 1; P.batch_shift = 0; P.scene_mask = 0;
     P.h2_lt = smallest_with_sqrt_ge(P.h);
     P.r2_lt = smallest_with_sqrt_ge(P.two_r);
     P.r2_le = smallest_with_sqrt_gt(P.two_r);
@@ -116,6 +118,7 @@ struct SetBufs {
     uint32_t* val = nullptr;
     float4* p4 = nullptr;
     float *invm = nullptr, *contrib = nullptr, *lambda = nullptr, *mass = nullptr;
+    uint32_t* sid = nullptr;   // scene id per sorted particle (batched runs)
 };
 
 struct Ctx {
@@ -141,7 +144,8 @@ static uint64_t g_ctx_gen = 0;   // bumped whenever the scratch buffers are (re)
 
 static void free_set(SetBufs& s)
 {
-    void* ptrs[] = {s.key, s.slot, s.tmp, s.cnt, s.off, s.bsum, s.val, s.p4, s.invm, s.contrib, s.lambda, s.mass};
+    void* ptrs[] = {s.key, s.slot, s.tmp, s.cnt, s.off, s.bsum, s.val, s.p4, s.invm, s.contrib, s.lambda, s.mass,
+                    s.sid};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     s = SetBufs();
@@ -166,6 +170,7 @@ static int alloc_sort(SetBufs& s, uint32_t cap, uint32_t ncells, bool attrs)
     CUDA_TRY(cudaMemset(s.cnt, 0, sizeof(uint32_t) * ncells));
     if (attrs) {
         TRY(dalloc(&s.p4, cap)); TRY(dalloc(&s.invm, cap)); TRY(dalloc(&s.contrib, cap)); TRY(dalloc(&s.lambda, cap));
+        TRY(dalloc(&s.sid, cap));
     }
     return SNOWB_OK;
 }
@@ -185,7 +190,7 @@ static int ensure_ctx(uint32_t full, uint32_t nb, uint32_t ncells)
     c.ncells = ncells;
     for (auto& s : c.s) TRY(alloc_sort(s, c.cap, ncells, true));
     TRY(dalloc(&c.b.p4, c.bcap)); TRY(dalloc(&c.b.invm, c.bcap)); TRY(dalloc(&c.b.mass, c.bcap));
-    TRY(dalloc(&c.b.lambda, c.bcap));
+    TRY(dalloc(&c.b.lambda, c.bcap)); TRY(dalloc(&c.b.sid, c.bcap));
     TRY(dalloc(&c.fl_s, c.cap)); TRY(dalloc(&c.fl_d, c.cap)); TRY(dalloc(&c.rk_s, c.cap)); TRY(dalloc(&c.rk_d, c.cap));
     TRY(dalloc(&c.sbsum, 4 * (c.cap / SCAN_CHUNK + 2)));
     TRY(dalloc(&c.active, c.cap));
@@ -223,8 +228,6 @@ static bool g_prof = false;
 static uint64_t g_launches = 0;
 static std::vector<ProfRec> g_prof_pool;
 static size_t g_prof_used = 0;
-static uint64_t g_graph_nodes_per_substep = 0;
-static size_t g_graph_prof_pairs = 0;
 static bool g_capturing = false;
 
 static void prof_begin(const char* name)
@@ -301,22 +304,25 @@ static int scan(const uint32_t* in, const uint32_t* n_ptr, uint32_t n_fixed, uin
 // hash + stable sort + reorder of one set (sort_and_reorder :398-420), writing the
 // caller's cell data and the compact sorted copies.  cond: skip unless *cond != 0.
 static int sort_set(const DevParams& P, SetBufs& B, const snowb_particle_data& D, const snowb_cell_data& cd,
-                    const uint32_t* n_ptr, uint32_t cap, const uint32_t* cond, bool clear_all)
+                    const uint32_t* n_ptr, uint32_t cap, const uint32_t* cond, bool clear_all,
+                    const uint32_t* sid_o = nullptr)
 {
     const uint32_t nc = P.ncells;
-    LAUNCH(k_hash_count, cap, 256, P, D.predict_positions, n_ptr, 0u, B.key, B.slot, B.cnt, cond);
+    LAUNCH(k_hash_count, cap, 256, P, D.predict_positions, n_ptr, 0u, B.key, B.slot, B.cnt, cond, sid_o);
     const unsigned nb = (nc + SCAN_CHUNK - 1) / SCAN_CHUNK;
     KL(k_block_sums, nb, SCAN_TPB, B.cnt, nc, B.bsum, cond);
     KL(k_cell_scan, nb, SCAN_TPB, B.cnt, B.bsum, nc, B.off, cd.cell_start, n_ptr, 0u, clear_all ? 1 : 0, cond);
     LAUNCH(k_scatter, cap, 256, B.key, B.slot, B.off, B.tmp, n_ptr, 0u, cond);
     LAUNCH(k_rank_reorder, cap, 256, B.key, B.off, B.tmp, D.predict_positions, D.mass, D.massInv, D.contrib, cd, B.p4,
-           B.invm, B.contrib, n_ptr, 0u, cond);
+           B.invm, B.contrib, n_ptr, 0u, cond, sid_o, sid_o ? B.sid : nullptr);
     return SNOWB_OK;
 }
 
-static SetView make_view(const snowb_cell_data& cd, const float4* p4, const float* wsrc)
+static SetView make_view(const snowb_cell_data& cd, const float4* p4, const float* wsrc,
+                         const uint32_t* sid_sorted = nullptr)
 {
     SetView v;
+    v.sid = sid_sorted;
     v.cs = cd.cell_start; v.ce = cd.cell_end; v.gi = cd.grid_index; v.gh = cd.grid_hash; v.p4 = p4;
     v.sp = cd.sorted_pos;
     v.wsrc = wsrc; v.n = 0;
@@ -333,6 +339,8 @@ struct StepArgs {
         dynamic, cd_on;
     float dTe;
     int stop_after;
+    const uint32_t *sid_sph, *sid_dem, *sid_bnd;   // batched runs: scene id per slot (else null)
+    uint32_t* sid_buf;
 };
 
 // One substep (cuda_simulation.cu:4861-5157) given step flags derived from the scene time.
@@ -344,9 +352,11 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
     const uint32_t full = a.full, cap = g_ctx.cap;
     const bool ref = P.quirks == SNOWB_QUIRKS_REFERENCE;
     Sets X{*a.sph, *a.dem, *a.bnd};
-    SetView vs = make_view(a.scd, c.s[0].p4, a.sph->mass);
-    SetView vd = make_view(a.dcd, c.s[1].p4, a.dem->mass);
-    SetView vb = make_view(a.bcd, c.b.p4, a.bnd->volume);
+    const bool batched = a.sid_sph != nullptr;
+    SetView vs = make_view(a.scd, c.s[0].p4, a.sph->mass, batched ? c.s[0].sid : nullptr);
+    SetView vd = make_view(a.dcd, c.s[1].p4, a.dem->mass, batched ? c.s[1].sid : nullptr);
+    SetView vb = make_view(a.bcd, c.b.p4, a.bnd->volume, batched ? c.b.sid : nullptr);
+    SceneIds scn{const_cast<uint32_t*>(a.sid_sph), const_cast<uint32_t*>(a.sid_dem), a.sid_buf};
     Sorted ss{c.s[0].invm, c.s[0].contrib, c.s[0].lambda, nullptr};
     Sorted sd{c.s[1].invm, c.s[1].contrib, c.s[1].lambda, nullptr};
     Sorted sb{c.b.invm, nullptr, c.b.lambda, c.b.mass};
@@ -360,7 +370,7 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
         bool& dirty = set ? dirty_d : dirty_s;
         if (!dirty && !cond) return SNOWB_OK;
         TRY(sort_set(P, c.s[set], set ? *a.dem : *a.sph, set ? a.dcd : a.scd, set ? n_d : n_s, cap, cond,
-                     !ref));
+                     !ref, set ? a.sid_dem : a.sid_sph));
         if (!cond) dirty = false;
         return SNOWB_OK;
     };
@@ -383,16 +393,16 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
         TRY(scan(c.fl_s, n_s, 0, cap, c.sbsum, c.rk_s, &S->n_freeze, nullptr));
         TRY(scan(c.fl_d, n_d, 0, cap, c.sbsum + sb_stride, c.rk_d, &S->n_melt, nullptr));
         LAUNCH1(k_phase_count, S);
-        LAUNCH(k_phase_move, 2 * full, 256, P, S, *a.sph, *a.dem, c.fl_s, c.rk_s, c.fl_d, c.rk_d);
+        LAUNCH(k_phase_move, 2 * full, 256, P, S, *a.sph, *a.dem, c.fl_s, c.rk_s, c.fl_d, c.rk_d, scn);
         // compact_and_clean (:4495-4589): predicate scans run every substep (they define
         // scan_index), the data movement only after a phase change.
         TRY(scan(a.sph->predicate, nullptr, full, full, c.sbsum, a.sph->scan_index, &S->new_sph, nullptr));
         TRY(scan(a.dem->predicate, nullptr, full, full, c.sbsum + sb_stride, a.dem->scan_index, &S->new_dem, nullptr));
         LAUNCH(k_shuffle_records, full, 256, P, S, *a.dem);
-        LAUNCH(k_copy_to_buffer, full, 256, P, S, *a.sph, *a.buf, full);
-        LAUNCH(k_scatter_set, full, 256, P, S, *a.sph, *a.buf, full);
-        LAUNCH(k_copy_to_buffer, full, 256, P, S, *a.dem, *a.buf, full);
-        LAUNCH(k_scatter_set, full, 256, P, S, *a.dem, *a.buf, full);
+        LAUNCH(k_copy_to_buffer, full, 256, P, S, *a.sph, *a.buf, full, scn.sph, scn.buf);
+        LAUNCH(k_scatter_set, full, 256, P, S, *a.sph, *a.buf, full, scn.sph, scn.buf, 0);
+        LAUNCH(k_copy_to_buffer, full, 256, P, S, *a.dem, *a.buf, full, scn.dem, scn.buf);
+        LAUNCH(k_scatter_set, full, 256, P, S, *a.dem, *a.buf, full, scn.dem, scn.buf, ref ? 0 : 1);
         LAUNCH(k_compact_finish, 2 * full, 256, P, S, *a.sph, *a.dem, full);
         LAUNCH1(k_commit_sizes, S);
         LAUNCH(k_update_records, (uint64_t)P.maxc * full, 256, P, S, *a.dem);
@@ -471,26 +481,44 @@ static int check_params()
 // ------------------------------------------------------------------ CUDA graph of a substep
 // One substep's launch sequence is fixed by its arguments (all sizes live on the device),
 // so it is captured once on a library-owned stream and replayed; the caller's stream and
-// the capture stream are ordered with events.
-struct GraphCache {
-    bool valid = false;
+// the capture stream are ordered with events.  Graphs are cached by their arguments, so a
+// host that alternates between several scenes (or batches) replays each scene's graph
+// without capturing it again; the least recently used graph goes when the cache is full.
+struct GraphEntry {
     std::vector<unsigned char> key;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    uint64_t nodes = 0;        // kernels per replay
+    size_t prof_pairs = 0;     // profiling event pairs recorded by one replay
+    bool prof = false;         // captured with profiling event nodes
+    uint64_t last_use = 0;
+};
+struct GraphCache {
+    std::vector<GraphEntry> entries;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
     int device = -1;
+    uint64_t tick = 0;
+    bool prof_replayed = false;   // a profiling graph ran since snowb_profile_begin
+    size_t prof_pairs = 0;        // its event pairs (already accumulated after each replay)
 };
 static GraphCache g_graph;
+static constexpr size_t kGraphCacheMax = 256;
 
-static void graph_reset()
+static void graph_destroy(GraphEntry& e)
 {
-    if (g_graph.exec) cudaGraphExecDestroy(g_graph.exec);
-    if (g_graph.graph) cudaGraphDestroy(g_graph.graph);
-    g_graph.exec = nullptr;
-    g_graph.graph = nullptr;
-    g_graph.valid = false;
-    g_graph.key.clear();
+    if (e.exec) cudaGraphExecDestroy(e.exec);
+    if (e.graph) cudaGraphDestroy(e.graph);
+    e.exec = nullptr;
+    e.graph = nullptr;
+}
+// drop cached graphs (only the profiling ones if prof_only)
+static void graph_reset(bool prof_only = false)
+{
+    auto& v = g_graph.entries;
+    for (auto& e : v)
+        if (!prof_only || e.prof) graph_destroy(e);
+    v.erase(std::remove_if(v.begin(), v.end(), [](const GraphEntry& e) { return e.exec == nullptr; }), v.end());
 }
 static void graph_free()
 {
@@ -534,8 +562,16 @@ static int graph_substeps(const DevParams& P, const StepArgs& a, bool step_sph, 
     key_add(key, g_ctx_gen);
     key_add(key, g_prof);
     const cudaStream_t user = g_stream;
-    if (!g_graph.valid || g_graph.key != key) {
-        graph_reset();
+    GraphEntry* ent = nullptr;
+    for (auto& e : g_graph.entries)
+        if (e.key == key) { ent = &e; break; }
+    if (!ent) {
+        if (g_graph.entries.size() >= kGraphCacheMax) {
+            auto lru = std::min_element(g_graph.entries.begin(), g_graph.entries.end(),
+                                        [](const GraphEntry& x, const GraphEntry& y) { return x.last_use < y.last_use; });
+            graph_destroy(*lru);
+            g_graph.entries.erase(lru);
+        }
         g_stream = g_graph.stream;
         // with profiling on, the events recorded around each launch become event nodes of
         // the graph, which time every kernel without host gaps between launches
@@ -545,39 +581,71 @@ static int graph_substeps(const DevParams& P, const StepArgs& a, bool step_sph, 
         g_capturing = true;
         int rc = e0 == cudaSuccess ? substep(P, a, step_sph, step_dem) : SNOWB_ERR_CUDA;
         g_capturing = false;
-        g_graph_nodes_per_substep = g_launches - before;
+        const uint64_t nodes = g_launches - before;
         g_launches = before;
         cudaGraph_t gr = nullptr;
         cudaError_t e1 = cudaStreamEndCapture(g_graph.stream, &gr);
         g_stream = user;
-        g_graph_prof_pairs = g_prof_used;
         if (e0 != cudaSuccess) return fail(SNOWB_ERR_CUDA, std::string("cudaStreamBeginCapture: ") + cudaGetErrorString(e0));
         if (rc != SNOWB_OK) { if (gr) cudaGraphDestroy(gr); return rc; }
         if (e1 != cudaSuccess) return fail(SNOWB_ERR_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e1));
-        g_graph.graph = gr;
-        CUDA_TRY(cudaGraphInstantiate(&g_graph.exec, gr, 0));
-        g_graph.key = key;
-        g_graph.valid = true;
+        GraphEntry e;
+        e.key = std::move(key);
+        e.graph = gr;
+        e.nodes = nodes;
+        e.prof = g_prof;
+        e.prof_pairs = g_prof_used;
+        cudaError_t e2 = cudaGraphInstantiate(&e.exec, gr, 0);
+        if (e2 != cudaSuccess) {
+            cudaGraphDestroy(gr);
+            return fail(SNOWB_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e2));
+        }
+        g_graph.entries.push_back(std::move(e));
+        ent = &g_graph.entries.back();
+    }
+    ent->last_use = ++g_graph.tick;
+    if (ent->prof) {
+        g_graph.prof_replayed = true;
+        g_graph.prof_pairs = ent->prof_pairs;
     }
     CUDA_TRY(cudaEventRecord(g_graph.ev_in, user));
     CUDA_TRY(cudaStreamWaitEvent(g_graph.stream, g_graph.ev_in, 0));
     for (int k = 0; k < count; ++k) {
-        CUDA_TRY(cudaGraphLaunch(g_graph.exec, g_graph.stream));
-        if (g_prof) {
+        CUDA_TRY(cudaGraphLaunch(ent->exec, g_graph.stream));
+        if (ent->prof) {
             CUDA_TRY(cudaStreamSynchronize(g_graph.stream));
-            if (prof_accumulate(0, g_graph_prof_pairs) != 0) return fail(SNOWB_ERR_CUDA, "profile events");
+            if (prof_accumulate(0, ent->prof_pairs) != 0) return fail(SNOWB_ERR_CUDA, "profile events");
         }
     }
     CUDA_TRY(cudaEventRecord(g_graph.ev_out, g_graph.stream));
     CUDA_TRY(cudaStreamWaitEvent(user, g_graph.ev_out, 0));
-    g_launches += (uint64_t)count * (uint64_t)g_graph_nodes_per_substep;
+    g_launches += (uint64_t)count * ent->nodes;
+    return SNOWB_OK;
+}
+
+// Grid of a batch: the scene grid repeated scenes_x times along x and scenes_z times along z.
+static int batch_layout(DevParams& P, const snowb_batch* b)
+{
+    if (!b) return fail(SNOWB_ERR_INVALID, "null batch");
+    const uint32_t nx = b->scenes_x, nz = b->scenes_z;
+    if (nx == 0 || nz == 0 || (nx & (nx - 1)) || (nz & (nz - 1)))
+        return fail(SNOWB_ERR_INVALID, "scenes_x and scenes_z must be powers of two");
+    const uint64_t cells = (uint64_t)P.gsx * nx * P.gsy * P.gsz * nz;
+    if (cells >= (1ull << 31)) return fail(SNOWB_ERR_INVALID, "batched cell grid too large");
+    P.sgx = P.gsx; P.sgz = P.gsz;
+    P.gsx *= nx; P.gsz *= nz;
+    P.ncells = (uint32_t)cells;
+    P.batch_nx = nx;
+    P.batch_shift = (uint32_t)__builtin_ctz(nx);
+    P.scene_mask = nx * nz - 1u;
     return SNOWB_OK;
 }
 
 static int run_steps(snowb_particle_data* sph, uint32_t* sph_size, snowb_particle_data* dem, uint32_t* dem_size,
                      snowb_particle_data* bnd, uint32_t nb, uint32_t full, snowb_particle_data* buf,
                      snowb_cell_data scd, snowb_cell_data dcd, snowb_cell_data bcd, snowb_scene_params* scene,
-                     float dt, int iterations, const int* fl, float dTe, const snowb_step_options& opt)
+                     float dt, int iterations, const int* fl, float dTe, const snowb_step_options& opt,
+                     const snowb_batch* batch = nullptr)
 {
     TRY(check_params());
     if (!sph || !dem || !bnd || !buf || !sph_size || !dem_size || !scene)
@@ -588,12 +656,25 @@ static int run_steps(snowb_particle_data* sph, uint32_t* sph_size, snowb_particl
     P.quirks = opt.quirks;
     if (P.gsx < 4 || P.gsy < 4 || P.gsz < 4) return fail(SNOWB_ERR_INVALID, "grid must be at least 4 cells per axis");
     if (full >= (1u << 25) || nb >= (1u << 25)) return fail(SNOWB_ERR_INVALID, "more than 2^25 particles per set");
+    if (batch) {
+        if (opt.quirks != SNOWB_QUIRKS_FIXED)
+            return fail(SNOWB_ERR_INVALID, "batched scenes need SNOWB_QUIRKS_FIXED (the reference's quirks depend "
+                                           "on whole-set sizes)");
+        if (!batch->scene_sph || !batch->scene_dem || !batch->scene_boundary || !batch->scene_buffer)
+            return fail(SNOWB_ERR_INVALID, "batch scene id arrays missing");
+        TRY(batch_layout(P, batch));
+    }
     TRY(ensure_ctx(full, nb, P.ncells));
     Ctx& c = g_ctx;
     StepArgs a{sph, dem, bnd, buf, nb, full, scd, dcd, bcd, dt, iterations,
-               fl[0], fl[1], fl[2], fl[3], fl[4], fl[5], fl[6], fl[7], fl[8], fl[9], fl[10], dTe, opt.stop_after};
+               fl[0], fl[1], fl[2], fl[3], fl[4], fl[5], fl[6], fl[7], fl[8], fl[9], fl[10], dTe, opt.stop_after,
+               batch ? batch->scene_sph : nullptr, batch ? batch->scene_dem : nullptr,
+               batch ? batch->scene_boundary : nullptr, batch ? batch->scene_buffer : nullptr};
     LAUNCH1(k_set_state, c.S, *sph_size, *dem_size, nb);
-    LAUNCH(k_boundary_prep, nb, 256, bcd, bnd->volume, bnd->massInv, bnd->mass, nb, c.b.p4, c.b.invm, c.b.mass);
+    if (batch)
+        LAUNCH(k_check_scenes, full > nb ? full : nb, 256, P, c.S, a.sid_sph, a.sid_dem, a.sid_bnd);
+    LAUNCH(k_boundary_prep, nb, 256, bcd, bnd->volume, bnd->massInv, bnd->mass, nb, c.b.p4, c.b.invm, c.b.mass,
+           a.sid_bnd, a.sid_bnd ? c.b.sid : nullptr);
     int k = 0;
     while (k < opt.substeps) {
         const bool step_sph = scene->current_time >= scene->fluid_start_time;
@@ -612,9 +693,7 @@ static int run_steps(snowb_particle_data* sph, uint32_t* sph_size, snowb_particl
             k += run;
             continue;
         }
-        const uint64_t before = g_launches;
         TRY(substep(P, a, step_sph, step_dem));
-        g_graph_nodes_per_substep = g_launches - before;
         if (opt.stop_after != 0) break;
         scene->current_time += dt;
         ++k;
@@ -626,6 +705,87 @@ static int run_steps(snowb_particle_data* sph, uint32_t* sph_size, snowb_particl
         *dem_size = c.S_host->n_dem;
         if (c.S_host->err) return fail(SNOWB_ERR_DEVICE, "device error flag " + std::to_string(c.S_host->err));
     }
+    return SNOWB_OK;
+}
+
+// ------------------------------------------------------- set-up passes (one or many scenes)
+static int calc_hash(const DevParams& P, snowb_cell_data cd, const snowb_float3* pos, const uint32_t* sid, uint32_t n)
+{
+    if (n == 0) return SNOWB_OK;
+    if (!pos || !cd.grid_hash || !cd.grid_index) return fail(SNOWB_ERR_INVALID, "null pointer");
+    LAUNCH(k_calc_hash, n, 256, P, cd, pos, n, sid);
+    return SNOWB_OK;
+}
+
+// stable sort of (grid_hash, grid_index) pairs by hash over a table of nc cells
+static int sort_pairs(uint32_t nc, snowb_cell_data cd, uint32_t n)
+{
+    if (n < 2) return SNOWB_OK;
+    if (!cd.grid_hash || !cd.grid_index) return fail(SNOWB_ERR_INVALID, "null pointer");
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (g_ctx.device != dev || g_ctx.ncells != nc) TRY(ensure_ctx(1, 1, nc));
+    TRY(ensure_gen(n, nc));
+    SetBufs& B = g_ctx.gen;
+    CUDA_TRY(cudaMemsetAsync(g_ctx.err_dev, 0, sizeof(uint32_t), g_stream));
+    LAUNCH(k_key_count, n, 256, cd.grid_hash, cd.grid_index, n, nc, B.key, B.val, B.slot, B.cnt, g_ctx.err_dev);
+    const unsigned nb = (nc + SCAN_CHUNK - 1) / SCAN_CHUNK;
+    KL(k_block_sums, nb, SCAN_TPB, B.cnt, nc, B.bsum, nullptr);
+    // cell_start is not touched by a plain sort: clear nothing (clear_all = 0, n = 0)
+    KL(k_cell_scan, nb, SCAN_TPB, B.cnt, B.bsum, nc, B.off, nullptr, nullptr, 0u, 0, nullptr);
+    LAUNCH(k_scatter, n, 256, B.key, B.slot, B.off, B.tmp, nullptr, n, nullptr);
+    LAUNCH(k_rank_pairs, n, 256, B.key, B.val, B.off, B.tmp, cd.grid_hash, cd.grid_index, n);
+    uint32_t err = 0;
+    CUDA_TRY(cudaMemcpyAsync(&err, g_ctx.err_dev, sizeof(uint32_t), cudaMemcpyDeviceToHost, g_stream));
+    CUDA_TRY(cudaStreamSynchronize(g_stream));
+    if (err) return fail(SNOWB_ERR_INVALID, "grid_hash holds keys >= num_cells");
+    return SNOWB_OK;
+}
+
+static int reorder(uint32_t table_cells, snowb_cell_data cd, const snowb_float3* old_pos, uint32_t n,
+                   uint32_t num_cells)
+{
+    if (!cd.cell_start || !cd.cell_end || !cd.grid_hash || !cd.grid_index || !cd.sorted_pos)
+        return fail(SNOWB_ERR_INVALID, "null pointer");
+    if (num_cells > table_cells) return fail(SNOWB_ERR_INVALID, "num_cells exceeds the cell table");
+    if (num_cells) CUDA_TRY(cudaMemsetAsync(cd.cell_start, 0xff, sizeof(uint32_t) * num_cells, g_stream));
+    if (n == 0) return SNOWB_OK;
+    if (!old_pos) return fail(SNOWB_ERR_INVALID, "null pointer");
+    LAUNCH(k_reorder, n, 256, cd, old_pos, n);
+    return SNOWB_OK;
+}
+
+static int boundary_volume(const DevParams& P, snowb_cell_data cd, float* mass, float* volume, const uint32_t* sid,
+                           uint32_t n)
+{
+    if (n == 0) return SNOWB_OK;
+    if (!mass || !volume) return fail(SNOWB_ERR_INVALID, "null pointer");
+    LAUNCH(k_boundary_volume, n, 128, P, cd, mass, volume, n, sid);
+    return SNOWB_OK;
+}
+
+// connect_and_record over a sorted snow set (sid: its scene ids in original order, or null)
+static int connect_links(const DevParams& P, snowb_particle_data* dem, uint32_t n, snowb_cell_data dcd, int dynamic,
+                         const uint32_t* sid)
+{
+    if (!dem) return fail(SNOWB_ERR_INVALID, "null pointer");
+    if (n == 0) return SNOWB_OK;
+    if (P.gsx < 4 || P.gsy < 4 || P.gsz < 4) return fail(SNOWB_ERR_INVALID, "grid must be at least 4 cells per axis");
+    TRY(ensure_ctx(g_ctx.cap > n ? g_ctx.cap : n, g_ctx.bcap ? g_ctx.bcap : 1, P.ncells));
+    Ctx& c = g_ctx;
+    LAUNCH1(k_set_state, c.S, 0u, n, 0u);
+    CUDA_TRY(cudaMemsetAsync(c.fs, 0, sizeof(uint32_t) * P.ncells, g_stream));
+    CUDA_TRY(cudaMemsetAsync(c.fe, 0, sizeof(uint32_t) * P.ncells, g_stream));
+    LAUNCH(k_fresh_ranges, n, 256, dcd.grid_hash, n, c.fs, c.fe);
+    // the view's compact copy (and sorted scene ids) are filled from sorted_pos
+    LAUNCH(k_boundary_prep, n, 256, dcd, dem->mass, dem->massInv, dem->mass, n, c.s[1].p4, c.s[1].invm, c.s[1].lambda,
+           sid, sid ? c.s[1].sid : nullptr);
+    SetView vd = make_view(dcd, c.s[1].p4, dem->mass, sid ? c.s[1].sid : nullptr);
+    LAUNCH(k_link_filter, n, 128, P, c.S, vd, *dem, dynamic, c.active);
+    for (uint32_t col = 0; col < 8; ++col)
+        LAUNCH(k_link_colour, (P.gsx / 4) * (P.gsy / 4) * (P.gsz / 4), 64, P, c.S, vd, *dem, c.fs, c.fe, c.active, col,
+               dynamic);
+    CUDA_TRY(cudaStreamSynchronize(g_stream));
     return SNOWB_OK;
 }
 
@@ -675,36 +835,13 @@ int snowb_compute_grid_size(uint32_t n, uint32_t block_size, uint32_t* num_block
 int snowb_calculate_hash(snowb_cell_data cd, const snowb_float3* pos, uint32_t n)
 {
     TRY(check_params());
-    if (n == 0) return SNOWB_OK;
-    if (!pos || !cd.grid_hash || !cd.grid_index) return fail(SNOWB_ERR_INVALID, "null pointer");
-    LAUNCH(k_calc_hash, n, 256, g_P, cd, pos, n);
-    return SNOWB_OK;
+    return calc_hash(g_P, cd, pos, nullptr, n);
 }
 
 int snowb_sort_particles(snowb_cell_data cd, uint32_t n)
 {
     TRY(check_params());
-    if (n < 2) return SNOWB_OK;
-    if (!cd.grid_hash || !cd.grid_index) return fail(SNOWB_ERR_INVALID, "null pointer");
-    const uint32_t nc = g_P.ncells;
-    int dev = 0;
-    CUDA_TRY(cudaGetDevice(&dev));
-    if (g_ctx.device != dev || g_ctx.ncells != nc) TRY(ensure_ctx(1, 1, nc));
-    TRY(ensure_gen(n, nc));
-    SetBufs& B = g_ctx.gen;
-    CUDA_TRY(cudaMemsetAsync(g_ctx.err_dev, 0, sizeof(uint32_t), g_stream));
-    LAUNCH(k_key_count, n, 256, cd.grid_hash, cd.grid_index, n, nc, B.key, B.val, B.slot, B.cnt, g_ctx.err_dev);
-    const unsigned nb = (nc + SCAN_CHUNK - 1) / SCAN_CHUNK;
-    KL(k_block_sums, nb, SCAN_TPB, B.cnt, nc, B.bsum, nullptr);
-    // cell_start is not touched by a plain sort: clear nothing (clear_all = 0, n = 0)
-    KL(k_cell_scan, nb, SCAN_TPB, B.cnt, B.bsum, nc, B.off, nullptr, nullptr, 0u, 0, nullptr);
-    LAUNCH(k_scatter, n, 256, B.key, B.slot, B.off, B.tmp, nullptr, n, nullptr);
-    LAUNCH(k_rank_pairs, n, 256, B.key, B.val, B.off, B.tmp, cd.grid_hash, cd.grid_index, n);
-    uint32_t err = 0;
-    CUDA_TRY(cudaMemcpyAsync(&err, g_ctx.err_dev, sizeof(uint32_t), cudaMemcpyDeviceToHost, g_stream));
-    CUDA_TRY(cudaStreamSynchronize(g_stream));
-    if (err) return fail(SNOWB_ERR_INVALID, "grid_hash holds keys >= num_cells");
-    return SNOWB_OK;
+    return sort_pairs(g_P.ncells, cd, n);
 }
 
 // ---------------------------------------------------------------------------
@@ -792,23 +929,13 @@ int snowb_sort_particles_static(snowb_cell_data cd, uint32_t n)
 int snowb_reorder_data(snowb_cell_data cd, const snowb_float3* old_pos, uint32_t n, uint32_t num_cells)
 {
     TRY(check_params());
-    if (!cd.cell_start || !cd.cell_end || !cd.grid_hash || !cd.grid_index || !cd.sorted_pos)
-        return fail(SNOWB_ERR_INVALID, "null pointer");
-    if (num_cells > g_P.ncells) return fail(SNOWB_ERR_INVALID, "num_cells exceeds the cell table");
-    if (num_cells) CUDA_TRY(cudaMemsetAsync(cd.cell_start, 0xff, sizeof(uint32_t) * num_cells, g_stream));
-    if (n == 0) return SNOWB_OK;
-    if (!old_pos) return fail(SNOWB_ERR_INVALID, "null pointer");
-    LAUNCH(k_reorder, n, 256, cd, old_pos, n);
-    return SNOWB_OK;
+    return reorder(g_P.ncells, cd, old_pos, n, num_cells);
 }
 
 int snowb_compute_boundary_volume(snowb_cell_data cd, float* mass, float* volume, uint32_t n)
 {
     TRY(check_params());
-    if (n == 0) return SNOWB_OK;
-    if (!mass || !volume) return fail(SNOWB_ERR_INVALID, "null pointer");
-    LAUNCH(k_boundary_volume, n, 128, g_P, cd, mass, volume, n);
-    return SNOWB_OK;
+    return boundary_volume(g_P, cd, mass, volume, nullptr, n);
 }
 
 int snowb_integrate_pbd(snowb_particle_data* particles, float dt, uint32_t n, int cd_on)
@@ -828,28 +955,7 @@ int snowb_integrate_pbd(snowb_particle_data* particles, float dt, uint32_t n, in
 int snowb_connect_and_record(snowb_particle_data* dem, uint32_t n, snowb_cell_data dcd, int dynamic)
 {
     TRY(check_params());
-    if (!dem) return fail(SNOWB_ERR_INVALID, "null pointer");
-    if (n == 0) return SNOWB_OK;
-    DevParams P = g_P;
-    if (P.gsx < 4 || P.gsy < 4 || P.gsz < 4) return fail(SNOWB_ERR_INVALID, "grid must be at least 4 cells per axis");
-    TRY(ensure_ctx(g_ctx.cap > n ? g_ctx.cap : n, g_ctx.bcap ? g_ctx.bcap : 1, P.ncells));
-    Ctx& c = g_ctx;
-    LAUNCH1(k_set_state, c.S, 0u, n, 0u);
-    CUDA_TRY(cudaMemsetAsync(c.fs, 0, sizeof(uint32_t) * P.ncells, g_stream));
-    CUDA_TRY(cudaMemsetAsync(c.fe, 0, sizeof(uint32_t) * P.ncells, g_stream));
-    LAUNCH(k_fresh_ranges, n, 256, dcd.grid_hash, n, c.fs, c.fe);
-    // this entry point reads positions from the caller's sorted_pos only
-    SetView vd = make_view(dcd, nullptr, dem->mass);
-    vd.p4 = nullptr;
-    // the view's compact copy is not available here: fill it from sorted_pos
-    LAUNCH(k_boundary_prep, n, 256, dcd, dem->mass, dem->massInv, dem->mass, n, c.s[1].p4, c.s[1].invm, c.s[1].lambda);
-    vd.p4 = c.s[1].p4;
-    LAUNCH(k_link_filter, n, 128, P, c.S, vd, *dem, dynamic, c.active);
-    for (uint32_t col = 0; col < 8; ++col)
-        LAUNCH(k_link_colour, (P.gsx / 4) * (P.gsy / 4) * (P.gsz / 4), 64, P, c.S, vd, *dem, c.fs, c.fe, c.active, col,
-               dynamic);
-    CUDA_TRY(cudaStreamSynchronize(g_stream));
-    return SNOWB_OK;
+    return connect_links(g_P, dem, n, dcd, dynamic, nullptr);
 }
 
 static snowb_step_options default_options()
@@ -892,6 +998,83 @@ int snowb_snow_simulation_ex(snowb_particle_data* sph, uint32_t* sph_size, snowb
         return fail(SNOWB_ERR_INVALID, "unknown quirk mode");
     return run_steps(sph, sph_size, dem, dem_size, boundary, boundary_size, full_size, buffer, scd, dcd, bcd, scene,
                      dt, iterations, fl, temperature_variation, o);
+}
+
+// ------------------------------------------------------------------ batched scenes
+static int batch_P(const snowb_batch* b, DevParams& P)
+{
+    TRY(check_params());
+    P = g_P;
+    return batch_layout(P, b);
+}
+
+int snowb_batch_num_cells(const snowb_batch* b, uint32_t* num_cells)
+{
+    if (!num_cells) return fail(SNOWB_ERR_INVALID, "null pointer");
+    DevParams P;
+    TRY(batch_P(b, P));
+    *num_cells = P.ncells;
+    return SNOWB_OK;
+}
+
+int snowb_batch_calculate_hash(const snowb_batch* b, snowb_cell_data cd, const snowb_float3* pos,
+                               const uint32_t* scene_of, uint32_t n)
+{
+    DevParams P;
+    TRY(batch_P(b, P));
+    if (n && !scene_of) return fail(SNOWB_ERR_INVALID, "null scene ids");
+    return calc_hash(P, cd, pos, scene_of, n);
+}
+
+int snowb_batch_sort_particles(const snowb_batch* b, snowb_cell_data cd, uint32_t n)
+{
+    DevParams P;
+    TRY(batch_P(b, P));
+    return sort_pairs(P.ncells, cd, n);
+}
+
+int snowb_batch_reorder_data(const snowb_batch* b, snowb_cell_data cd, const snowb_float3* old_pos, uint32_t n)
+{
+    DevParams P;
+    TRY(batch_P(b, P));
+    return reorder(P.ncells, cd, old_pos, n, P.ncells);
+}
+
+int snowb_batch_compute_boundary_volume(const snowb_batch* b, snowb_cell_data cd, float* mass, float* volume,
+                                        uint32_t n)
+{
+    DevParams P;
+    TRY(batch_P(b, P));
+    if (n && !b->scene_boundary) return fail(SNOWB_ERR_INVALID, "null scene ids");
+    return boundary_volume(P, cd, mass, volume, b->scene_boundary, n);
+}
+
+int snowb_batch_connect_and_record(const snowb_batch* b, snowb_particle_data* dem, uint32_t n,
+                                   snowb_cell_data dcd, int dynamic)
+{
+    DevParams P;
+    TRY(batch_P(b, P));
+    if (n && !b->scene_dem) return fail(SNOWB_ERR_INVALID, "null scene ids");
+    return connect_links(P, dem, n, dcd, dynamic, b->scene_dem);
+}
+
+int snowb_batch_snow_simulation(const snowb_batch* b, snowb_particle_data* sph, uint32_t* sph_size,
+                                snowb_particle_data* dem, uint32_t* dem_size, snowb_particle_data* boundary,
+                                uint32_t boundary_size, uint32_t full_size, snowb_particle_data* buffer,
+                                snowb_cell_data scd, snowb_cell_data dcd, snowb_cell_data bcd,
+                                snowb_scene_params* scene, float dt, int iterations, int sph_dem_correction,
+                                int sph_sph_correction, int dem_friction, int compute_temperature, int change_phase,
+                                int simulate_freezing, int simulate_melting, int dem_viscosity, int use_interlink,
+                                int dynamic_max_connections, int cd_on, float temperature_variation,
+                                const snowb_step_options* options)
+{
+    if (!b) return fail(SNOWB_ERR_INVALID, "null batch");
+    const int fl[11] = {sph_dem_correction, sph_sph_correction, dem_friction, compute_temperature, change_phase,
+                        simulate_freezing, simulate_melting, dem_viscosity, use_interlink, dynamic_max_connections,
+                        cd_on};
+    snowb_step_options o = options ? *options : default_options();
+    return run_steps(sph, sph_size, dem, dem_size, boundary, boundary_size, full_size, buffer, scd, dcd, bcd, scene,
+                     dt, iterations, fl, temperature_variation, o, b);
 }
 
 int snowb_read_sizes(uint32_t* sph_size, uint32_t* dem_size)
@@ -960,6 +1143,8 @@ int snowb_profile_begin(void)
 {
     g_prof = true;
     g_prof_used = 0;
+    g_graph.prof_replayed = false;
+    g_graph.prof_pairs = 0;
     g_acc_name.clear(); g_acc_count.clear(); g_acc_ms.clear();
     return SNOWB_OK;
 }
@@ -969,12 +1154,14 @@ int snowb_profile_end(char* out, size_t cap)
     CUDA_TRY(cudaStreamSynchronize(g_stream));
     if (g_graph.stream) CUDA_TRY(cudaStreamSynchronize(g_graph.stream));
     // launches issued directly (not through a graph) are still pending in the pool
-    if (!g_graph.valid || g_prof_used > g_graph_prof_pairs)
-        if (prof_accumulate(g_graph.valid ? g_graph_prof_pairs : 0, g_prof_used) != 0)
-            return fail(SNOWB_ERR_CUDA, "profile events");
+    const size_t done = g_graph.prof_replayed ? g_graph.prof_pairs : 0;
+    if (!g_graph.prof_replayed || g_prof_used > done)
+        if (prof_accumulate(done, g_prof_used) != 0) return fail(SNOWB_ERR_CUDA, "profile events");
     g_prof = false;
     g_prof_used = 0;
-    graph_reset();   // the profiling graph carries event nodes; recapture without them
+    g_graph.prof_replayed = false;
+    g_graph.prof_pairs = 0;
+    graph_reset(true);   // profiling graphs carry event nodes; the plain ones stay cached
     std::string txt;
     for (size_t i = 0; i < g_acc_name.size(); ++i)
         txt += g_acc_name[i] + " " + std::to_string(g_acc_count[i]) + " " + std::to_string(g_acc_ms[i]) + "\n";

@@ -51,7 +51,7 @@ struct NLWriter {
 
 // ------------------------------------------------------------ per-cell neighbour sums
 // pbf_correction (:883-929)
-__device__ __forceinline__ float3 acc_pbf_own(const DevParams& P, float3 acc, const SetView& v, float3 p, int3 g,
+__device__ __forceinline__ float3 acc_pbf_own(const DevParams& P, float3 acc, const SetView& v, float3 p, GCell g,
                                               uint32_t skip, float li, const float* lam_s, const float* lam_o,
                                               const float* con_s, const float* con_o, float dt)
 {
@@ -76,7 +76,7 @@ __device__ __forceinline__ float3 acc_pbf_own(const DevParams& P, float3 acc, co
     return acc;
 }
 // pbf_correction_boundary (:932-979)
-__device__ __forceinline__ float3 acc_pbf_bnd(const DevParams& P, float3 acc, const SetView& v, float3 p, int3 g,
+__device__ __forceinline__ float3 acc_pbf_bnd(const DevParams& P, float3 acc, const SetView& v, float3 p, GCell g,
                                               float li, const float* lam_s, const float* lam_o, float dt)
 {
     FOR27 {
@@ -99,7 +99,7 @@ __device__ __forceinline__ float3 acc_pbf_bnd(const DevParams& P, float3 acc, co
 }
 // pbf_correction_coupling (:982-1034); reference quirks: the self-skip compares indices of
 // two different sets, and s_corr is taken as 0 (it reads an uninitialised value times 0)
-__device__ __forceinline__ float3 acc_pbf_cpl(const DevParams& P, float3 acc, const SetView& v, float3 p, int3 g,
+__device__ __forceinline__ float3 acc_pbf_cpl(const DevParams& P, float3 acc, const SetView& v, float3 p, GCell g,
                                               uint32_t skip, float li, const float* lam_s, const float* lam_o,
                                               float dt)
 {
@@ -128,7 +128,7 @@ __device__ __forceinline__ float3 acc_pbf_cpl(const DevParams& P, float3 acc, co
 }
 // non-penetration: pbd_distance_correction_contrib (:1470-1527, skip) and
 // pbd_distance_correction_coupling_contrib (:1648-1705, no skip)
-__device__ __forceinline__ float3 acc_contact(const DevParams& P, float3 acc, const SetView& v, float3 p, int3 g,
+__device__ __forceinline__ float3 acc_contact(const DevParams& P, float3 acc, const SetView& v, float3 p, GCell g,
                                               uint32_t skip, float w0, const float* invm_s, const float* invm_o)
 {
     FOR27 {
@@ -154,7 +154,7 @@ __device__ __forceinline__ float3 acc_contact(const DevParams& P, float3 acc, co
 }
 // pbd_sph_sph_distance_correction (:1586-1646)
 __device__ __forceinline__ float3 acc_contact_sph(const DevParams& P, float3 acc, const SetView& v, float3 p,
-                                                  int3 g, uint32_t skip, float w0, float contrib_i,
+                                                  GCell g, uint32_t skip, float w0, float contrib_i,
                                                   const float* invm_s, const float* invm_o)
 {
     if (!(contrib_i <= 0.99f)) return add3(acc, f3(0.f, 0.f, 0.f));
@@ -270,7 +270,7 @@ __device__ __forceinline__ bool segments(const NList& L, uint32_t slot, Seg& own
 // own C and neighbour positions only, so both come out of one traversal.  Each quantity
 // keeps its own per-cell accumulation in the reference's loop order.
 template <bool LAMBDA>
-__device__ __forceinline__ void acc_WG(const DevParams& P, float& rho, float& gs, const SetView& v, float3 p, int3 g,
+__device__ __forceinline__ void acc_WG(const DevParams& P, float& rho, float& gs, const SetView& v, float3 p, GCell g,
                                        uint32_t skip, bool vol, int mode, float m_self, const float* mass_s,
                                        const float* mass_o, NLWriter* wr = nullptr, int set = 0)
 {
@@ -324,7 +324,7 @@ __global__ void __launch_bounds__(128) k_density(DevParams P, const DevState* __
             D = w ? &X.sph : &X.dem;
             lam_s = w ? ss.lambda : sd.lambda;
             o = own.gi[i];
-            float3 p = xyz(own.p4[i]); int3 g = grid_pos(P, p);
+            float3 p = xyz(own.p4[i]); GCell g = grid_pos(P, p, own.scene(i));
             rho = D->mass[o] * P.W0;
             NLWriter wr{L.e, L.stride, (w ? 0u : L.cap) + i, 0u};
             NLWriter* pw = LAMBDA ? &wr : nullptr;
@@ -340,7 +340,7 @@ __global__ void __launch_bounds__(128) k_density(DevParams P, const DevState* __
         } else {
             // boundary: density visits (b, snow, water), lambda (b, water, snow)
             i = t - ns - nd; o = vb.gi[i];
-            float3 p = xyz(vb.p4[i]); int3 g = grid_pos(P, p);
+            float3 p = xyz(vb.p4[i]); GCell g = grid_pos(P, p, vb.scene(i));
             rho = (P.rho0 * X.bnd.volume[o]) * P.W0;
             acc_WG<LAMBDA>(P, rho, gs, vb, p, g, i, true, 2, 0.f, sb.mass, X.bnd.mass);
             float unused = 0.f;
@@ -383,7 +383,7 @@ __global__ void __launch_bounds__(128) k_pbf(DevParams P, const DevState* __rest
     GRID_LOOP(t, ns + nd) {
         if (t < ns) {
             const uint32_t i = t, o = vs.gi[i];
-            float3 p = xyz(vs.p4[i]); int3 g = grid_pos(P, p);
+            float3 p = xyz(vs.p4[i]); GCell g = grid_pos(P, p, vs.scene(i));
             const float li = ss.lambda[i];
             float3 c = f3(0.f, 0.f, 0.f);
             Seg so, sx, sbn;
@@ -421,7 +421,7 @@ __global__ void __launch_bounds__(128) k_pbf(DevParams P, const DevState* __rest
         } else {
             const uint32_t i = t - ns;
             const uint32_t o = ref ? vs.gi[i] : vd.gi[i];   // Q3: SPH grid_index in the reference
-            float3 p = xyz(vd.p4[i]); int3 g = grid_pos(P, p);
+            float3 p = xyz(vd.p4[i]); GCell g = grid_pos(P, p, vd.scene(i));
             const float li = X.dem.lambda[o];
             float3 c = f3(0.f, 0.f, 0.f);
             Seg so, sx, sbn;
@@ -494,7 +494,7 @@ __global__ void __launch_bounds__(128) k_dem_corr(DevParams P, const DevState* _
     const float3 z = f3(0.f, 0.f, 0.f);
     GRID_LOOP(i, nd) {
         const uint32_t o = vd.gi[i];
-        float3 p = xyz(vd.p4[i]); int3 g = grid_pos(P, p);
+        float3 p = xyz(vd.p4[i]); GCell g = grid_pos(P, p, vd.scene(i));
         const float w0 = X.dem.massInv[o], ci = X.dem.contrib[o];
         float3 acc = ldv3(X.dem.correction, o);
         Seg so, sx, sbn;
@@ -590,7 +590,7 @@ __global__ void __launch_bounds__(128) k_friction(DevParams P, const DevState* _
         float3 p = xyz(vd.p4[i]);
         float3 op0 = ldv3(X.dem.positions, o);
         const float w0 = X.dem.massInv[o];
-        int3 g = grid_pos(P, p);
+        GCell g = grid_pos(P, p, vd.scene(i));
         float3 c = f3(0.f, 0.f, 0.f);
         FOR27 {
             float3 cs = f3(0.f, 0.f, 0.f);
@@ -697,7 +697,7 @@ __global__ void k_finalize(DevParams P, const DevState* __restrict__ S, Sets X, 
 // ======================================================================== heat
 // heat_transfer_cell (:3764-3810) over one cell
 __device__ __forceinline__ float heat_cell(const DevParams& P, const SetView& v, const snowb_particle_data& O,
-                                           int3 g, int ox, int oy, int oz, uint32_t skip, float3 p, float Ti,
+                                           GCell g, int ox, int oy, int oz, uint32_t skip, float3 p, float Ti,
                                            float kk)
 {
     float res = 0.f;
@@ -715,7 +715,7 @@ __device__ __forceinline__ float heat_cell(const DevParams& P, const SetView& v,
     return res;
 }
 __device__ __forceinline__ float heat_sum(const DevParams& P, float dT, const SetView& v, const snowb_particle_data& O,
-                                          int3 g, uint32_t skip, float3 p, float Ti, float kk)
+                                          GCell g, uint32_t skip, float3 p, float Ti, float kk)
 {
     if (P.quirks == SNOWB_QUIRKS_REFERENCE) {
         // Q7: the reference passes the particle's own cell to all 27 calls
@@ -744,7 +744,7 @@ __global__ void __launch_bounds__(128) k_heat(DevParams P, const DevState* __res
         const snowb_particle_data& A = w ? X.sph : X.dem;
         const snowb_particle_data& B = w ? X.dem : X.sph;
         const uint32_t o = own.gi[i];
-        float3 p = xyz(own.p4[i]); int3 g = grid_pos(P, p);
+        float3 p = xyz(own.p4[i]); GCell g = grid_pos(P, p, own.scene(i));
         const float Ti = A.T[o];
         float dT = 0.f;
         dT = heat_sum(P, dT, own, A, g, i, p, Ti, w ? kww : kss);
@@ -771,7 +771,7 @@ __global__ void k_heat_commit(const DevState* __restrict__ S, Sets X, float dTe,
 // xsph_viscosity_cell{,_coupling} (:3419-3502): sum of (m_j/rho_j) (v_j - v_i) W
 __device__ __forceinline__ float3 acc_xsph(const DevParams& P, float3 acc, const SetView& v,
                                            const snowb_particle_data& O, const snowb_float3* vel, float3 p,
-                                           int3 g, uint32_t skip, float3 vi)
+                                           GCell g, uint32_t skip, float3 vi)
 {
     FOR27 {
         float3 cs = f3(0.f, 0.f, 0.f);
@@ -806,7 +806,7 @@ __global__ void __launch_bounds__(128) k_xsph(DevParams P, const DevState* __res
                          : (P.quirks == SNOWB_QUIRKS_REFERENCE ? umin32(coverage(ns), nd) : nd);
     GRID_LOOP(i, limit) {
         const uint32_t o = vown.gi[i];
-        float3 p = xyz(vown.p4[i]); int3 g = grid_pos(P, p);
+        float3 p = xyz(vown.p4[i]); GCell g = grid_pos(P, p, vown.scene(i));
         float3 vi = ldv3(A.velocity, o);
         float3 c = f3(0.f, 0.f, 0.f);
         c = acc_xsph(P, c, vown, A, A.velocity, p, g, i, vi);
@@ -832,7 +832,7 @@ __device__ __forceinline__ float3 warp_ordered_sum(float3 acc, float3 part)
     return acc;
 }
 __device__ __forceinline__ float3 xsph_cell(const DevParams& P, const SetView& v, const snowb_particle_data& O,
-                                            const snowb_float3* vel, float3 p, int3 g, int ox, int oy, int oz,
+                                            const snowb_float3* vel, float3 p, GCell g, int ox, int oy, int oz,
                                             uint32_t skip, float3 vi)
 {
     float3 cs = f3(0.f, 0.f, 0.f);
@@ -868,7 +868,7 @@ __global__ void __launch_bounds__(128) k_xsph_warp(DevParams P, const DevState* 
     for (uint32_t i = warp; i < limit; i += nwarps) {
         const uint32_t o = vown.gi[i];
         const float3 p = xyz(vown.p4[i]);
-        const int3 g = grid_pos(P, p);
+        const GCell g = grid_pos(P, p, vown.scene(i));
         const float3 vi = ldv3(A.velocity, o);
         const float3 z = f3(0.f, 0.f, 0.f);
         float3 part = lane < 27 ? xsph_cell(P, vown, A, A.velocity, p, g, ox, oy, oz, i, vi) : z;
@@ -896,13 +896,13 @@ __global__ void k_xsph_commit(DevParams P, const DevState* __restrict__ S, SetVi
 // compute_boundary_volume_d (:303-346) with sph_boundary_volume (:159-192); reads the
 // caller's sorted positions directly (one-time setup).
 __global__ void k_boundary_volume(DevParams P, snowb_cell_data cd, const float* __restrict__ mass,
-                                  float* __restrict__ volume, uint32_t n)
+                                  float* __restrict__ volume, uint32_t n, const uint32_t* __restrict__ sid_o)
 {
     GRID_LOOP(i, n) {
         const uint32_t o = cd.grid_index[i];
         float3 p = ldv3(cd.sorted_pos, i);
         float rho = mass[o] * P.W0;
-        int3 g = grid_pos(P, p);
+        GCell g = grid_pos(P, p, sid_o ? sid_o[o] : 0u);
         FOR27 {
             float cs = 0.f;
             uint32_t h = grid_hash(P, g, ox, oy, oz);
@@ -924,7 +924,8 @@ __global__ void k_boundary_volume(DevParams P, snowb_cell_data cd, const float* 
 // compact sorted view of the boundary set: p4 = (pos, volume), invm/mass by sorted index
 __global__ void k_boundary_prep(snowb_cell_data cd, const float* __restrict__ volume, const float* __restrict__ invm,
                                 const float* __restrict__ mass, uint32_t n, float4* __restrict__ p4,
-                                float* __restrict__ invm_s, float* __restrict__ mass_s)
+                                float* __restrict__ invm_s, float* __restrict__ mass_s,
+                                const uint32_t* __restrict__ sid_o, uint32_t* __restrict__ sid_s)
 {
     GRID_LOOP(i, n) {
         const uint32_t o = cd.grid_index[i];
@@ -932,6 +933,7 @@ __global__ void k_boundary_prep(snowb_cell_data cd, const float* __restrict__ vo
         p4[i] = make_float4(q.x, q.y, q.z, volume[o]);
         invm_s[i] = invm[o];
         mass_s[i] = mass[o];
+        if (sid_s) sid_s[i] = sid_o[o];
     }
 }
 __global__ void k_set_state(DevState* S, uint32_t ns, uint32_t nd, uint32_t nb)
@@ -940,6 +942,18 @@ __global__ void k_set_state(DevState* S, uint32_t ns, uint32_t nd, uint32_t nb)
         S->n_sph = ns; S->n_dem = nd; S->n_b = nb;
         S->n0_sph = ns; S->n0_dem = nd;
         S->n_freeze = 0; S->n_melt = 0; S->changed = 0; S->new_sph = ns; S->new_dem = nd;
+    }
+}
+// batched runs: every live slot's scene id must name a scene of the batch
+__global__ void k_check_scenes(DevParams P, DevState* S, const uint32_t* __restrict__ sph,
+                               const uint32_t* __restrict__ dem, const uint32_t* __restrict__ bnd)
+{
+    const uint32_t ns = S->n_sph, nd = S->n_dem, nb = S->n_b;
+    const uint32_t n = ns > nd ? (ns > nb ? ns : nb) : (nd > nb ? nd : nb);
+    GRID_LOOP(i, n) {
+        bool bad = (i < ns && sph[i] > P.scene_mask) || (i < nd && dem[i] > P.scene_mask) ||
+                   (i < nb && bnd[i] > P.scene_mask);
+        if (bad) atomicOr(&S->err, SNOWB_DEVERR_SCENE);
     }
 }
 __global__ void k_begin_substep(DevState* S)

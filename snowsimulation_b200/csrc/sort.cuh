@@ -71,13 +71,13 @@ __device__ __forceinline__ uint32_t prefix_of_blocks(const uint32_t* bsum, uint3
 // Fused path: hash of pos[o] for o < n (calcHashD :194-212).
 __global__ void k_hash_count(DevParams P, const snowb_float3* __restrict__ pos, const uint32_t* n_ptr,
                              uint32_t n_fixed, uint32_t* __restrict__ key_o, uint32_t* __restrict__ slot_o,
-                             uint32_t* __restrict__ cnt, const uint32_t* cond)
+                             uint32_t* __restrict__ cnt, const uint32_t* cond, const uint32_t* __restrict__ sid_o)
 {
     if (cond && *cond == 0) return;
     const uint32_t n = n_ptr ? *n_ptr : n_fixed;
     GRID_LOOP(o, n) {
         float3 p = ldv3(pos, o);
-        uint32_t h = grid_hash(P, grid_pos(P, p), 0, 0, 0);
+        uint32_t h = grid_hash(P, grid_pos(P, p, sid_o ? sid_o[o] : 0u), 0, 0, 0);
         key_o[o] = h;
         slot_o[o] = atomicAdd(cnt + h, 1u);
     }
@@ -181,7 +181,8 @@ __global__ void k_rank_reorder(const uint32_t* __restrict__ key_o, const uint32_
                                const float* __restrict__ w, const float* __restrict__ invm,
                                const float* __restrict__ contrib, snowb_cell_data cd, float4* __restrict__ p4,
                                float* __restrict__ invm_s, float* __restrict__ contrib_s,
-                               const uint32_t* n_ptr, uint32_t n_fixed, const uint32_t* cond)
+                               const uint32_t* n_ptr, uint32_t n_fixed, const uint32_t* cond,
+                               const uint32_t* __restrict__ sid_o, uint32_t* __restrict__ sid_s)
 {
     if (cond && *cond == 0) return;
     const uint32_t n = n_ptr ? *n_ptr : n_fixed;
@@ -197,6 +198,7 @@ __global__ void k_rank_reorder(const uint32_t* __restrict__ key_o, const uint32_
         if (p4) p4[p] = make_float4(q.x, q.y, q.z, w ? w[o] : 0.f);
         if (invm_s) invm_s[p] = invm[o];
         if (contrib_s) contrib_s[p] = contrib[o];
+        if (sid_s) sid_s[p] = sid_o[o];
     }
 }
 // sort_particles path: write the sorted keys and values only.
@@ -213,11 +215,12 @@ __global__ void k_rank_pairs(const uint32_t* __restrict__ key_o, const uint32_t*
 }
 
 // calcHashD (:194-212) alone
-__global__ void k_calc_hash(DevParams P, snowb_cell_data cd, const snowb_float3* __restrict__ pos, uint32_t n)
+__global__ void k_calc_hash(DevParams P, snowb_cell_data cd, const snowb_float3* __restrict__ pos, uint32_t n,
+                            const uint32_t* __restrict__ sid_o)
 {
     GRID_LOOP(i, n) {
         float3 p = ldv3(pos, i);
-        cd.grid_hash[i] = grid_hash(P, grid_pos(P, p), 0, 0, 0);
+        cd.grid_hash[i] = grid_hash(P, grid_pos(P, p, sid_o ? sid_o[i] : 0u), 0, 0, 0);
         cd.grid_index[i] = i;
     }
 }

@@ -13,6 +13,8 @@ Mirrors, with a seeded PRNG instead of std::rand(time(NULL)):
 Buffers the reference leaves uninitialised get a defined value here: cell_start is
 all-empty, cell_end 0, grid_index the identity, contrib 1 in the padding.
 """
+import functools
+import math
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -100,6 +102,11 @@ def lattice(counts, spacing, origin_min, jitter=0.0, rng=None):
 
 def boundary_box(particle_radius):
     """InitializeBoundaryParticles (Simulation.cpp:425-556) in float32 arithmetic."""
+    return _boundary_box(float(np.float32(particle_radius))).copy()
+
+
+@functools.lru_cache(maxsize=4)
+def _boundary_box(particle_radius):
     f = np.float32
     thickness = 1
     d = f(2.0) * f(particle_radius)
@@ -242,6 +249,28 @@ def tiny(seed=0, water=(4, 4, 4), snow=(6, 4, 6), drop=0.06, **kw):
     """A small scene that the FP32/FP64 oracle steps through in well under a second."""
     return scene_drop(water, snow, seed=seed, water_jitter=0.002, snow_jitter=0.002,
                       drop_height=drop, name="tiny", **kw)
+
+
+def config2(seed=0, n_scenes=64, lo=2000, hi=40000):
+    """Scenes for a batched run: particle counts log-uniform in [lo, hi] per scene, water
+    fraction uniform in 0.02-0.3, drop height uniform in 0.1-0.5 m, snow temperature uniform
+    in -20..-2 C (water 100 C); each block is the nearest cube lattice (spacing 0.02 m,
+    jitter +-2 mm), snow resting on the floor with initial interlinks.  Returns a list of
+    HostWorlds sharing one SimParams."""
+    rng = np.random.default_rng(seed)
+    p = make_sim_params()
+    worlds = []
+    for s in range(n_scenes):
+        n = math.exp(rng.uniform(math.log(lo), math.log(hi)))
+        frac = rng.uniform(0.02, 0.3)
+        drop = rng.uniform(0.1, 0.5)
+        t_snow = rng.uniform(-20.0, -2.0)
+        kw = max(1, int(round((n * frac) ** (1.0 / 3.0))))
+        ks = max(1, int(round((n * (1.0 - frac)) ** (1.0 / 3.0))))
+        worlds.append(scene_drop((kw, kw, kw), (ks, ks, ks), seed=seed * 1000 + s, water_jitter=0.002,
+                                 snow_jitter=0.002, drop_height=drop, T_snow=float(np.float32(t_snow)),
+                                 params=p, name="config2 scene %d" % s, init_links=True))
+    return worlds
 
 
 SCENES = {"config0": config0, "config1": config1, "tiny": tiny}
