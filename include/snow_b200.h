@@ -241,6 +241,37 @@ int snowb_batch_snow_simulation(const snowb_batch* batch,
                                 int dynamic_max_connections, int cd_on, float temperature_variation,
                                 const snowb_step_options* options);
 
+/* ---- adjoint of the substep (no reference counterpart) -------------------------------
+ * Reverse-mode derivatives of snowb_snow_simulation_ex substeps in the fixed quirk mode,
+ * with the forward pass's discrete decisions held fixed (neighbour sets, interlink
+ * topology and breaking, C > 0, friction branch, wall and speed clamps).  Between
+ * snowb_adjoint_begin and snowb_adjoint_end every substep is recorded (requirements: fixed
+ * quirks, no graph, sph_sph_correction and dynamic links off, scorr_coeff 0, no phase
+ * change and contrib 1 while recording; sizes and iterations constant).  The tape holds
+ * about (30 + 8 x iterations x maximum_connection) bytes per particle slot per substep;
+ * hosts bound it by checkpointing (record a segment, run its backward, re-record the
+ * previous segment from a saved state). */
+typedef struct snowb_adjoint_io {
+    /* device arrays in original index order, in: adjoint of the state after the last
+     * recorded substep; out: adjoint of the state before the first */
+    float *gx_sph, *gv_sph, *gT_sph;   /* positions (n x 3), velocities (n x 3), temperatures (n) */
+    float *gx_dem, *gv_dem, *gT_dem;
+    float* gL_dem;   /* interlink rest lengths (connect_length, n_dem x maximum_connection); a
+                        length depends on the positions where its link formed, so its
+                        adjoint travels back to that substep */
+    /* host, accumulated: dL/d k_refreezing (interlink stiffness), k_stretch (water-snow
+     * contact), k_water, k_snow (conductivities) */
+    double grad_params[4];
+} snowb_adjoint_io;
+
+int snowb_adjoint_begin(void);
+/* Stop recording; *substeps = number of substeps on the tape. */
+int snowb_adjoint_end(uint32_t* substeps);
+/* Reverse pass over the recorded substeps (last to first); empties the tape. */
+int snowb_adjoint_backward(snowb_adjoint_io* io);
+/* Free the tape and the reverse pass's buffers. */
+int snowb_adjoint_release(void);
+
 /* Set sizes kept on the device by the last call with options->sync = 0 (blocks). */
 int snowb_read_sizes(uint32_t* sph_size, uint32_t* dem_size);
 

@@ -12,6 +12,13 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libsnowb200.so")
 
 
+class AdjointIO(C.Structure):
+    """snowb_adjoint_io: device gradient buffers (in/out) and the accumulated parameter gradients."""
+    _fields_ = [("gx_sph", C.c_void_p), ("gv_sph", C.c_void_p), ("gT_sph", C.c_void_p),
+                ("gx_dem", C.c_void_p), ("gv_dem", C.c_void_p), ("gT_dem", C.c_void_p),
+                ("gL_dem", C.c_void_p), ("grad_params", C.c_double * 4)]
+
+
 class StepOptions(C.Structure):
     _fields_ = [("quirks", C.c_int), ("substeps", C.c_int), ("stop_after", C.c_int),
                 ("use_graph", C.c_int), ("sync", C.c_int)]
@@ -29,6 +36,7 @@ EXPORTS = (
     "snowb_batch_num_cells", "snowb_batch_calculate_hash", "snowb_batch_sort_particles",
     "snowb_batch_reorder_data", "snowb_batch_compute_boundary_volume", "snowb_batch_connect_and_record",
     "snowb_batch_snow_simulation",
+    "snowb_adjoint_begin", "snowb_adjoint_end", "snowb_adjoint_backward", "snowb_adjoint_release",
 )
 
 _lib = None
@@ -83,6 +91,10 @@ def load(path=LIB_PATH):
         "snowb_batch_compute_boundary_volume": [PB, CD, C.c_void_p, C.c_void_p, u32],
         "snowb_batch_connect_and_record": [PB, PPD, u32, CD, i],
         "snowb_batch_snow_simulation": [PB] + sig["snowb_snow_simulation_ex"],
+        "snowb_adjoint_begin": [],
+        "snowb_adjoint_end": [pu32],
+        "snowb_adjoint_backward": [C.POINTER(AdjointIO)],
+        "snowb_adjoint_release": [],
     })
     for name, args in sig.items():
         fn = getattr(lib, name)

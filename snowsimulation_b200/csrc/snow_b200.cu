@@ -18,6 +18,7 @@
 #include "sort.cuh"
 #include "solver.cuh"
 #include "phase.cuh"
+#include "adjoint.cuh"
 
 namespace snowb {
 
@@ -343,6 +344,119 @@ struct StepArgs {
     uint32_t* sid_buf;
 };
 
+
+// ------------------------------------------------------------------ adjoint tape
+// While recording (snowb_adjoint_begin .. snowb_adjoint_end) every substep saves what its
+// reverse needs: the state at its start, the positions after integration, the input
+// and corrected positions of every solver iteration with the interlink records seen by
+// that iteration, and the velocities after finalize and after the water XSPH.  Sizes
+// are those of the recorded substeps (no phase change may happen while recording).
+struct TapeStep {
+    std::vector<void*> bufs;
+    float *x0[2], *v0[2], *T0[2], *x0p[2], *vf[2], *vw1;
+    std::vector<float*> xit[2], xmid[2];
+    std::vector<uint32_t*> rec;
+    std::vector<float*> len;
+    uint32_t* rec_pre;   // records at the substep's start (before link formation)
+};
+struct Tape {
+    bool recording = false;
+    std::vector<TapeStep> steps;   // allocated entries, reused across recordings
+    size_t used = 0;
+    uint32_t full = 0, n[2] = {0, 0}, nb = 0, maxc = 0;
+    int iterations = 0;
+    int device = -1;
+    // forward context of the recorded substeps
+    snowb_particle_data sph{}, dem{}, bnd{};
+    snowb_cell_data bcd{};
+    DevParams P{};
+    float dt = 0.f;
+    int friction = 0, temperature = 0, correct_dem = 0, interlink = 0, dem_visc = 0, cd_on = 0;
+    uint32_t* viol = nullptr;      // device flag: a phase change or contrib != 1 while recording
+};
+static Tape g_tape;
+
+static void tape_free_steps()
+{
+    for (auto& st : g_tape.steps)
+        for (void* p : st.bufs) cudaFree(p);
+    g_tape.steps.clear();
+    g_tape.used = 0;
+}
+static int tape_alloc_step(TapeStep& T)
+{
+    const size_t f3n = (size_t)g_tape.full * 3, f1n = g_tape.full;
+    auto F = [&](float** p, size_t n) -> int { TRY(dalloc(p, n)); T.bufs.push_back(*p); return SNOWB_OK; };
+    for (int s = 0; s < 2; ++s) {
+        TRY(F(&T.x0[s], f3n)); TRY(F(&T.v0[s], f3n)); TRY(F(&T.T0[s], f1n)); TRY(F(&T.x0p[s], f3n));
+        TRY(F(&T.vf[s], f3n));
+        T.xit[s].assign(g_tape.iterations, nullptr);
+        T.xmid[s].assign(g_tape.iterations, nullptr);
+        for (int it = 0; it < g_tape.iterations; ++it) { TRY(F(&T.xit[s][it], f3n)); TRY(F(&T.xmid[s][it], f3n)); }
+    }
+    TRY(F(&T.vw1, f3n));
+    TRY(dalloc(&T.rec_pre, (size_t)g_tape.full * g_tape.maxc)); T.bufs.push_back(T.rec_pre);
+    T.rec.assign(g_tape.iterations, nullptr);
+    T.len.assign(g_tape.iterations, nullptr);
+    for (int it = 0; it < g_tape.iterations; ++it) {
+        TRY(dalloc(&T.rec[it], (size_t)g_tape.full * g_tape.maxc)); T.bufs.push_back(T.rec[it]);
+        TRY(F(&T.len[it], (size_t)g_tape.full * g_tape.maxc));
+    }
+    return SNOWB_OK;
+}
+static int tape_copy(void* dst, const void* src, size_t bytes)
+{
+    if (bytes) CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, g_stream));
+    return SNOWB_OK;
+}
+// kind: 0 substep start, 1 after integration, 2 iteration start, 3 after the iteration's
+// apply, 4 after finalize, 5 after the water XSPH, 6 substep end
+static int tape_hook(const StepArgs& a, int kind, int it)
+{
+    Tape& tp = g_tape;
+    if (kind == 0 && tp.used == tp.steps.size()) {
+        tp.steps.emplace_back();
+        TRY(tape_alloc_step(tp.steps.back()));
+    }
+    TapeStep& T = tp.steps[tp.used];
+    const size_t b3[2] = {(size_t)tp.n[0] * 12, (size_t)tp.n[1] * 12};
+    const snowb_particle_data* D[2] = {a.sph, a.dem};
+    switch (kind) {
+    case 0:
+        for (int s = 0; s < 2; ++s) {
+            TRY(tape_copy(T.x0[s], D[s]->positions, b3[s]));
+            TRY(tape_copy(T.v0[s], D[s]->velocity, b3[s]));
+            TRY(tape_copy(T.T0[s], D[s]->T, (size_t)tp.n[s] * 4));
+        }
+        TRY(tape_copy(T.rec_pre, a.dem->connect_record, (size_t)tp.n[1] * tp.maxc * 4));
+        LAUNCH(ka_check_contrib, tp.n[0] + tp.n[1], 256, tp.n[0], tp.n[1], a.sph->contrib, a.dem->contrib, tp.viol);
+        break;
+    case 1:
+        for (int s = 0; s < 2; ++s) TRY(tape_copy(T.x0p[s], D[s]->positions, b3[s]));
+        break;
+    case 2:
+        for (int s = 0; s < 2; ++s) TRY(tape_copy(T.xit[s][it], D[s]->predict_positions, b3[s]));
+        TRY(tape_copy(T.rec[it], a.dem->connect_record, (size_t)tp.n[1] * tp.maxc * 4));
+        TRY(tape_copy(T.len[it], a.dem->connect_length, (size_t)tp.n[1] * tp.maxc * 4));
+        break;
+    case 3:
+        for (int s = 0; s < 2; ++s) TRY(tape_copy(T.xmid[s][it], D[s]->predict_positions, b3[s]));
+        break;
+    case 4:
+        for (int s = 0; s < 2; ++s) TRY(tape_copy(T.vf[s], D[s]->velocity, b3[s]));
+        break;
+    case 5:
+        TRY(tape_copy(T.vw1, a.sph->velocity, b3[0]));
+        break;
+    case 6:
+        LAUNCH1(ka_check_phase, g_ctx.S, tp.viol);
+        ++tp.used;
+        break;
+    }
+    return SNOWB_OK;
+}
+#define TAPE_HOOK(kind, it) do { if (g_tape.recording) TRY(tape_hook(a, (kind), (it))); } while (0)
+
 // One substep (cuda_simulation.cu:4861-5157) given step flags derived from the scene time.
 // Returns SNOWB_OK; stops early after stage `stop_after` (0 = complete).
 static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool step_dem)
@@ -376,6 +490,7 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
     };
 #define STOP(k) do { if (a.stop_after == (k)) return SNOWB_OK; } while (0)
 
+    TAPE_HOOK(0, 0);
     LAUNCH1(k_begin_substep, S);
     TRY(sort_if(1, nullptr));
     TRY(sort_if(0, nullptr));
@@ -427,11 +542,13 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
         if (step_sph) dirty_s = true;
         if (step_dem) dirty_d = true;
     }
+    TAPE_HOOK(1, 0);
     STOP(7);
     for (int it = 0; it < a.iterations; ++it) {
         const int base = 10 + 10 * it;
         TRY(sort_if(1, nullptr));
         TRY(sort_if(0, nullptr));
+        TAPE_HOOK(2, it);
         STOP(base + 0);
         // density + lambda in one pass (stage boundaries base+1 and base+2 coincide)
         LAUNCH(k_density<true>, work3, 128, P, S, vs, vd, vb, X, ss, sd, sb, NL);
@@ -446,6 +563,7 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
             if (step_sph) dirty_s = true;
             if (step_dem) dirty_d = true;
         }
+        TAPE_HOOK(3, it);
         STOP(base + 6);
         if (a.friction && step_dem) {
             TRY(sort_if(1, nullptr));
@@ -458,17 +576,260 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
     }
     if (step_sph || step_dem)
         LAUNCH(k_finalize, 2 * full, 256, P, S, X, a.dt, step_sph ? 1 : 0, step_dem ? 1 : 0);
+    TAPE_HOOK(4, 0);
     STOP(90);
     // apply_XSPH_viscosity (:3663-3711), Jacobi
     if (step_sph) {
         LAUNCH(k_xsph_warp, (uint64_t)full * 32, 128, P, S, vs, vd, *a.sph, *a.dem, 1, P.sph_visc, c.tmp_vel);
         LAUNCH(k_xsph_commit, full, 256, P, S, vs, 1, c.tmp_vel, a.sph->velocity);
     }
+    TAPE_HOOK(5, 0);
     if (a.dem_visc && step_dem) {
         LAUNCH(k_xsph_warp, (uint64_t)full * 32, 128, P, S, vd, vs, *a.dem, *a.sph, 0, P.dem_visc, c.tmp_vel);
         LAUNCH(k_xsph_commit, full, 256, P, S, vd, 0, c.tmp_vel, a.dem->velocity);
     }
+    TAPE_HOOK(6, 0);
 #undef STOP
+    return SNOWB_OK;
+}
+
+
+// ------------------------------------------------------------------ adjoint: recording
+// Checks of a call made while recording; the first recorded call fixes the context.
+static int tape_start_call(const DevParams& P, snowb_particle_data* sph, uint32_t ns, snowb_particle_data* dem,
+                           uint32_t nd, snowb_particle_data* bnd, uint32_t nb, uint32_t full, snowb_cell_data bcd,
+                           float dt, int iterations, const int* fl, const snowb_step_options& opt,
+                           const snowb_batch* batch)
+{
+    Tape& tp = g_tape;
+    if (opt.quirks != SNOWB_QUIRKS_FIXED) return fail(SNOWB_ERR_INVALID, "adjoint recording needs SNOWB_QUIRKS_FIXED");
+    if (opt.use_graph || opt.stop_after || batch)
+        return fail(SNOWB_ERR_INVALID, "adjoint recording runs plain substeps (no graph, no stop, no batch)");
+    // flags: sph_dem, sph_sph, friction, temperature, change_phase, freezing, melting, dem_visc,
+    // interlink, dynamic, cd_on
+    if (fl[1] || fl[9]) return fail(SNOWB_ERR_INVALID, "adjoint: sph_sph_correction and dynamic links must be off");
+    if (P.scorr_coeff != 0.f) return fail(SNOWB_ERR_INVALID, "adjoint: scorr_coeff must be 0");
+    if (iterations < 1) return fail(SNOWB_ERR_INVALID, "adjoint: at least one iteration");
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    const bool first = tp.used == 0;
+    const bool same = tp.device == dev && tp.full == full && tp.n[0] == ns && tp.n[1] == nd && tp.nb == nb &&
+                      tp.maxc == P.maxc && tp.iterations == iterations;
+    if (!first && !same) return fail(SNOWB_ERR_INVALID, "adjoint: recorded calls must keep sizes and iterations");
+    if (first && !same) {
+        tape_free_steps();
+        tp.device = dev; tp.full = full; tp.n[0] = ns; tp.n[1] = nd; tp.nb = nb; tp.maxc = P.maxc;
+        tp.iterations = iterations;
+    }
+    if (!tp.viol) {
+        TRY(dalloc(&tp.viol, 1));
+        CUDA_TRY(cudaMemset(tp.viol, 0, sizeof(uint32_t)));
+    }
+    tp.sph = *sph; tp.dem = *dem; tp.bnd = *bnd; tp.bcd = bcd; tp.P = P; tp.dt = dt;
+    tp.correct_dem = fl[0]; tp.friction = fl[2]; tp.temperature = fl[3]; tp.dem_visc = fl[7];
+    tp.interlink = fl[8]; tp.cd_on = fl[10];
+    return SNOWB_OK;
+}
+
+// ------------------------------------------------------------------ adjoint: reverse pass
+struct AdjBufs {
+    int device = -1;
+    uint32_t cap = 0, bcap = 0, ncells = 0;
+    snowb_cell_data cd[2] = {};
+    SetBufs sb[2];
+    float4* bp4 = nullptr;
+    float *binvm = nullptr, *bmass = nullptr;
+    float* f[3][7] = {};            // rho, C, S, lam, lamb, rhob, Sb
+    float *XB[2] = {}, *U[2] = {}, *X0B[2] = {}, *VB[2] = {}, *XBX[2] = {}, *XH[2] = {}, *T0B[2] = {};
+    float* GVW = nullptr;
+    uint32_t* nbuf = nullptr;
+    double* gp = nullptr;
+    std::vector<void*> bufs;
+};
+static AdjBufs g_adj;
+
+static void adj_free()
+{
+    for (auto& s : g_adj.sb) free_set(s);
+    for (void* p : g_adj.bufs) cudaFree(p);
+    g_adj = AdjBufs();
+}
+static int adj_ensure(uint32_t cap, uint32_t bcap, uint32_t ncells)
+{
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    AdjBufs& B = g_adj;
+    if (B.device == dev && B.cap >= cap && B.bcap >= bcap && B.ncells == ncells) return SNOWB_OK;
+    adj_free();
+    B.device = dev; B.cap = cap; B.bcap = bcap; B.ncells = ncells;
+    auto A = [&](auto** p, size_t n) -> int { TRY(dalloc(p, n)); B.bufs.push_back(*p); return SNOWB_OK; };
+    for (int s = 0; s < 2; ++s) {
+        TRY(alloc_sort(B.sb[s], cap, ncells, true));
+        TRY(A(&B.cd[s].grid_hash, cap)); TRY(A(&B.cd[s].grid_index, cap));
+        TRY(A(&B.cd[s].cell_start, ncells)); TRY(A(&B.cd[s].cell_end, ncells));
+        TRY(A(&B.cd[s].sorted_pos, cap));
+        for (float** q : {&B.XB[s], &B.U[s], &B.X0B[s], &B.VB[s], &B.XBX[s], &B.XH[s]}) TRY(A(q, (size_t)cap * 3));
+        TRY(A(&B.T0B[s], cap));
+    }
+    for (int s = 0; s < 3; ++s)
+        for (int k = 0; k < 7; ++k) TRY(A(&B.f[s][k], s == 2 ? bcap : cap));
+    TRY(A(&B.bp4, bcap)); TRY(A(&B.binvm, bcap)); TRY(A(&B.bmass, bcap));
+    TRY(A(&B.GVW, (size_t)cap * 3));
+    TRY(A(&B.nbuf, 4)); TRY(A(&B.gp, 4));
+    return SNOWB_OK;
+}
+static inline snowb_float3* F3(float* p) { return reinterpret_cast<snowb_float3*>(p); }
+static inline const snowb_float3* F3(const float* p) { return reinterpret_cast<const snowb_float3*>(p); }
+static int zero(void* p, size_t bytes)
+{
+    if (bytes) CUDA_TRY(cudaMemsetAsync(p, 0, bytes, g_stream));
+    return SNOWB_OK;
+}
+static int dcopy(void* dst, const void* src, size_t bytes)
+{
+    if (bytes) CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, g_stream));
+    return SNOWB_OK;
+}
+
+// reverse of one recorded substep; gx/gv/gT (per set) hold the adjoint of the state after
+// it on entry and the adjoint of the state before it on return
+static int adj_substep(const TapeStep& T, float* const gx[2], float* const gv[2], float* const gT[2], float* gL)
+{
+    Tape& tp = g_tape;
+    AdjBufs& B = g_adj;
+    const DevParams& P = tp.P;
+    const uint32_t n[2] = {tp.n[0], tp.n[1]}, nw = n[0], ns = n[1], nb = tp.nb, cap = B.cap;
+    const size_t b3[2] = {(size_t)nw * 12, (size_t)ns * 12};
+    const int last = tp.iterations - 1;
+    Sets X{tp.sph, tp.dem, tp.bnd};
+    AdjField F[3];
+    for (int s = 0; s < 3; ++s)
+        F[s] = AdjField{B.f[s][0], B.f[s][1], B.f[s][2], B.f[s][3], B.f[s][4], B.f[s][5], B.f[s][6]};
+    const size_t fb[3] = {(size_t)nw * 4, (size_t)ns * 4, (size_t)nb * 4};
+    AdjParams G{B.gp};
+    SetView vw = make_view(B.cd[0], B.sb[0].p4, tp.sph.mass);
+    SetView vs = make_view(B.cd[1], B.sb[1].p4, tp.dem.mass);
+    SetView vb = make_view(tp.bcd, B.bp4, tp.bnd.volume);
+    auto sort2 = [&](const float* pw, const float* ps) -> int {
+        snowb_particle_data dw = tp.sph, ds = tp.dem;
+        dw.predict_positions = const_cast<snowb_float3*>(F3(pw));
+        ds.predict_positions = const_cast<snowb_float3*>(F3(ps));
+        TRY(sort_set(P, B.sb[0], dw, B.cd[0], B.nbuf + 0, cap, nullptr, true));
+        TRY(sort_set(P, B.sb[1], ds, B.cd[1], B.nbuf + 1, cap, nullptr, true));
+        return SNOWB_OK;
+    };
+    auto zero_rhob = [&]() -> int {
+        for (int s = 0; s < 3; ++s) TRY(zero(F[s].rhob, fb[s]));
+        return SNOWB_OK;
+    };
+    auto fields = [&]() -> int {
+        LAUNCH(ka_fields, nw + ns + nb, 128, P, nw, ns, nb, vw, vs, vb, X, F[0], F[1], F[2]);
+        return SNOWB_OK;
+    };
+    // 1. fields at the last iteration's input positions (densities read by the XSPH)
+    TRY(sort2(T.xit[0][last], T.xit[1][last]));
+    TRY(fields());
+    TRY(zero_rhob());
+    // 2. XSPH at the positions of the last sort (after the friction pass's sort)
+    const float* xx[2] = {tp.friction ? T.xmid[0][last] : T.xit[0][last],
+                          tp.friction ? T.xmid[1][last] : T.xit[1][last]};
+    if (tp.friction) TRY(sort2(xx[0], xx[1]));
+    for (int s = 0; s < 2; ++s) { TRY(zero(B.VB[s], b3[s])); TRY(zero(B.XBX[s], b3[s])); }
+    TRY(dcopy(B.GVW, gv[0], b3[0]));
+    if (tp.dem_visc)
+        LAUNCH(ka_xsph_rev, ns + nw, 128, P, ns, nw, vs, vw, F3(T.vf[1]), F3(T.vw1), tp.dem.mass, tp.sph.mass,
+               F[1].rho, F[0].rho, P.dem_visc, F3(gv[1]), F3(B.VB[1]), F3(B.GVW), F3(B.XBX[1]), F3(B.XBX[0]),
+               F[1].rhob, F[0].rhob);
+    else
+        TRY(dcopy(B.VB[1], gv[1], b3[1]));
+    LAUNCH(ka_xsph_rev, nw + ns, 128, P, nw, ns, vw, vs, F3(T.vf[0]), F3(T.vf[1]), tp.sph.mass, tp.dem.mass, F[0].rho,
+           F[1].rho, P.sph_visc, F3(B.GVW), F3(B.VB[0]), F3(B.VB[1]), F3(B.XBX[0]), F3(B.XBX[1]), F[0].rhob,
+           F[1].rhob);
+    // 3. finalize: x = x_new, v = (x_new - x0p)/dt
+    for (int s = 0; s < 2; ++s) {
+        TRY(dcopy(B.XB[s], gx[s], b3[s]));
+        TRY(zero(B.X0B[s], b3[s]));
+        LAUNCH(ka_finalize_rev, n[s], 256, n[s], tp.dt, F3(B.VB[s]), F3(B.XB[s]), F3(B.X0B[s]));
+    }
+    AdjSet AW{F3(B.XB[0]), F3(B.U[0]), F3(B.X0B[0]), F3(T.x0p[0])};
+    AdjSet AS{F3(B.XB[1]), F3(B.U[1]), F3(B.X0B[1]), F3(T.x0p[1])};
+    // 4. solver iterations, last to first
+    for (int it = last; it >= 0; --it) {
+        if (tp.friction) {
+            if (it != last) TRY(sort2(T.xmid[0][it], T.xmid[1][it]));
+            LAUNCH(ka_scale3, ns, 256, ns, F3(B.U[1]), P.sor, F3(B.XB[1]));
+            LAUNCH(ka_friction_rev, ns, 128, P, ns, nb, vs, vb, X, AS);
+        }
+        if (it == last && tp.friction)
+            for (int s = 0; s < 2; ++s) LAUNCH(ka_axpy3, n[s], 256, n[s], F3(B.XB[s]), F3(B.XB[s]), 1.f, F3(B.XBX[s]));
+        TRY(sort2(T.xit[0][it], T.xit[1][it]));
+        TRY(fields());
+        for (int s = 0; s < 2; ++s) LAUNCH(ka_scale3, n[s], 256, n[s], F3(B.U[s]), P.sor, F3(B.XB[s]));
+        LAUNCH(ka_pbf_lambar, nw + ns + nb, 128, P, nw, ns, nb, vw, vs, vb, X, F[0], F[1], F[2], AW);
+        LAUNCH(ka_pos_rev, nw + ns, 128, P, nw, ns, nb, vw, vs, vb, X, F[0], F[1], F[2], AW, AS, G, 1,
+               tp.correct_dem);
+        if (tp.interlink)
+            LAUNCH(ka_interlink_rev, ns, 128, P, ns, F3(T.xit[1][it]), T.rec[it], T.len[it], tp.dem.massInv, AS, G,
+                   gL);
+        if (it == last && !tp.friction)
+            for (int s = 0; s < 2; ++s) LAUNCH(ka_axpy3, n[s], 256, n[s], F3(B.XB[s]), F3(B.XB[s]), 1.f, F3(B.XBX[s]));
+        TRY(zero_rhob());
+    }
+    // 5. heat and link formation at the substep's start positions
+    for (int s = 0; s < 2; ++s) TRY(zero(B.XH[s], b3[s]));
+    if (tp.interlink)
+        LAUNCH(ka_linkform_rev, ns, 128, P, ns, F3(T.x0[1]), T.rec_pre, T.rec[0], gL, F3(B.XH[1]));
+    if (tp.temperature) {
+        TRY(sort2(T.x0[0], T.x0[1]));
+        TRY(fields());
+        AdjSet HW{F3(B.XH[0]), F3(B.U[0]), F3(B.X0B[0]), F3(T.x0p[0])};
+        AdjSet HS{F3(B.XH[1]), F3(B.U[1]), F3(B.X0B[1]), F3(T.x0p[1])};
+        LAUNCH(ka_heat_rev, nw + ns, 128, P, nw, ns, vw, vs, X, T.T0[0], T.T0[1], gT[0], gT[1], B.T0B[0], B.T0B[1],
+               F[0], F[1], HW, HS, G, tp.dt);
+        LAUNCH(ka_pos_rev, nw + ns, 128, P, nw, ns, nb, vw, vs, vb, X, F[0], F[1], F[2], HW, HS, G, 0, 0);
+        TRY(zero_rhob());
+        for (int s = 0; s < 2; ++s) TRY(dcopy(gT[s], B.T0B[s], fb[s]));
+    }
+    // 6. integration (velocity adjoint written to gv, positions added to XH)
+    for (int s = 0; s < 2; ++s) {
+        LAUNCH(ka_integrate_rev, n[s], 256, P, n[s], tp.dt, tp.cd_on, F3(T.x0[s]), F3(T.v0[s]), F3(B.XB[s]),
+               F3(B.X0B[s]), F3(B.XH[s]), F3(gv[s]));
+        TRY(dcopy(gx[s], B.XH[s], b3[s]));
+    }
+    return SNOWB_OK;
+}
+
+static int adjoint_backward(const snowb_adjoint_io* io)
+{
+    Tape& tp = g_tape;
+    if (tp.recording) return fail(SNOWB_ERR_INVALID, "adjoint: call snowb_adjoint_end before the backward pass");
+    if (tp.used == 0) return fail(SNOWB_ERR_INVALID, "adjoint: nothing recorded");
+    if (!io || !io->gx_sph || !io->gv_sph || !io->gT_sph || !io->gx_dem || !io->gv_dem || !io->gT_dem ||
+        !io->gL_dem)
+        return fail(SNOWB_ERR_INVALID, "adjoint: null gradient buffer");
+    uint32_t viol = 0;
+    CUDA_TRY(cudaMemcpyAsync(&viol, tp.viol, sizeof(uint32_t), cudaMemcpyDeviceToHost, g_stream));
+    CUDA_TRY(cudaStreamSynchronize(g_stream));
+    if (viol & 1u) return fail(SNOWB_ERR_INVALID, "adjoint: a particle changed phase while recording");
+    if (viol & 2u) return fail(SNOWB_ERR_INVALID, "adjoint: recorded particles need contrib == 1");
+    TRY(adj_ensure(tp.full, tp.nb, tp.P.ncells));
+    AdjBufs& B = g_adj;
+    const uint32_t nh[4] = {tp.n[0], tp.n[1], tp.nb, 0};
+    CUDA_TRY(cudaMemcpyAsync(B.nbuf, nh, sizeof(nh), cudaMemcpyHostToDevice, g_stream));
+    CUDA_TRY(cudaMemsetAsync(B.gp, 0, 4 * sizeof(double), g_stream));
+    LAUNCH(k_boundary_prep, tp.nb, 256, tp.bcd, tp.bnd.volume, tp.bnd.massInv, tp.bnd.mass, tp.nb, B.bp4, B.binvm,
+           B.bmass, nullptr, nullptr);
+    float* gx[2] = {io->gx_sph, io->gx_dem};
+    float* gv[2] = {io->gv_sph, io->gv_dem};
+    float* gT[2] = {io->gT_sph, io->gT_dem};
+    for (size_t k = tp.used; k-- > 0;) TRY(adj_substep(tp.steps[k], gx, gv, gT, io->gL_dem));
+    double g[4];
+    CUDA_TRY(cudaMemcpyAsync(g, B.gp, sizeof(g), cudaMemcpyDeviceToHost, g_stream));
+    CUDA_TRY(cudaStreamSynchronize(g_stream));
+    snowb_adjoint_io* w = const_cast<snowb_adjoint_io*>(io);
+    for (int k = 0; k < 4; ++k) w->grad_params[k] += g[k];
+    tp.used = 0;
+    CUDA_TRY(cudaMemsetAsync(tp.viol, 0, sizeof(uint32_t), g_stream));
     return SNOWB_OK;
 }
 
@@ -666,6 +1027,8 @@ static int run_steps(snowb_particle_data* sph, uint32_t* sph_size, snowb_particl
     }
     TRY(ensure_ctx(full, nb, P.ncells));
     Ctx& c = g_ctx;
+    if (g_tape.recording) TRY(tape_start_call(P, sph, *sph_size, dem, *dem_size, bnd, nb, full, bcd, dt, iterations,
+                                              fl, opt, batch));
     StepArgs a{sph, dem, bnd, buf, nb, full, scd, dcd, bcd, dt, iterations,
                fl[0], fl[1], fl[2], fl[3], fl[4], fl[5], fl[6], fl[7], fl[8], fl[9], fl[10], dTe, opt.stop_after,
                batch ? batch->scene_sph : nullptr, batch ? batch->scene_dem : nullptr,
@@ -1077,6 +1440,39 @@ int snowb_batch_snow_simulation(const snowb_batch* b, snowb_particle_data* sph, 
                      dt, iterations, fl, temperature_variation, o, b);
 }
 
+// ------------------------------------------------------------------ adjoint
+int snowb_adjoint_begin(void)
+{
+    if (g_tape.recording) return fail(SNOWB_ERR_INVALID, "adjoint: already recording");
+    g_tape.recording = true;
+    g_tape.used = 0;
+    if (g_tape.viol) CUDA_TRY(cudaMemsetAsync(g_tape.viol, 0, sizeof(uint32_t), g_stream));
+    return SNOWB_OK;
+}
+
+int snowb_adjoint_end(uint32_t* substeps)
+{
+    if (!g_tape.recording) return fail(SNOWB_ERR_INVALID, "adjoint: not recording");
+    g_tape.recording = false;
+    if (substeps) *substeps = (uint32_t)g_tape.used;
+    return SNOWB_OK;
+}
+
+int snowb_adjoint_backward(snowb_adjoint_io* io)
+{
+    return adjoint_backward(io);
+}
+
+int snowb_adjoint_release(void)
+{
+    g_tape.recording = false;
+    tape_free_steps();
+    if (g_tape.viol) cudaFree(g_tape.viol);
+    g_tape = Tape();
+    adj_free();
+    return SNOWB_OK;
+}
+
 int snowb_read_sizes(uint32_t* sph_size, uint32_t* dem_size)
 {
     if (!g_ctx.S) return fail(SNOWB_ERR_INVALID, "no step has run");
@@ -1179,6 +1575,8 @@ int snowb_release(void)
     std::lock_guard<std::mutex> lk(g_mu);
     graph_free();
     free_ctx(g_ctx);
+    tape_free_steps();
+    adj_free();
     return SNOWB_OK;
 }
 

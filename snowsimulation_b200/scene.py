@@ -273,4 +273,24 @@ def config2(seed=0, n_scenes=64, lo=2000, hi=40000):
     return worlds
 
 
-SCENES = {"config0": config0, "config1": config1, "tiny": tiny}
+def config3(seed=0):
+    """Adjoint scene: 1,024 water (8x16x8 column, jitter +-2 mm, 100 C) falling onto an
+    8,192-particle snow block (32x8x32, jitter +-2 mm, -10 C) with initial interlinks.
+    Phase change is off: the adjoint holds phase flags fixed, so a differentiated run may
+    not move particles between sets."""
+    w = scene_drop((8, 16, 8), (32, 8, 32), seed=seed, water_jitter=0.002, snow_jitter=0.002, drop_height=0.1,
+                   name="config3: 1024 water + 8192 snow", init_links=True)
+    w.flags["change_phase"] = False
+    return w
+
+
+def adjoint_tiny(seed=0):
+    """A small scene for adjoint tests: 27 water particles dropped onto a 6x3x6 snow block
+    with interlinks, phase change off."""
+    w = scene_drop((3, 3, 3), (6, 3, 6), seed=seed, water_jitter=0.002, snow_jitter=0.002, drop_height=0.005,
+                   name="adjoint tiny", init_links=True)
+    w.flags["change_phase"] = False
+    return w
+
+
+SCENES = {"config0": config0, "config1": config1, "config3": config3, "tiny": tiny}
