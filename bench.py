@@ -14,7 +14,9 @@ the slowest rank's time.
 
 The line also carries "batched": 64 scenes of uneven size (log-uniform 2k-40k particles)
 stepped as one batch, against the same scenes stepped one after another through the
-plain entry point (--no-batched skips it).
+plain entry point (--no-batched skips it), and "adjoint": a differentiable rollout of
+config 3 (40 substeps, forward with checkpoints + backward) against the same substeps run
+plain (--no-adjoint skips it).
 
 --impl reference times the CPU restatement of the same substep (FP32, all host threads,
 one substep per step), the only CPU implementation of this path: the reference itself
@@ -47,6 +49,7 @@ def parse():
     ap.add_argument("--scene", default="config1")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--profile-out", default="")
     return ap.parse_args()
 
@@ -227,6 +230,65 @@ def batched_compare(frames, dev, seed, flush):
             "speedup_vs_plain": plain_ms / batch_ms}
 
 
+# ----------------------------------------------------------------- adjoint vs plain
+def adjoint_compare(substeps, dev, seed, checkpoint_every=10):
+    """Config 3 (1,024 water on 8,192 snow with interlinks, phase change off): device time of
+    `substeps` plain substeps (graph replay) against a differentiable rollout of the same
+    substeps (forward with checkpoints + backward: recomputation with the tape on and the
+    reverse kernels), loss = snow-position MSE + temperature MSE, gradients w.r.t. the
+    water's initial velocities and k_refreezing, k_stretch, k_water, k_snow."""
+    import torch
+    from snowsimulation_b200 import scene
+    from snowsimulation_b200.abi import QUIRKS_FIXED
+    from snowsimulation_b200.adjoint import loss_fn, params_of, restore, rollout, snapshot
+    from snowsimulation_b200.world import Simulation
+
+    w = scene.config3(seed=seed)
+    sim = Simulation(w, device=dev, quirks=QUIRKS_FIXED).setup()
+    n = sim.n_sph + sim.n_dem
+    start = snapshot(sim)
+    stream = torch.cuda.current_stream(dev)
+
+    def ev_time(fn):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        a.record(stream)
+        out = fn()
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        return a.elapsed_time(b), out
+
+    for _ in range(2):   # warm-up (graph capture)
+        restore(sim, start)
+        sim.step(substeps=substeps, use_graph=True)
+    restore(sim, start)
+    plain_ms, _ = ev_time(lambda: sim.step(substeps=substeps, use_graph=True))
+    restore(sim, start)
+    theta = params_of(sim)
+    v0 = sim.sph.t["velocity"][:sim.n_sph].clone()
+    with torch.no_grad():
+        _, xd, _, Td = rollout(sim, v0, theta, substeps, checkpoint_every)
+    tx, tT = xd + 0.005, Td + 1.0
+
+    def adj():
+        restore(sim, start)
+        vv = v0.clone().requires_grad_(True)
+        th = theta.clone().requires_grad_(True)
+        _, xd, _, Td = rollout(sim, vv, th, substeps, checkpoint_every)
+        L = loss_fn(xd, Td, tx, tT, 1e-4)
+        L.backward()
+        return th.grad
+
+    adj()   # warm-up (tape and reverse buffers)
+    adj_ms, g = ev_time(adj)
+    return {"workload": "config3: %d water + %d snow + %d boundary, %d substeps, checkpoint every %d, fixed quirks"
+                        % (sim.n_sph, sim.n_dem, sim.n_b, substeps, checkpoint_every),
+            "plain_ms_per_substep": plain_ms / substeps, "adjoint_ms_per_substep": adj_ms / substeps,
+            "adjoint_over_plain": adj_ms / plain_ms,
+            "plain_value": n * substeps / (plain_ms / 1000.0), "adjoint_value": n * substeps / (adj_ms / 1000.0),
+            "unit": UNIT, "grad_params": [float(x) for x in g]}
+
+
 # ----------------------------------------------------------------- our arm
 def main():
     args = parse()
@@ -375,6 +437,10 @@ def main():
             batched_res["ms_per_step"], batched_res["plain_ms_per_step"] = float(t[0]), float(t[1])
             batched_res["speedup_vs_plain"] = float(t[1]) / float(t[0])
 
+    adjoint_res = None
+    if not args.no_adjoint:
+        adjoint_res = adjoint_compare(40, dev, rank)
+
     if rank != 0:
         if ws > 1:
             dist.destroy_process_group()
@@ -403,6 +469,8 @@ def main():
     }
     if not args.no_batched:
         line["batched"] = batched_res
+    if adjoint_res is not None:
+        line["adjoint"] = adjoint_res
     if ws == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.scene)
     print(json.dumps(line))

@@ -241,6 +241,35 @@ int snowb_batch_snow_simulation(const snowb_batch* batch,
                                 int dynamic_max_connections, int cd_on, float temperature_variation,
                                 const snowb_step_options* options);
 
+/* ---- autotuner (no reference counterpart) ------------------------------------------------
+ * Times the tunable kernels of the substep (neighbour passes, link colouring, apply) under
+ * nine launch shapes (64/128/256 threads per block x grid caps of 8/16/64 blocks per SM),
+ * each over `substeps` graph-replayed substeps timed from CUDA-event nodes, and keeps the
+ * fastest shape per kernel and work-size bucket (floor(log2(threads of work))).  The
+ * arguments are those of snowb_snow_simulation_ex (batch: NULL for one scene, else the
+ * batch of snowb_batch_snow_simulation); the state advances by 9 x (substeps + 1) substeps,
+ * so callers snapshot it first if they need it.  Launch shapes never change results. */
+int snowb_autotune(snowb_particle_data* sph, uint32_t* sph_size,
+                   snowb_particle_data* dem, uint32_t* dem_size,
+                   snowb_particle_data* boundary, uint32_t boundary_size,
+                   uint32_t full_size,
+                   snowb_particle_data* phase_change_buffer,
+                   snowb_cell_data sph_cell_data, snowb_cell_data dem_cell_data,
+                   snowb_cell_data b_cell_data,
+                   snowb_scene_params* scene_params,
+                   float dt, int iterations,
+                   int sph_dem_correction, int sph_sph_correction, int dem_friction,
+                   int compute_temperature, int change_phase, int simulate_freezing,
+                   int simulate_melting, int dem_viscosity, int use_interlink,
+                   int dynamic_max_connections, int cd_on, float temperature_variation,
+                   int quirks, int substeps, const snowb_batch* batch);
+/* The table as text, one "kernel bucket threads_per_block grid_cap_per_sm" line per entry. */
+int snowb_autotune_table(char* out, size_t cap);
+/* Replace the table with one in that format (e.g. saved from an earlier run). */
+int snowb_autotune_load(const char* table);
+/* Forget all tuned shapes (back to the built-in ones). */
+int snowb_autotune_reset(void);
+
 /* ---- adjoint of the substep (no reference counterpart) -------------------------------
  * Reverse-mode derivatives of snowb_snow_simulation_ex substeps in the fixed quirk mode,
  * with the forward pass's discrete decisions held fixed (neighbour sets, interlink

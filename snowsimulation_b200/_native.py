@@ -37,6 +37,7 @@ EXPORTS = (
     "snowb_batch_reorder_data", "snowb_batch_compute_boundary_volume", "snowb_batch_connect_and_record",
     "snowb_batch_snow_simulation",
     "snowb_adjoint_begin", "snowb_adjoint_end", "snowb_adjoint_backward", "snowb_adjoint_release",
+    "snowb_autotune", "snowb_autotune_table", "snowb_autotune_load", "snowb_autotune_reset",
 )
 
 _lib = None
@@ -95,6 +96,10 @@ def load(path=LIB_PATH):
         "snowb_adjoint_end": [pu32],
         "snowb_adjoint_backward": [C.POINTER(AdjointIO)],
         "snowb_adjoint_release": [],
+        "snowb_autotune": sig["snowb_snow_simulation"] + [i, i, PB],
+        "snowb_autotune_table": [C.c_char_p, C.c_size_t],
+        "snowb_autotune_load": [C.c_char_p],
+        "snowb_autotune_reset": [],
     })
     for name, args in sig.items():
         fn = getattr(lib, name)

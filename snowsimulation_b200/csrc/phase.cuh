@@ -219,7 +219,7 @@ __device__ __forceinline__ bool has_free_slot(const uint32_t* rec, uint32_t o, u
         if (rec[q] == SNOWB_UMAX) return true;
     return false;
 }
-__global__ void __launch_bounds__(128) k_link_filter(DevParams P, DevState* S, SetView vd,
+__global__ void __launch_bounds__(256) k_link_filter(DevParams P, DevState* S, SetView vd,
                                                      snowb_particle_data dem, int dynamic,
                                                      uint8_t* __restrict__ active)
 {

@@ -52,6 +52,7 @@ static DevParams g_P;
 static int g_quirks = SNOWB_QUIRKS_REFERENCE;
 static cudaStream_t g_stream = 0;
 static int g_max_blocks = 148 * 16;
+static int g_sms = 148;
 
 static float smallest_with_sqrt_ge(float t)   // min x: sqrtf(x) >= t
 {
@@ -207,6 +208,7 @@ static int ensure_ctx(uint32_t full, uint32_t nb, uint32_t ncells)
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     g_max_blocks = sms * 16;
+    g_sms = sms;
     return SNOWB_OK;
 }
 static int ensure_gen(uint32_t n, uint32_t ncells)
@@ -288,6 +290,62 @@ static inline unsigned blocks_for(uint64_t work, int tpb)
             return fail(SNOWB_ERR_CUDA, std::string(#kernel) + ": " + cudaGetErrorString(_e)); \
     } while (0)
 #define LAUNCH(kernel, work, tpb, ...) KL(kernel, blocks_for((work), (tpb)), (tpb), __VA_ARGS__)
+
+// ------------------------------------------------------------------ autotuner
+// Launch shapes of the tunable kernels (threads per block, grid cap in blocks per SM),
+// chosen per kernel and work-size bucket (floor(log2(threads of work))) by
+// snowb_autotune, which times every candidate shape from CUDA-event nodes inside the
+// substep's graph.  Launch shapes never change results: every thread's work and every
+// reduction order are independent of the block and grid shape.
+struct TuneEntry {
+    std::string name;
+    int bucket, tpb, capm;
+};
+static std::vector<TuneEntry> g_tune;
+static uint64_t g_tune_gen = 0;        // bumped when the table or the forced shape changes (graph key)
+static int g_tune_force_tpb = 0, g_tune_force_capm = 0;
+static std::vector<std::pair<std::string, int>> g_tune_seen;   // (kernel, bucket) launched while forcing
+static inline int ilog2_u64(uint64_t x)
+{
+    int b = 0;
+    while (x > 1) { x >>= 1; ++b; }
+    return b;
+}
+static void tune_pick(const char* name, uint64_t work, int tpb0, int max_tpb, int& tpb, unsigned& grid)
+{
+    const int bucket = ilog2_u64(work ? work : 1);
+    tpb = tpb0;
+    int capm = 0;
+    if (g_tune_force_tpb) {
+        tpb = g_tune_force_tpb < max_tpb ? g_tune_force_tpb : max_tpb;
+        capm = g_tune_force_capm;
+        bool seen = false;
+        for (auto& e : g_tune_seen) seen |= e.first == name && e.second == bucket;
+        if (!seen) g_tune_seen.emplace_back(name, bucket);
+    } else {
+        for (const auto& e : g_tune)
+            if (e.bucket == bucket && e.name == name) { tpb = e.tpb; capm = e.capm; break; }
+        if (tpb > max_tpb) tpb = max_tpb;
+    }
+    uint64_t b = (work + tpb - 1) / tpb;
+    if (b < 1) b = 1;
+    const uint64_t cap = capm ? (uint64_t)capm * g_sms : (uint64_t)g_max_blocks;
+    if (b > cap) b = cap;
+    grid = (unsigned)b;
+}
+#define TLAUNCH(kernel, max_tpb, work, tpb0, ...)                                            \
+    do {                                                                                     \
+        int _tpb;                                                                            \
+        unsigned _grid;                                                                      \
+        tune_pick(#kernel, (work), (tpb0), (max_tpb), _tpb, _grid);                          \
+        KL(kernel, _grid, _tpb, __VA_ARGS__);                                                \
+    } while (0)
+// tunable only when `tunable` holds (else the built-in shape)
+#define TLAUNCH_IF(tunable, kernel, max_tpb, work, tpb0, ...)                                \
+    do {                                                                                     \
+        if (tunable) TLAUNCH(kernel, max_tpb, work, tpb0, __VA_ARGS__);                       \
+        else LAUNCH(kernel, work, tpb0, __VA_ARGS__);                                        \
+    } while (0)
 #define LAUNCH1(kernel, ...) KL(kernel, 1, 32, __VA_ARGS__)
 
 static inline unsigned scan_blocks(uint32_t n) { return (n + SCAN_CHUNK - 1) / SCAN_CHUNK + (n == 0); }
@@ -495,10 +553,10 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
     TRY(sort_if(1, nullptr));
     TRY(sort_if(0, nullptr));
     STOP(1);
-    LAUNCH(k_density<false>, work3, 128, P, S, vs, vd, vb, X, ss, sd, sb, NL);
+    TLAUNCH(k_density<false>, 256, work3, 128, P, S, vs, vd, vb, X, ss, sd, sb, NL);
     STOP(2);
     if (a.temperature) {
-        LAUNCH(k_heat, 2 * full, 128, P, S, vs, vd, X, a.dt);
+        TLAUNCH(k_heat, 256, 2 * full, 128, P, S, vs, vd, X, a.dt);
         LAUNCH(k_heat_commit, 2 * full, 256, S, X, a.dTe, step_sph ? 1 : 0, step_dem ? 1 : 0);
     }
     STOP(3);
@@ -530,9 +588,9 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
     }
     STOP(5);
     if (a.interlink) {
-        LAUNCH(k_link_filter, full, 128, P, S, vd, *a.dem, a.dynamic, c.active);
+        TLAUNCH(k_link_filter, 256, full, 128, P, S, vd, *a.dem, a.dynamic, c.active);
         for (uint32_t col = 0; col < 8; ++col)
-            LAUNCH(k_link_colour, (P.gsx / 4) * (P.gsy / 4) * (P.gsz / 4), 64, P, S, vd, *a.dem, c.s[1].off,
+            TLAUNCH(k_link_colour, 128, (P.gsx / 4) * (P.gsy / 4) * (P.gsz / 4), 64, P, S, vd, *a.dem, c.s[1].off,
                    c.s[1].off + 1, c.active, col, a.dynamic);
         if (a.dynamic) LAUNCH1(k_adjust_links, P, S, *a.dem, full);
     }
@@ -551,15 +609,17 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
         TAPE_HOOK(2, it);
         STOP(base + 0);
         // density + lambda in one pass (stage boundaries base+1 and base+2 coincide)
-        LAUNCH(k_density<true>, work3, 128, P, S, vs, vd, vb, X, ss, sd, sb, NL);
+        TLAUNCH(k_density<true>, 256, work3, 128, P, S, vs, vd, vb, X, ss, sd, sb, NL);
         STOP(base + 2);
-        LAUNCH(k_pbf, 2 * full, 128, P, S, vs, vd, vb, X, ss, sd, sb, a.dt, F, NL);
+        // the reference's snow PBF pass adds into repeated targets with float atomics (Q3):
+        // its order follows the launch shape, so that pass keeps the built-in shape
+        TLAUNCH_IF(!ref, k_pbf, 256, 2 * full, 128, P, S, vs, vd, vb, X, ss, sd, sb, a.dt, F, NL);
         STOP(base + 3);
-        LAUNCH(k_dem_corr, full, 128, P, S, vs, vd, vb, X, ss, sd, sb, F, NL);
-        if (a.interlink) LAUNCH(k_interlink, full, 128, P, S, *a.dem);
+        TLAUNCH(k_dem_corr, 256, full, 128, P, S, vs, vd, vb, X, ss, sd, sb, F, NL);
+        if (a.interlink) TLAUNCH(k_interlink, 1024, full, 128, P, S, *a.dem);
         STOP(base + 5);
         if (step_sph || step_dem) {
-            LAUNCH(k_apply, 2 * full, 256, P, S, vs, vd, X, step_sph ? 1 : 0, step_dem ? 1 : 0);
+            TLAUNCH(k_apply, 1024, 2 * full, 256, P, S, vs, vd, X, step_sph ? 1 : 0, step_dem ? 1 : 0);
             if (step_sph) dirty_s = true;
             if (step_dem) dirty_d = true;
         }
@@ -568,8 +628,8 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
         if (a.friction && step_dem) {
             TRY(sort_if(1, nullptr));
             TRY(sort_if(0, nullptr));
-            LAUNCH(k_friction, full, 128, P, S, vd, vb, X, sd, sb);
-            LAUNCH(k_apply, full, 256, P, S, vs, vd, X, 0, 1);
+            TLAUNCH(k_friction, 256, full, 128, P, S, vd, vb, X, sd, sb);
+            TLAUNCH(k_apply, 1024, full, 256, P, S, vs, vd, X, 0, 1);
             dirty_d = true;
         }
         STOP(base + 7);
@@ -580,12 +640,12 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
     STOP(90);
     // apply_XSPH_viscosity (:3663-3711), Jacobi
     if (step_sph) {
-        LAUNCH(k_xsph_warp, (uint64_t)full * 32, 128, P, S, vs, vd, *a.sph, *a.dem, 1, P.sph_visc, c.tmp_vel);
+        TLAUNCH(k_xsph_warp, 256, (uint64_t)full * 32, 128, P, S, vs, vd, *a.sph, *a.dem, 1, P.sph_visc, c.tmp_vel);
         LAUNCH(k_xsph_commit, full, 256, P, S, vs, 1, c.tmp_vel, a.sph->velocity);
     }
     TAPE_HOOK(5, 0);
     if (a.dem_visc && step_dem) {
-        LAUNCH(k_xsph_warp, (uint64_t)full * 32, 128, P, S, vd, vs, *a.dem, *a.sph, 0, P.dem_visc, c.tmp_vel);
+        TLAUNCH(k_xsph_warp, 256, (uint64_t)full * 32, 128, P, S, vd, vs, *a.dem, *a.sph, 0, P.dem_visc, c.tmp_vel);
         LAUNCH(k_xsph_commit, full, 256, P, S, vd, 0, c.tmp_vel, a.dem->velocity);
     }
     TAPE_HOOK(6, 0);
@@ -922,6 +982,7 @@ static int graph_substeps(const DevParams& P, const StepArgs& a, bool step_sph, 
     key_add(key, g_ctx.S);
     key_add(key, g_ctx_gen);
     key_add(key, g_prof);
+    key_add(key, g_tune_gen);
     const cudaStream_t user = g_stream;
     GraphEntry* ent = nullptr;
     for (auto& e : g_graph.entries)
@@ -1438,6 +1499,120 @@ int snowb_batch_snow_simulation(const snowb_batch* b, snowb_particle_data* sph, 
     snowb_step_options o = options ? *options : default_options();
     return run_steps(sph, sph_size, dem, dem_size, boundary, boundary_size, full_size, buffer, scd, dcd, bcd, scene,
                      dt, iterations, fl, temperature_variation, o, b);
+}
+
+// ------------------------------------------------------------------ autotuner
+int snowb_autotune(snowb_particle_data* sph, uint32_t* sph_size, snowb_particle_data* dem, uint32_t* dem_size,
+                   snowb_particle_data* boundary, uint32_t boundary_size, uint32_t full_size,
+                   snowb_particle_data* buffer, snowb_cell_data scd, snowb_cell_data dcd, snowb_cell_data bcd,
+                   snowb_scene_params* scene, float dt, int iterations, int sph_dem_correction,
+                   int sph_sph_correction, int dem_friction, int compute_temperature, int change_phase,
+                   int simulate_freezing, int simulate_melting, int dem_viscosity, int use_interlink,
+                   int dynamic_max_connections, int cd_on, float temperature_variation, int quirks,
+                   int substeps, const snowb_batch* batch)
+{
+    if (substeps < 1) return fail(SNOWB_ERR_INVALID, "autotune: substeps must be >= 1");
+    if (g_prof || g_tape.recording) return fail(SNOWB_ERR_INVALID, "autotune: profiling or adjoint recording active");
+    if (quirks != SNOWB_QUIRKS_REFERENCE && quirks != SNOWB_QUIRKS_FIXED)
+        return fail(SNOWB_ERR_INVALID, "unknown quirk mode");
+    const int fl[11] = {sph_dem_correction, sph_sph_correction, dem_friction, compute_temperature, change_phase,
+                        simulate_freezing, simulate_melting, dem_viscosity, use_interlink, dynamic_max_connections,
+                        cd_on};
+    static const int tpbs[3] = {64, 128, 256};
+    static const int caps[3] = {8, 16, 64};
+    snowb_step_options o;
+    o.quirks = quirks; o.stop_after = 0; o.use_graph = 1; o.sync = 1;
+    std::vector<std::string> names;
+    std::vector<std::vector<double>> ms;   // [name][candidate]
+    g_tune_seen.clear();
+    int rc = SNOWB_OK;
+    for (int c = 0; c < 9 && rc == SNOWB_OK; ++c) {
+        g_tune_force_tpb = tpbs[c / 3];
+        g_tune_force_capm = caps[c % 3];
+        ++g_tune_gen;
+        o.substeps = 1;   // capture and warm the candidate's graph, untimed
+        rc = run_steps(sph, sph_size, dem, dem_size, boundary, boundary_size, full_size, buffer, scd, dcd, bcd, scene,
+                       dt, iterations, fl, temperature_variation, o, batch);
+        if (rc != SNOWB_OK) break;
+        snowb_profile_begin();
+        o.substeps = substeps;
+        rc = run_steps(sph, sph_size, dem, dem_size, boundary, boundary_size, full_size, buffer, scd, dcd, bcd, scene,
+                       dt, iterations, fl, temperature_variation, o, batch);
+        const int rc2 = snowb_profile_end(nullptr, 0);
+        if (rc == SNOWB_OK) rc = rc2;
+        for (size_t k = 0; k < g_acc_name.size(); ++k) {
+            size_t idx = 0;
+            while (idx < names.size() && names[idx] != g_acc_name[k]) ++idx;
+            if (idx == names.size()) { names.push_back(g_acc_name[k]); ms.emplace_back(9, -1.0); }
+            ms[idx][c] = g_acc_ms[k];
+        }
+    }
+    g_tune_force_tpb = 0;
+    g_tune_force_capm = 0;
+    ++g_tune_gen;
+    if (rc != SNOWB_OK) return rc;
+    for (const auto& sb : g_tune_seen) {
+        size_t idx = 0;
+        while (idx < names.size() && names[idx] != sb.first) ++idx;
+        if (idx == names.size()) continue;
+        int best = -1;
+        for (int c = 0; c < 9; ++c)
+            if (ms[idx][c] >= 0.0 && (best < 0 || ms[idx][c] < ms[idx][best])) best = c;
+        if (best < 0) continue;
+        bool found = false;
+        for (auto& e : g_tune)
+            if (e.name == sb.first && e.bucket == sb.second) {
+                e.tpb = tpbs[best / 3]; e.capm = caps[best % 3]; found = true;
+            }
+        if (!found) g_tune.push_back(TuneEntry{sb.first, sb.second, tpbs[best / 3], caps[best % 3]});
+    }
+    ++g_tune_gen;
+    return SNOWB_OK;
+}
+
+int snowb_autotune_table(char* out, size_t cap)
+{
+    if (!out || cap == 0) return fail(SNOWB_ERR_INVALID, "null buffer");
+    std::string txt;
+    for (const auto& e : g_tune)
+        txt += e.name + " " + std::to_string(e.bucket) + " " + std::to_string(e.tpb) + " " + std::to_string(e.capm) +
+               "\n";
+    const size_t n = txt.size() < cap - 1 ? txt.size() : cap - 1;
+    std::memcpy(out, txt.data(), n);
+    out[n] = 0;
+    if (txt.size() >= cap) return fail(SNOWB_ERR_INVALID, "table buffer too small");
+    return SNOWB_OK;
+}
+
+int snowb_autotune_load(const char* table)
+{
+    if (!table) return fail(SNOWB_ERR_INVALID, "null table");
+    std::vector<TuneEntry> t;
+    const char* p = table;
+    while (*p) {
+        const char* eol = std::strchr(p, '\n');
+        std::string line(p, eol ? (size_t)(eol - p) : std::strlen(p));
+        p = eol ? eol + 1 : p + line.size();
+        if (line.empty()) continue;
+        char name[128];
+        int bucket, tpb, capm;
+        if (std::sscanf(line.c_str(), "%127s %d %d %d", name, &bucket, &tpb, &capm) != 4)
+            return fail(SNOWB_ERR_INVALID, "autotune table: bad line '" + line + "'");
+        if (bucket < 0 || bucket > 63 || (tpb != 32 && tpb != 64 && tpb != 128 && tpb != 256 && tpb != 512 && tpb != 1024) ||
+            capm < 0 || capm > 1024)
+            return fail(SNOWB_ERR_INVALID, "autotune table: value out of range in '" + line + "'");
+        t.push_back(TuneEntry{name, bucket, tpb, capm});
+    }
+    g_tune = t;
+    ++g_tune_gen;
+    return SNOWB_OK;
+}
+
+int snowb_autotune_reset(void)
+{
+    g_tune.clear();
+    ++g_tune_gen;
+    return SNOWB_OK;
 }
 
 // ------------------------------------------------------------------ adjoint

@@ -305,7 +305,7 @@ __device__ __forceinline__ void acc_WG(const DevParams& P, float& rho, float& gs
     }
 }
 template <bool LAMBDA>
-__global__ void __launch_bounds__(128) k_density(DevParams P, const DevState* __restrict__ S, SetView vs, SetView vd,
+__global__ void __launch_bounds__(256) k_density(DevParams P, const DevState* __restrict__ S, SetView vs, SetView vd,
                                                  SetView vb, Sets X, Sorted ss, Sorted sd, Sorted sb, NList L)
 {
     const uint32_t ns = S->n_sph, nd = S->n_dem, nb = S->n_b;
@@ -373,7 +373,7 @@ __global__ void __launch_bounds__(128) k_density(DevParams P, const DevState* __
 struct StageFlags {
     int correct_dem, sph_sph, interlink, step_sph, step_dem;
 };
-__global__ void __launch_bounds__(128) k_pbf(DevParams P, const DevState* __restrict__ S, SetView vs, SetView vd,
+__global__ void __launch_bounds__(256) k_pbf(DevParams P, const DevState* __restrict__ S, SetView vs, SetView vd,
                                              SetView vb, Sets X, Sorted ss, Sorted sd, Sorted sb, float dt,
                                              StageFlags F, NList L)
 {
@@ -485,7 +485,7 @@ __device__ __forceinline__ float3 link_corr(const DevParams& P, const snowb_part
 // compute_dem_sph_distance_correction (:2112-2162), compute_dem_distance_correction
 // (:1765-1834) and solve_snow_interlink_constraint_d (:4742-4765) for snow particle o,
 // added to its correction in the reference's kernel order (after the PBF pass).
-__global__ void __launch_bounds__(128) k_dem_corr(DevParams P, const DevState* __restrict__ S, SetView vs, SetView vd,
+__global__ void __launch_bounds__(256) k_dem_corr(DevParams P, const DevState* __restrict__ S, SetView vs, SetView vd,
                                                   SetView vb, Sets X, Sorted ss, Sorted sd, Sorted sb, StageFlags F,
                                                   NList L)
 {
@@ -580,7 +580,7 @@ __device__ __forceinline__ float3 friction_term(const DevParams& P, float3 dx, f
     }
     return sc3(-(w0 / ws), dxt);
 }
-__global__ void __launch_bounds__(128) k_friction(DevParams P, const DevState* __restrict__ S, SetView vd, SetView vb,
+__global__ void __launch_bounds__(256) k_friction(DevParams P, const DevState* __restrict__ S, SetView vd, SetView vb,
                                                   Sets X, Sorted sd, Sorted sb)
 {
     vd.n = S->n_dem; vb.n = S->n_b;
@@ -727,7 +727,7 @@ __device__ __forceinline__ float heat_sum(const DevParams& P, float dT, const Se
     return dT;
 }
 // transfer_heat_sph / transfer_heat_dem (:3812-3937): new_T from T
-__global__ void __launch_bounds__(128) k_heat(DevParams P, const DevState* __restrict__ S, SetView vs, SetView vd,
+__global__ void __launch_bounds__(256) k_heat(DevParams P, const DevState* __restrict__ S, SetView vs, SetView vd,
                                               Sets X, float dt)
 {
     const uint32_t ns = S->n_sph, nd = S->n_dem;
@@ -852,7 +852,7 @@ __device__ __forceinline__ float3 xsph_cell(const DevParams& P, const SetView& v
         }
     return cs;
 }
-__global__ void __launch_bounds__(128) k_xsph_warp(DevParams P, const DevState* __restrict__ S, SetView vown,
+__global__ void __launch_bounds__(256) k_xsph_warp(DevParams P, const DevState* __restrict__ S, SetView vown,
                                                    SetView voth, snowb_particle_data A, snowb_particle_data B,
                                                    int own_is_sph, float visc, snowb_float3* __restrict__ out_vel)
 {
@@ -942,6 +942,9 @@ __global__ void k_set_state(DevState* S, uint32_t ns, uint32_t nd, uint32_t nb)
         S->n_sph = ns; S->n_dem = nd; S->n_b = nb;
         S->n0_sph = ns; S->n0_dem = nd;
         S->n_freeze = 0; S->n_melt = 0; S->changed = 0; S->new_sph = ns; S->new_dem = nd;
+        // the caller may have changed the tail slots between calls: the first compaction
+        // of a call cleans the tail as the reference's does every substep
+        S->tail_dirty = 1u;
     }
 }
 // batched runs: every live slot's scene id must name a scene of the batch

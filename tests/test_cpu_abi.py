@@ -47,3 +47,21 @@ def test_calls_without_params_fail_cleanly():
     assert (n.value, t.value) == (2, 512)
     assert lib.snowb_compute_grid_size(0, 512, C.byref(n), C.byref(t)) == 0
     assert (n.value, t.value) == (0, 0)
+
+
+def test_autotune_table_round_trip():
+    """The autotuner's table parser and printer (no GPU work involved)."""
+    import ctypes as C
+    lib = _native.load()
+    text = "k_density<true> 18 128 16\nk_pbf 18 256 8\nk_link_colour 12 64 64\n"
+    assert lib.snowb_autotune_load(text.encode()) == 0
+    buf = C.create_string_buffer(4096)
+    assert lib.snowb_autotune_table(buf, len(buf)) == 0
+    assert buf.value.decode() == text
+    for bad in ("k_pbf 18 100 8\n", "k_pbf x 128 8\n", "k_pbf 18 128\n", "k_pbf 99 128 8\n"):
+        assert lib.snowb_autotune_load(bad.encode()) != 0
+    assert lib.snowb_autotune_table(buf, len(buf)) == 0
+    assert buf.value.decode() == text          # a rejected table leaves the old one
+    assert lib.snowb_autotune_reset() == 0
+    assert lib.snowb_autotune_table(buf, len(buf)) == 0
+    assert buf.value.decode() == ""
