@@ -330,6 +330,123 @@ __device__ void link_particle_fast(const DevParams& P, const SetView& vd, const 
         }
     }
 }
+// link_particle_fast with the candidate scan spread over a warp.  The warp walks the 27
+// cells in order; in each cell 32 candidates at a time are tested for d < h in parallel
+// and the passing ones are handled one after another in ascending index, by the same
+// sequential rule as link_particle_fast (the dup test ends the cell, own slots are kept in
+// registers, claims go through memory).  Every lane holds the same state; lane 0 writes.
+// Results are those of link_particle_fast.
+__device__ void link_particle_warp(const DevParams& P, const SetView& vd, const snowb_particle_data& d, uint32_t i,
+                                   int dynamic, DevState* S)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t M = P.maxc;
+    const float3 p = vd.pos(i);
+    const uint32_t o = vd.gi[i];
+    const GCell g = grid_pos(P, p, vd.scene(i));
+    const uint32_t tol = link_tolerance(P, d.T[o], dynamic);
+    const uint32_t base = o * M;
+    uint32_t count = d.iter_end[o] - base;
+    // own slots: lane k holds slot k
+    uint32_t rk = lane < M ? d.connect_record[base + lane] : 0u;
+    FOR27 {
+        uint32_t s, e;
+        if (!vd.range(P, g, ox, oy, oz, s, e)) continue;
+        bool cell_done = false;
+        for (uint32_t j0 = s; j0 < e && !cell_done; j0 += 32u) {
+            const uint32_t j = j0 + lane;
+            float d2 = 0.f;
+            bool in = false;
+            if (j < e && j != i) {
+                const float3 dv = sub3(p, vd.pos(j));
+                d2 = dot3(dv, dv);
+                in = d2 < P.h2_lt;
+            }
+            uint32_t mask = __ballot_sync(0xffffffffu, in);
+            while (mask) {
+                const int k = __ffs(mask) - 1;
+                mask &= mask - 1u;
+                if (!(count < tol)) continue;
+                const uint32_t jj = j0 + (uint32_t)k;
+                const float dk2 = __shfl_sync(0xffffffffu, d2, k);
+                const uint32_t o1 = vd.gi[jj];
+                const float dist = sqrtf(dk2);
+                const bool dup = __any_sync(0xffffffffu, lane < M && rk == o1);
+                if (dup) { cell_done = true; break; }   // the reference returns from the cell helper
+                const uint32_t freem = __ballot_sync(0xffffffffu, lane < M && rk == SNOWB_UMAX);
+                if (!freem) continue;                      // no free slot: the claim loop finds nothing
+                const int free_k = __ffs(freem) - 1;
+                if (lane == 0) d.connect_record[base + free_k] = o1;   // claim
+                if (lane == (uint32_t)free_k) rk = o1;
+                __syncwarp();
+                const uint32_t b1 = o1 * M;
+                bool valid = false;
+                if (d.iter_end[o1] < b1 + M) {
+                    const uint32_t q = lane < M ? d.connect_record[b1 + lane] : 0u;
+                    const uint32_t pm = __ballot_sync(0xffffffffu, lane < M && q == SNOWB_UMAX);
+                    if (pm) {
+                        const int pk = __ffs(pm) - 1;
+                        if (lane == 0) {
+                            d.connect_record[b1 + pk] = o;
+                            d.connect_length[b1 + pk] = dist;
+                            d.iter_end[o1]++;
+                            if (o1 >= vd.n) atomicOr(&S->tail_dirty, 1u);
+                        }
+                        if (o1 == o) {                       // self link (stale cell range)
+                            ++count;
+                            if (lane == (uint32_t)pk) rk = o;
+                        }
+                        valid = true;
+                    }
+                }
+                if (valid) {
+                    ++count;
+                    if (lane == 0) {
+                        d.connect_length[base + free_k] = dist;
+                        d.iter_end[o] = base + count;
+                        atomicAdd(&S->n_links, 1u);
+                    }
+                } else {
+                    if (lane == 0) d.connect_record[base + free_k] = SNOWB_UMAX;
+                    if (lane == (uint32_t)free_k) rk = SNOWB_UMAX;
+                }
+                __syncwarp();
+            }
+        }
+    }
+}
+// One colour with one warp per super-cell: the warp walks the super-cell's particles in
+// ascending sorted index and links the active ones with link_particle_warp.
+__global__ void k_link_colour_warp(DevParams P, DevState* S, SetView vd, snowb_particle_data dem,
+                                   const uint32_t* __restrict__ fs, const uint32_t* __restrict__ fe,
+                                   const uint8_t* __restrict__ active, uint32_t colour, int dynamic)
+{
+    vd.n = S->n_dem;
+    const uint32_t qx = P.gsx >> 2, qy = P.gsy >> 2, qz = P.gsz >> 2;
+    const uint32_t total = qx * qy * qz;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < total; t += nwarps) {
+        const uint32_t sx = 2u * (t % qx) + (colour & 1u);
+        const uint32_t sy = 2u * ((t / qx) % qy) + ((colour >> 1) & 1u);
+        const uint32_t sz = 2u * (t / (qx * qy)) + ((colour >> 2) & 1u);
+        for (uint32_t dz = 0; dz < 2; ++dz)
+            for (uint32_t dy = 0; dy < 2; ++dy)
+                for (uint32_t dx = 0; dx < 2; ++dx) {
+                    const uint32_t h = ((2u * sz + dz) * P.gsy + (2u * sy + dy)) * P.gsx + (2u * sx + dx);
+                    const uint32_t b = fs[h], e = fe[h];
+                    for (uint32_t i0 = b; i0 < e; i0 += 32u) {
+                        const uint32_t i = i0 + lane;
+                        uint32_t am = __ballot_sync(0xffffffffu, i < e && active[i]);
+                        while (am) {
+                            const int k = __ffs(am) - 1;
+                            am &= am - 1u;
+                            link_particle_warp(P, vd, dem, i0 + (uint32_t)k, dynamic, S);
+                        }
+                    }
+                }
+    }
+}
 // general maximum_connection: the plain restatement with every access in memory
 __device__ void link_particle(const DevParams& P, const SetView& vd, const snowb_particle_data& d, uint32_t i,
                               int dynamic, DevState* S)

@@ -589,9 +589,15 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
     STOP(5);
     if (a.interlink) {
         TLAUNCH(k_link_filter, 256, full, 128, P, S, vd, *a.dem, a.dynamic, c.active);
-        for (uint32_t col = 0; col < 8; ++col)
-            TLAUNCH(k_link_colour, 128, (P.gsx / 4) * (P.gsy / 4) * (P.gsz / 4), 64, P, S, vd, *a.dem, c.s[1].off,
-                   c.s[1].off + 1, c.active, col, a.dynamic);
+        const uint32_t nsc = (P.gsx / 4) * (P.gsy / 4) * (P.gsz / 4);   // super-cells per colour
+        for (uint32_t col = 0; col < 8; ++col) {
+            if (P.maxc <= SNOWB_MAXC_FAST)
+                TLAUNCH(k_link_colour_warp, 256, (uint64_t)nsc * 32, 128, P, S, vd, *a.dem, c.s[1].off,
+                        c.s[1].off + 1, c.active, col, a.dynamic);
+            else
+                TLAUNCH(k_link_colour, 128, nsc, 64, P, S, vd, *a.dem, c.s[1].off, c.s[1].off + 1, c.active, col,
+                        a.dynamic);
+        }
         if (a.dynamic) LAUNCH1(k_adjust_links, P, S, *a.dem, full);
     }
     STOP(6);
@@ -1206,9 +1212,13 @@ static int connect_links(const DevParams& P, snowb_particle_data* dem, uint32_t 
            sid, sid ? c.s[1].sid : nullptr);
     SetView vd = make_view(dcd, c.s[1].p4, dem->mass, sid ? c.s[1].sid : nullptr);
     LAUNCH(k_link_filter, n, 128, P, c.S, vd, *dem, dynamic, c.active);
-    for (uint32_t col = 0; col < 8; ++col)
-        LAUNCH(k_link_colour, (P.gsx / 4) * (P.gsy / 4) * (P.gsz / 4), 64, P, c.S, vd, *dem, c.fs, c.fe, c.active, col,
-               dynamic);
+    const uint32_t nsc = (P.gsx / 4) * (P.gsy / 4) * (P.gsz / 4);
+    for (uint32_t col = 0; col < 8; ++col) {
+        if (P.maxc <= SNOWB_MAXC_FAST)
+            LAUNCH(k_link_colour_warp, (uint64_t)nsc * 32, 128, P, c.S, vd, *dem, c.fs, c.fe, c.active, col, dynamic);
+        else
+            LAUNCH(k_link_colour, nsc, 64, P, c.S, vd, *dem, c.fs, c.fe, c.active, col, dynamic);
+    }
     CUDA_TRY(cudaStreamSynchronize(g_stream));
     return SNOWB_OK;
 }
