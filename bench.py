@@ -339,6 +339,9 @@ def main():
     clk = clocks.stop()
     ms = [a.elapsed_time(b) for a, b in evs]
     tot_ms = sum(ms)
+    ms_sorted = sorted(ms)
+    pct = {"ms_p10": ms_sorted[int(0.1 * (len(ms) - 1))], "ms_p50": statistics.median(ms),
+           "ms_p90": ms_sorted[int(round(0.9 * (len(ms) - 1)))]}
     sim.read_sizes()
     if ws > 1:
         t = torch.tensor([tot_ms], device=dev)
@@ -347,7 +350,14 @@ def main():
     value = ws * n_part * SUBSTEPS * args.steps / (tot_ms / 1000.0)
     ms_per_step = tot_ms / args.steps
 
-    # ---- end to end through the C-ABI call with host buffers
+    # ---- end to end through the C-ABI call with host buffers, over the same frames of the
+    # scene as the timed region: a second, identical simulation warmed up the same way (the
+    # scene's cost changes as the water melts into the snow, so later frames would not compare)
+    del sim
+    sim = Simulation(getattr(scene, args.scene)(seed=rank), device=dev).setup()
+    for _ in range(max(3, args.warmup)):
+        frame()
+    torch.cuda.synchronize(dev)
     fields = ("positions", "velocity", "T")
     host = {(s, f): torch.empty_like(getattr(sim, s).t[f], device="cpu").pin_memory()
             for s in ("sph", "dem") for f in fields}
@@ -447,7 +457,8 @@ def main():
         return 0
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
-        "warmup": max(3, args.warmup), "ms_per_step": ms_per_step, "higher_is_better": True,
+        "warmup": max(3, args.warmup), "ms_per_step": ms_per_step, "frame_ms_percentiles": pct,
+        "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "%s: %d water + %d snow + %d boundary particles, 1 step = 1 frame = %d substeps "
                                "(dt 1/240 s, 3 iterations), seeded lattice" % (args.scene, w.n_sph, w.n_dem,

@@ -306,7 +306,8 @@ int snowb_read_sizes(uint32_t* sph_size, uint32_t* dem_size);
 
 /* Device counters of the last substep, in this order: n_sph, n_dem, n_boundary, sizes at
  * substep start (2), particles freezing, melting, phase-change flag, sizes after compaction
- * (2), device error bits, tail-dirty flag, particles kept by the link prefilter, links added.
+ * (2), device error bits, tail-dirty flag, particles kept by the link prefilter, links added,
+ * neighbour lists that overflowed in the substep's density+lambda passes.
  * Copies min(n, 16) values into out (blocks). */
 int snowb_device_counters(uint32_t* out, int n);
 

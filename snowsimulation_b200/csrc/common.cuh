@@ -49,7 +49,8 @@ struct DevState {
     uint32_t tail_dirty;            // a link pass wrote slots beyond the snow set (stale cell range)
     uint32_t n_active;              // particles the link prefilter kept for the last link pass
     uint32_t n_links;               // links added by the last link pass
-    uint32_t pad[2];
+    uint32_t n_nl_ovf;              // neighbour lists that overflowed in the last density+lambda pass
+    uint32_t pad;
 };
 #define SNOWB_DEVERR_SCATTER 1u
 #define SNOWB_DEVERR_SCENE 2u      // a batched scene id >= the scene count

@@ -29,7 +29,7 @@ struct Sorted {
 // (their supports are d < h or smaller) instead of re-testing ~300 candidates over 81
 // cells, keeping the per-cell partial sums.  A particle with more than NLIST_K entries is
 // marked overflowed and its consumers traverse the cells as before.
-constexpr uint32_t NLIST_K = 96;
+constexpr uint32_t NLIST_K = 192;
 constexpr uint32_t NL_J_MASK = (1u << 25) - 1u;
 constexpr uint32_t NL_OVF = 1u << 31;
 struct NList {
@@ -305,7 +305,7 @@ __device__ __forceinline__ void acc_WG(const DevParams& P, float& rho, float& gs
     }
 }
 template <bool LAMBDA>
-__global__ void __launch_bounds__(256) k_density(DevParams P, const DevState* __restrict__ S, SetView vs, SetView vd,
+__global__ void __launch_bounds__(256) k_density(DevParams P, DevState* __restrict__ S, SetView vs, SetView vd,
                                                  SetView vb, Sets X, Sorted ss, Sorted sd, Sorted sb, NList L)
 {
     const uint32_t ns = S->n_sph, nd = S->n_dem, nb = S->n_b;
@@ -336,6 +336,7 @@ __global__ void __launch_bounds__(256) k_density(DevParams P, const DevState* __
             if (LAMBDA) {
                 const uint32_t n_bnd = wr.n - n_own - n_oth;
                 L.cnt[wr.slot] = wr.n > NLIST_K ? NL_OVF : (n_own | (n_oth << 10) | (n_bnd << 20));
+                if (wr.n > NLIST_K) atomicAdd(&S->n_nl_ovf, 1u);
             }
         } else {
             // boundary: density visits (b, snow, water), lambda (b, water, snow)
@@ -404,14 +405,16 @@ __global__ void __launch_bounds__(256) k_pbf(DevParams P, const DevState* __rest
             float3 acc = add3(ldv3(X.sph.correction, o), c);
             const float3 z = f3(0.f, 0.f, 0.f);
             const float w0 = X.sph.massInv[o];
-            if (F.correct_dem) {     // compute_sph_dem_distance_correction
+            // the contact terms are scaled by (1 - contrib): with contrib == 1 they add a
+            // zero to a correction that is never -0 here, which leaves it unchanged
+            if (F.correct_dem && ci != 1.f) {     // compute_sph_dem_distance_correction
                 float3 d = lst ? seg_contact(P, z, sx, vd, p, w0, sd.invm, X.dem.massInv)
                                : acc_contact(P, z, vd, p, g, SNOWB_UMAX, w0, sd.invm, X.dem.massInv);
                 d = sc3(1.f - ci, d);
                 if (nan3(d)) d = z;
                 acc = add3(acc, sc3(P.k_stretch, d));
             }
-            if (F.sph_sph) {         // compute_sph_sph_distance_correction
+            if (F.sph_sph && ci != 1.f) {         // compute_sph_sph_distance_correction
                 float3 d = acc_contact_sph(P, z, vs, p, g, i, w0, ci, ss.invm, X.sph.massInv);
                 d = sc3(1.f - ci, d);
                 if (nan3(d)) d = z;
@@ -421,6 +424,9 @@ __global__ void __launch_bounds__(256) k_pbf(DevParams P, const DevState* __rest
         } else {
             const uint32_t i = t - ns;
             const uint32_t o = ref ? vs.gi[i] : vd.gi[i];   // Q3: SPH grid_index in the reference
+            // the snow PBF correction is scaled by (1 - contrib): with contrib == 1 it adds a
+            // zero (a NaN or infinity becomes zero too) to the +0 the last apply left
+            if (X.dem.contrib[o] == 1.f) continue;
             float3 p = xyz(vd.p4[i]); GCell g = grid_pos(P, p, vd.scene(i));
             const float li = X.dem.lambda[o];
             float3 c = f3(0.f, 0.f, 0.f);
@@ -963,7 +969,7 @@ __global__ void k_begin_substep(DevState* S)
 {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         S->n0_sph = S->n_sph; S->n0_dem = S->n_dem;
-        S->n_freeze = 0; S->n_melt = 0; S->changed = 0; S->n_active = 0; S->n_links = 0;
+        S->n_freeze = 0; S->n_melt = 0; S->changed = 0; S->n_active = 0; S->n_links = 0; S->n_nl_ovf = 0;
     }
 }
 
