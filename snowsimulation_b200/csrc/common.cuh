@@ -156,6 +156,55 @@ __device__ __host__ __forceinline__ uint32_t coverage(uint32_t n)
 }
 __device__ __host__ __forceinline__ uint32_t umin32(uint32_t a, uint32_t b) { return a < b ? a : b; }
 
+// The 27 neighbour cells of a particle, computed once and shared by every set and pass of
+// a kernel: wrapped per-axis hash terms (hash = z term + y term + x term, the value of
+// grid_hash) and a mask of the cells whose box lies at squared distance >= cut2 from p
+// (bit (oz+1)*9 + (oy+1)*3 + (ox+1)), with the same face arithmetic as range_culled.
+struct Nbhd {
+    uint32_t x0, x1, x2, y0, y1, y2, z0, z1, z2;   // terms for offsets -1, 0, +1
+    uint32_t far;
+    __device__ __forceinline__ uint32_t hash(int ox, int oy, int oz) const
+    {
+        const uint32_t z = oz < 0 ? z0 : (oz > 0 ? z2 : z1);
+        const uint32_t y = oy < 0 ? y0 : (oy > 0 ? y2 : y1);
+        const uint32_t x = ox < 0 ? x0 : (ox > 0 ? x2 : x1);
+        return z + y + x;
+    }
+};
+__device__ __forceinline__ Nbhd make_nbhd(const DevParams& P, GCell g, float3 p, float cut2)
+{
+    Nbhd nb;
+    float lo[3], hi[3];
+    const float m = 1e-6f;
+    const uint32_t gx = (uint32_t)g.x, gy = (uint32_t)g.y, gz = (uint32_t)g.z, plane = P.gsy * P.gsx;
+    nb.x0 = ((gx - 1u) & (P.sgx - 1u)) + g.bx;
+    nb.x1 = (gx & (P.sgx - 1u)) + g.bx;
+    nb.x2 = ((gx + 1u) & (P.sgx - 1u)) + g.bx;
+    nb.y0 = ((gy - 1u) & (P.gsy - 1u)) * P.gsx;
+    nb.y1 = (gy & (P.gsy - 1u)) * P.gsx;
+    nb.y2 = ((gy + 1u) & (P.gsy - 1u)) * P.gsx;
+    nb.z0 = (((gz - 1u) & (P.sgz - 1u)) + g.bz) * plane;
+    nb.z1 = ((gz & (P.sgz - 1u)) + g.bz) * plane;
+    nb.z2 = (((gz + 1u) & (P.sgz - 1u)) + g.bz) * plane;
+    lo[0] = fmaxf((p.x - ((float)g.x * P.csx + P.ox)) - m, 0.f);
+    hi[0] = fmaxf((((float)(g.x + 1) * P.csx + P.ox) - p.x) - m, 0.f);
+    lo[1] = fmaxf((p.y - ((float)g.y * P.csy + P.oy)) - m, 0.f);
+    hi[1] = fmaxf((((float)(g.y + 1) * P.csy + P.oy) - p.y) - m, 0.f);
+    lo[2] = fmaxf((p.z - ((float)g.z * P.csz + P.oz)) - m, 0.f);
+    hi[2] = fmaxf((((float)(g.z + 1) * P.csz + P.oz) - p.z) - m, 0.f);
+    nb.far = 0u;
+#pragma unroll
+    for (int c = 0; c < 27; ++c) {
+        const int ox = c % 3 - 1, oy = (c / 3) % 3 - 1, oz = c / 9 - 1;
+        if ((ox | oy | oz) == 0) continue;
+        const float gx = ox < 0 ? lo[0] : (ox > 0 ? hi[0] : 0.f);
+        const float gy = oy < 0 ? lo[1] : (oy > 0 ? hi[1] : 0.f);
+        const float gz = oz < 0 ? lo[2] : (oz > 0 ? hi[2] : 0.f);
+        if (gx * gx + gy * gy + gz * gz >= cut2) nb.far |= 1u << c;
+    }
+    return nb;
+}
+
 // Sorted view of one particle set for the 27-cell neighbor loops.  Entries j < n come
 // from the compact float4 copy written at the last sort; a stale cell range (cells the
 // reference leaves uncleared) may reach j >= n, which reads the caller's arrays exactly
@@ -201,6 +250,17 @@ struct SetView {
     // current sort and carries its hash) and whose box lies at squared distance >= cut2
     // from p is reported empty: every member is then beyond the support, so all its terms
     // are exact zeros.  Stale ranges (members anywhere) are never culled.
+    // range_culled with the neighbourhood precomputed (same culling rule)
+    __device__ __forceinline__ bool range_nb(const Nbhd& nb, int ox, int oy, int oz, uint32_t& s, uint32_t& e) const
+    {
+        const uint32_t h = nb.hash(ox, oy, oz);
+        s = __ldg(cs + h);
+        if (s == SNOWB_EMPTY) return false;
+        e = __ldg(ce + h);
+        if ((nb.far >> ((oz + 1) * 9 + (oy + 1) * 3 + (ox + 1))) & 1u)
+            if (s < n && __ldg(gh + s) == h) return false;
+        return true;
+    }
     __device__ __forceinline__ bool range_culled(const DevParams& P, GCell g, int ox, int oy, int oz, float3 p,
                                                  float cut2, uint32_t& s, uint32_t& e) const
     {

@@ -24,6 +24,8 @@
 
 namespace snowb {
 
+#define SNOWB_MAXC_FAST 32   // interlink slots kept in registers (maximum_connection <= 32)
+
 // copy_particle_info (:3974-4002)
 __device__ __forceinline__ void copy_info(const snowb_particle_data& s, const snowb_particle_data& d, uint32_t i,
                                           uint32_t t, uint32_t M)
@@ -230,6 +232,11 @@ __global__ void __launch_bounds__(256) k_link_filter(DevParams P, DevState* S, S
         const float3 p = vd.pos(i);
         const uint32_t count = dem.iter_end[o] - o * M;
         uint8_t act = 0;
+        // own slots in registers (M <= SNOWB_MAXC_FAST), else read from memory
+        uint32_t r[SNOWB_MAXC_FAST];
+        const bool fast = M <= SNOWB_MAXC_FAST;
+#pragma unroll
+        for (int k = 0; k < SNOWB_MAXC_FAST; ++k) r[k] = fast && (uint32_t)k < M ? dem.connect_record[M * o + k] : 0u;
         if (count < link_tolerance(P, dem.T[o], dynamic) && has_free_slot(dem.connect_record, o, M)) {
             const GCell g = grid_pos(P, p, vd.scene(i));
             FOR27 {
@@ -242,8 +249,13 @@ __global__ void __launch_bounds__(256) k_link_filter(DevParams P, DevState* S, S
                         const uint32_t o1 = vd.gi[j];
                         if (o1 == o) { act = 1; break; }
                         bool found = false;
-                        for (uint32_t q = M * o; q < M * (o + 1); ++q)
-                            if (dem.connect_record[q] == o1) { found = true; break; }
+                        if (fast) {
+#pragma unroll
+                            for (int k = 0; k < SNOWB_MAXC_FAST; ++k) found |= (uint32_t)k < M && r[k] == o1;
+                        } else {
+                            for (uint32_t q = M * o; q < M * (o + 1); ++q)
+                                if (dem.connect_record[q] == o1) { found = true; break; }
+                        }
                         // a linked candidate ends the reference's scan of this cell, and it
                         // stays linked, so nothing after it in the cell is reached
                         if (found) break;
@@ -262,7 +274,6 @@ __global__ void __launch_bounds__(256) k_link_filter(DevParams P, DevState* S, S
 // slots, count and tolerance are kept in registers (M <= SNOWB_MAXC_FAST); every record
 // write goes through to memory, where the partner search reads it.  Candidates are
 // screened with the exact squared-distance test (dist < h <=> d2 < h2_lt).
-#define SNOWB_MAXC_FAST 32
 __device__ void link_particle_fast(const DevParams& P, const SetView& vd, const snowb_particle_data& d, uint32_t i,
                                    int dynamic, DevState* S)
 {

@@ -170,6 +170,7 @@ static int alloc_sort(SetBufs& s, uint32_t cap, uint32_t ncells, bool attrs)
     TRY(dalloc(&s.cnt, ncells)); TRY(dalloc(&s.off, ncells + 1));
     TRY(dalloc(&s.bsum, ncells / SCAN_CHUNK + 2));
     CUDA_TRY(cudaMemset(s.cnt, 0, sizeof(uint32_t) * ncells));
+    CUDA_TRY(cudaMemset(s.bsum, 0, sizeof(uint32_t) * (ncells / SCAN_CHUNK + 2)));
     if (attrs) {
         TRY(dalloc(&s.p4, cap)); TRY(dalloc(&s.invm, cap)); TRY(dalloc(&s.contrib, cap)); TRY(dalloc(&s.lambda, cap));
         TRY(dalloc(&s.sid, cap));
@@ -367,11 +368,11 @@ static int sort_set(const DevParams& P, SetBufs& B, const snowb_particle_data& D
                     const uint32_t* sid_o = nullptr)
 {
     const uint32_t nc = P.ncells;
-    LAUNCH(k_hash_count, cap, 256, P, D.predict_positions, n_ptr, 0u, B.key, B.slot, B.cnt, cond, sid_o);
     const unsigned nb = (nc + SCAN_CHUNK - 1) / SCAN_CHUNK;
-    KL(k_block_sums, nb, SCAN_TPB, B.cnt, nc, B.bsum, cond);
+    // chunk counts come from the hash pass (bsum is all zero between sorts)
+    LAUNCH(k_hash_count, cap, 256, P, D.predict_positions, n_ptr, 0u, B.key, B.slot, B.cnt, cond, sid_o, B.bsum);
     KL(k_cell_scan, nb, SCAN_TPB, B.cnt, B.bsum, nc, B.off, cd.cell_start, n_ptr, 0u, clear_all ? 1 : 0, cond);
-    LAUNCH(k_scatter, cap, 256, B.key, B.slot, B.off, B.tmp, n_ptr, 0u, cond);
+    LAUNCH(k_scatter, cap, 256, B.key, B.slot, B.off, B.tmp, n_ptr, 0u, cond, B.bsum, nb);
     LAUNCH(k_rank_reorder, cap, 256, B.key, B.off, B.tmp, D.predict_positions, D.mass, D.massInv, D.contrib, cd, B.p4,
            B.invm, B.contrib, n_ptr, 0u, cond, sid_o, sid_o ? B.sid : nullptr);
     return SNOWB_OK;

@@ -269,37 +269,55 @@ __device__ __forceinline__ bool segments(const NList& L, uint32_t slot, Seg& own
 // compute_snow_{sph,dem_sph,boundary}_lambdas_d (:2598-2898): lambda needs the particle's
 // own C and neighbour positions only, so both come out of one traversal.  Each quantity
 // keeps its own per-cell accumulation in the reference's loop order.
+// one candidate of acc_WG
 template <bool LAMBDA>
-__device__ __forceinline__ void acc_WG(const DevParams& P, float& rho, float& gs, const SetView& v, float3 p, GCell g,
-                                       uint32_t skip, bool vol, int mode, float m_self, const float* mass_s,
-                                       const float* mass_o, NLWriter* wr = nullptr, int set = 0)
+__device__ __forceinline__ void wg_term(const DevParams& P, float& cs, float& cg, float4 q, float3 p, uint32_t j,
+                                        bool vol, int mode, float m_self, float m_j, NLWriter* wr, int cell, int set)
+{
+    float3 dv = sub3(p, xyz(q));
+    float d2 = dot3(dv, dv);
+    if (d2 < P.h2_lt) {
+        if (wr) wr->push(j, cell, set);
+        float d = sqrtf(d2);
+        float w = vol ? P.rho0 * q.w : q.w;
+        cs += w * W_poly6(P, d);
+        if (LAMBDA) {
+            float sc;
+            if (mode == 0) sc = P.inv_rho0;
+            else {
+                float m = mode == 1 ? m_self : m_j;
+                sc = P.inv_rho0 * ((P.rho0 * q.w) / m);
+            }
+            float3 gc = sc3(sc, G_spiky(P, dv, d));
+            cg += dot3(gc, gc);
+        }
+    }
+}
+template <bool LAMBDA>
+__device__ __forceinline__ void acc_WG(const DevParams& P, float& rho, float& gs, const SetView& v, float3 p,
+                                       const Nbhd& nb, uint32_t skip, bool vol, int mode, float m_self,
+                                       const float* mass_s, const float* mass_o, NLWriter* wr = nullptr, int set = 0)
 {
     FOR27 {
         float cs = 0.f, cg = 0.f;
         uint32_t s, e;
-        if (v.range_culled(P, g, ox, oy, oz, p, P.h2_cull, s, e))
-            for (uint32_t j = s; j < e; ++j) {
-                if (j == skip) continue;
-                float4 q = v.pw(j);
-                float3 dv = sub3(p, xyz(q));
-                float d2 = dot3(dv, dv);
-                if (d2 < P.h2_lt) {
-                    if (wr) wr->push(j, CELL27, set);
-                    float d = sqrtf(d2);
-                    float w = vol ? P.rho0 * q.w : q.w;
-                    cs += w * W_poly6(P, d);
-                    if (LAMBDA) {
-                        float sc;
-                        if (mode == 0) sc = P.inv_rho0;
-                        else {
-                            float m = mode == 1 ? m_self : v.attr(mass_s, mass_o, j);
-                            sc = P.inv_rho0 * ((P.rho0 * q.w) / m);
-                        }
-                        float3 gc = sc3(sc, G_spiky(P, dv, d));
-                        cg += dot3(gc, gc);
-                    }
+        if (v.range_nb(nb, ox, oy, oz, s, e)) {
+            const int cell = CELL27;
+            if (e <= v.n) {
+                // current entries only: the compact sorted copies
+                for (uint32_t j = s; j < e; ++j) {
+                    if (j == skip) continue;
+                    const float mj = (LAMBDA && mode == 2) ? __ldg(mass_s + j) : 0.f;
+                    wg_term<LAMBDA>(P, cs, cg, __ldg(v.p4 + j), p, j, vol, mode, m_self, mj, wr, cell, set);
+                }
+            } else {
+                for (uint32_t j = s; j < e; ++j) {
+                    if (j == skip) continue;
+                    const float mj = (LAMBDA && mode == 2) ? v.attr(mass_s, mass_o, j) : 0.f;
+                    wg_term<LAMBDA>(P, cs, cg, v.pw(j), p, j, vol, mode, m_self, mj, wr, cell, set);
                 }
             }
+        }
         rho += cs;
         if (LAMBDA) gs += cg;
     }
@@ -325,14 +343,15 @@ __global__ void __launch_bounds__(256) k_density(DevParams P, DevState* __restri
             lam_s = w ? ss.lambda : sd.lambda;
             o = own.gi[i];
             float3 p = xyz(own.p4[i]); GCell g = grid_pos(P, p, own.scene(i));
+            const Nbhd nb = make_nbhd(P, g, p, P.h2_cull);
             rho = D->mass[o] * P.W0;
             NLWriter wr{L.e, L.stride, (w ? 0u : L.cap) + i, 0u};
             NLWriter* pw = LAMBDA ? &wr : nullptr;
-            acc_WG<LAMBDA>(P, rho, gs, own, p, g, i, false, 0, 0.f, nullptr, nullptr, pw, 0);
+            acc_WG<LAMBDA>(P, rho, gs, own, p, nb, i, false, 0, 0.f, nullptr, nullptr, pw, 0);
             const uint32_t n_own = wr.n;
-            acc_WG<LAMBDA>(P, rho, gs, oth, p, g, SNOWB_UMAX, false, 0, 0.f, nullptr, nullptr, pw, 1);
+            acc_WG<LAMBDA>(P, rho, gs, oth, p, nb, SNOWB_UMAX, false, 0, 0.f, nullptr, nullptr, pw, 1);
             const uint32_t n_oth = wr.n - n_own;
-            acc_WG<LAMBDA>(P, rho, gs, vb, p, g, SNOWB_UMAX, true, 1, D->mass[o], nullptr, nullptr, pw, 2);
+            acc_WG<LAMBDA>(P, rho, gs, vb, p, nb, SNOWB_UMAX, true, 1, D->mass[o], nullptr, nullptr, pw, 2);
             if (LAMBDA) {
                 const uint32_t n_bnd = wr.n - n_own - n_oth;
                 L.cnt[wr.slot] = wr.n > NLIST_K ? NL_OVF : (n_own | (n_oth << 10) | (n_bnd << 20));
@@ -342,15 +361,16 @@ __global__ void __launch_bounds__(256) k_density(DevParams P, DevState* __restri
             // boundary: density visits (b, snow, water), lambda (b, water, snow)
             i = t - ns - nd; o = vb.gi[i];
             float3 p = xyz(vb.p4[i]); GCell g = grid_pos(P, p, vb.scene(i));
+            const Nbhd nb = make_nbhd(P, g, p, P.h2_cull);
             rho = (P.rho0 * X.bnd.volume[o]) * P.W0;
-            acc_WG<LAMBDA>(P, rho, gs, vb, p, g, i, true, 2, 0.f, sb.mass, X.bnd.mass);
+            acc_WG<LAMBDA>(P, rho, gs, vb, p, nb, i, true, 2, 0.f, sb.mass, X.bnd.mass);
             float unused = 0.f;
-            acc_WG<false>(P, rho, unused, vd, p, g, SNOWB_UMAX, false, 0, 0.f, nullptr, nullptr);
-            acc_WG<false>(P, rho, unused, vs, p, g, SNOWB_UMAX, false, 0, 0.f, nullptr, nullptr);
+            acc_WG<false>(P, rho, unused, vd, p, nb, SNOWB_UMAX, false, 0, 0.f, nullptr, nullptr);
+            acc_WG<false>(P, rho, unused, vs, p, nb, SNOWB_UMAX, false, 0, 0.f, nullptr, nullptr);
             if (LAMBDA) {
                 float r2 = 0.f;
-                acc_WG<true>(P, r2, gs, vs, p, g, SNOWB_UMAX, false, 0, 0.f, nullptr, nullptr);
-                acc_WG<true>(P, r2, gs, vd, p, g, SNOWB_UMAX, false, 0, 0.f, nullptr, nullptr);
+                acc_WG<true>(P, r2, gs, vs, p, nb, SNOWB_UMAX, false, 0, 0.f, nullptr, nullptr);
+                acc_WG<true>(P, r2, gs, vd, p, nb, SNOWB_UMAX, false, 0, 0.f, nullptr, nullptr);
             }
             D = &X.bnd; lam_s = sb.lambda;
         }
@@ -597,11 +617,12 @@ __global__ void __launch_bounds__(256) k_friction(DevParams P, const DevState* _
         float3 op0 = ldv3(X.dem.positions, o);
         const float w0 = X.dem.massInv[o];
         GCell g = grid_pos(P, p, vd.scene(i));
+        const Nbhd nb = make_nbhd(P, g, p, P.r2_cull);
         float3 c = f3(0.f, 0.f, 0.f);
         FOR27 {
             float3 cs = f3(0.f, 0.f, 0.f);
             uint32_t s, e;
-            if (vd.range_culled(P, g, ox, oy, oz, p, P.r2_cull, s, e))
+            if (vd.range_nb(nb, ox, oy, oz, s, e))
                 for (uint32_t j = s; j < e; ++j) {
                     if (j == i) continue;
                     float3 pp1 = vd.pos(j);
@@ -619,7 +640,7 @@ __global__ void __launch_bounds__(256) k_friction(DevParams P, const DevState* _
         FOR27 {
             float3 cs = f3(0.f, 0.f, 0.f);
             uint32_t s, e;
-            if (vb.range_culled(P, g, ox, oy, oz, p, P.r2_cull, s, e))
+            if (vb.range_nb(nb, ox, oy, oz, s, e))
                 for (uint32_t j = s; j < e; ++j) {
                     float3 v = sub3(p, vb.pos(j));
                     float d2 = dot3(v, v);

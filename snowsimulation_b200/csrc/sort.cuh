@@ -68,18 +68,32 @@ __device__ __forceinline__ uint32_t prefix_of_blocks(const uint32_t* bsum, uint3
 }
 
 // ------------------------------------------------------------------ 1. hash + count
-// Fused path: hash of pos[o] for o < n (calcHashD :194-212).
+// Fused path: hash of pos[o] for o < n (calcHashD :194-212).  Also adds every particle to
+// the count of its scan chunk (bsum, SCAN_CHUNK cells each, one atomic per chunk and warp),
+// which the cell scan needs; the scatter pass re-zeroes bsum for the next sort.
 __global__ void k_hash_count(DevParams P, const snowb_float3* __restrict__ pos, const uint32_t* n_ptr,
                              uint32_t n_fixed, uint32_t* __restrict__ key_o, uint32_t* __restrict__ slot_o,
-                             uint32_t* __restrict__ cnt, const uint32_t* cond, const uint32_t* __restrict__ sid_o)
+                             uint32_t* __restrict__ cnt, const uint32_t* cond, const uint32_t* __restrict__ sid_o,
+                             uint32_t* __restrict__ bsum)
 {
     if (cond && *cond == 0) return;
     const uint32_t n = n_ptr ? *n_ptr : n_fixed;
-    GRID_LOOP(o, n) {
-        float3 p = ldv3(pos, o);
-        uint32_t h = grid_hash(P, grid_pos(P, p, sid_o ? sid_o[o] : 0u), 0, 0, 0);
-        key_o[o] = h;
-        slot_o[o] = atomicAdd(cnt + h, 1u);
+    const uint32_t lane = threadIdx.x & 31u;
+    // whole warps iterate together so the chunk counts can be aggregated with warp votes
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
+        const uint32_t o = base + lane;
+        const bool live = o < n;
+        uint32_t chunk = 0xFFFFFFFFu;
+        if (live) {
+            float3 p = ldv3(pos, o);
+            uint32_t h = grid_hash(P, grid_pos(P, p, sid_o ? sid_o[o] : 0u), 0, 0, 0);
+            key_o[o] = h;
+            slot_o[o] = atomicAdd(cnt + h, 1u);
+            chunk = h / (uint32_t)SCAN_CHUNK;
+        }
+        const uint32_t peers = __match_any_sync(0xffffffffu, chunk);
+        if (live && lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(bsum + chunk, (uint32_t)__popc(peers));
     }
 }
 // sort_particles path: keys and values already in (grid_hash, grid_index).
@@ -158,11 +172,13 @@ __global__ void k_cell_scan(uint32_t* __restrict__ cnt, const uint32_t* __restri
 // ------------------------------------------------------------------ 3. scatter
 __global__ void k_scatter(const uint32_t* __restrict__ key_o, const uint32_t* __restrict__ slot_o,
                           const uint32_t* __restrict__ off, uint32_t* __restrict__ tmp,
-                          const uint32_t* n_ptr, uint32_t n_fixed, const uint32_t* cond)
+                          const uint32_t* n_ptr, uint32_t n_fixed, const uint32_t* cond,
+                          uint32_t* __restrict__ bsum_zero = nullptr, uint32_t nbsum = 0)
 {
     if (cond && *cond == 0) return;
     const uint32_t n = n_ptr ? *n_ptr : n_fixed;
     GRID_LOOP(o, n) tmp[off[key_o[o]] + slot_o[o]] = o;
+    if (bsum_zero) GRID_LOOP(k, nbsum) bsum_zero[k] = 0u;
 }
 
 // rank of element o among the (unordered) members of its cell, by ascending o
