@@ -61,6 +61,22 @@ def dist_env():
     return ws, rank, local
 
 
+def slowest(values_ms, ws, dev):
+    """Per-rank device times -> their maximum over the ranks (one all_reduce for the list)."""
+    if ws == 1:
+        return [float(v) for v in values_ms]
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(v) for v in values_ms], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.cpu()]
+
+
+def job_rate(units_per_rank, ws, ms):
+    """Whole-job throughput: every rank's units over the slowest rank's time."""
+    return ws * units_per_rank / (ms / 1000.0)
+
+
 # ----------------------------------------------------------------- clocks sampling
 class Clocks:
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -343,11 +359,8 @@ def main():
     pct = {"ms_p10": ms_sorted[int(0.1 * (len(ms) - 1))], "ms_p50": statistics.median(ms),
            "ms_p90": ms_sorted[int(round(0.9 * (len(ms) - 1)))]}
     sim.read_sizes()
-    if ws > 1:
-        t = torch.tensor([tot_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot_ms = float(t.item())
-    value = ws * n_part * SUBSTEPS * args.steps / (tot_ms / 1000.0)
+    tot_ms = slowest([tot_ms], ws, dev)[0]
+    value = job_rate(n_part * SUBSTEPS * args.steps, ws, tot_ms)
     ms_per_step = tot_ms / args.steps
 
     # ---- end to end through the C-ABI call with host buffers, over the same frames of the
@@ -381,11 +394,8 @@ def main():
         b.synchronize()
         e_ms.append(a.elapsed_time(b))
     e_tot = sum(e_ms)
-    if ws > 1:
-        t = torch.tensor([e_tot], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e_tot = float(t.item())
-    e2e = ws * n_part * SUBSTEPS * args.steps / (e_tot / 1000.0)
+    e_tot = slowest([e_tot], ws, dev)[0]
+    e2e = job_rate(n_part * SUBSTEPS * args.steps, ws, e_tot)
 
     # ---- per-kernel device time over the same frames as the timed region: a second,
     # identical simulation is warmed up the same way, then its substep graph is captured
@@ -438,14 +448,13 @@ def main():
     if not args.no_batched:
         batched_res = batched_compare(min(args.steps, 5), dev, rank, flush)
         if ws > 1:
-            t = torch.tensor([batched_res["ms_per_step"], batched_res["plain_ms_per_step"]], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            b_ms, p_ms = slowest([batched_res["ms_per_step"], batched_res["plain_ms_per_step"]], ws, dev)
             f = batched_res["frames"]
             ps_rank = batched_res["value"] * batched_res["ms_per_step"] * f / 1000.0
-            batched_res["value"] = ws * ps_rank / (float(t[0]) * f / 1000.0)
-            batched_res["plain_value"] = ws * ps_rank / (float(t[1]) * f / 1000.0)
-            batched_res["ms_per_step"], batched_res["plain_ms_per_step"] = float(t[0]), float(t[1])
-            batched_res["speedup_vs_plain"] = float(t[1]) / float(t[0])
+            batched_res["value"] = job_rate(ps_rank, ws, b_ms * f)
+            batched_res["plain_value"] = job_rate(ps_rank, ws, p_ms * f)
+            batched_res["ms_per_step"], batched_res["plain_ms_per_step"] = b_ms, p_ms
+            batched_res["speedup_vs_plain"] = p_ms / b_ms
 
     adjoint_res = None
     if not args.no_adjoint:
