@@ -16,7 +16,8 @@ The line also carries "batched": 64 scenes of uneven size (log-uniform 2k-40k pa
 stepped as one batch, against the same scenes stepped one after another through the
 plain entry point (--no-batched skips it), and "adjoint": a differentiable rollout of
 config 3 (40 substeps, forward with checkpoints + backward) against the same substeps run
-plain (--no-adjoint skips it).
+plain (--no-adjoint skips it), and "large": 3 frames of the 1.18M-particle config 4 in a
+widened domain (--no-large skips it).
 
 --impl reference times the CPU restatement of the same substep (FP32, all host threads,
 one substep per step), the only CPU implementation of this path: the reference itself
@@ -50,6 +51,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-large", action="store_true")
     ap.add_argument("--profile-out", default="")
     return ap.parse_args()
 
@@ -244,6 +246,40 @@ def batched_compare(frames, dev, seed, flush):
             "frames": frames, "value": ps / (batch_ms / 1000.0), "unit": UNIT, "ms_per_step": batch_ms / frames,
             "plain_value": ps / (plain_ms / 1000.0), "plain_ms_per_step": plain_ms / frames,
             "speedup_vs_plain": plain_ms / batch_ms}
+
+
+# ----------------------------------------------------------------- large scene
+def large_scene(frames, dev, seed, flush, warmup=2):
+    """Config 4 (1,048,576 snow + 131,072 water, walls at +-1.5 m, 128^3 grid): device time of
+    `frames` graph-replayed frames of 4 substeps after `warmup` frames, reference quirks."""
+    import torch
+    from snowsimulation_b200 import scene
+    from snowsimulation_b200.world import Simulation
+    w = scene.config4(seed=seed)
+    sim = Simulation(w, device=dev).setup()
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(warmup):
+        sim.step(substeps=SUBSTEPS, sync=False, use_graph=True)
+    torch.cuda.synchronize(dev)
+    ms = []
+    for _ in range(frames):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        sim.step(substeps=SUBSTEPS, sync=False, use_graph=True)
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        ms.append(a.elapsed_time(b))
+    sim.read_sizes()
+    n = w.n_sph + w.n_dem
+    res = {"workload": "config4: %d water + %d snow + %d boundary, 128^3 grid, walls +-1.5 m, frames %d-%d"
+                       % (w.n_sph, w.n_dem, w.n_b, warmup, warmup + frames - 1),
+           "frames": frames, "ms_per_step": sum(ms) / frames,
+           "value": n * SUBSTEPS * frames / (sum(ms) / 1000.0), "unit": UNIT,
+           "sizes_after": [sim.n_sph, sim.n_dem]}
+    del sim
+    torch.cuda.empty_cache()
+    return res
 
 
 # ----------------------------------------------------------------- adjoint vs plain
@@ -456,6 +492,14 @@ def main():
             batched_res["ms_per_step"], batched_res["plain_ms_per_step"] = b_ms, p_ms
             batched_res["speedup_vs_plain"] = p_ms / b_ms
 
+    large_res = None
+    if not args.no_large:
+        large_res = large_scene(3, dev, rank, flush)
+        if ws > 1:
+            ms_max = slowest([large_res["ms_per_step"]], ws, dev)[0]
+            n = large_res["value"] * large_res["ms_per_step"] / 1000.0
+            large_res["value"] = job_rate(n, ws, ms_max)
+            large_res["ms_per_step"] = ms_max
     adjoint_res = None
     if not args.no_adjoint:
         adjoint_res = adjoint_compare(40, dev, rank)
@@ -491,6 +535,8 @@ def main():
         line["batched"] = batched_res
     if adjoint_res is not None:
         line["adjoint"] = adjoint_res
+    if large_res is not None:
+        line["large"] = large_res
     if ws == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.scene)
     print(json.dumps(line))

@@ -110,6 +110,12 @@ int snowb_allocate_array(void** dev_ptr, size_t size);
 /* set_sim_params (cuda_simulation.cu:1415-1419): the constants for all later calls. */
 int snowb_set_sim_params(const snowb_sim_params* params);
 
+/* No counterpart in the reference, which fixes the walls at x, z = +-1 and the floor at
+ * y = 0 (integrate_pbd_cd_d, cuda_simulation.cu:487-513).  Moves them for all later calls;
+ * the defaults (-1, 1, -1, 1, 0) reproduce the reference bit for bit.  With a larger
+ * power-of-two grid (snowb_sim_params.grid_size) this holds scenes wider than 2 m. */
+int snowb_set_domain(float x_min, float x_max, float z_min, float z_max, float floor_y);
+
 /* compute_grid_size (cuda_simulation.cu:348-357): the reference's 1-D launch shape. */
 int snowb_compute_grid_size(uint32_t n, uint32_t block_size, uint32_t* num_blocks, uint32_t* num_threads);
 

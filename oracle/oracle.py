@@ -56,6 +56,7 @@ def load(precision=32):
     lib.or_connect_and_record.argtypes = [P, PP, u32, CD, C.c_int]
     lib.or_energy_momentum.argtypes = [P, PP, u32, PP, u32, C.POINTER(C.c_double)]
     lib.or_set_threads.argtypes = [C.c_int]
+    lib.or_set_domain.argtypes = [C.c_float] * 5
     lib.or_real_size.restype = C.c_int
     assert lib.or_real_size() == precision // 8
     _LIBS[precision] = lib
@@ -83,6 +84,7 @@ class OracleWorld:
                         d[k] = v.astype(np.float64)
         self.w = w
         self.params = w.params
+        self.lib.or_set_domain(*[C.c_float(x) for x in w.domain])
         self._structs()
 
     def _pset(self, d):
@@ -123,6 +125,7 @@ class OracleWorld:
 
     def step(self, stop_after=0, dt=None, iterations=None):
         w = self.w
+        self.lib.or_set_domain(*[C.c_float(x) for x in w.domain])
         ns, nd = C.c_uint32(w.n_sph), C.c_uint32(w.n_dem)
         sc = _Scene(*w.scene)
         rc = self.lib.or_snow_simulation(

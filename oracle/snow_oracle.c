@@ -60,6 +60,11 @@
 
 int or_real_size(void) { return (int)sizeof(real); }
 
+static float g_dom[5] = {-1.f, 1.f, -1.f, 1.f, 0.f};   /* walls x, z and floor y (the reference: +-1, 0) */
+void or_set_domain(float x_min, float x_max, float z_min, float z_max, float floor_y)
+{
+    g_dom[0] = x_min; g_dom[1] = x_max; g_dom[2] = z_min; g_dom[3] = z_max; g_dom[4] = floor_y;
+}
 void or_set_threads(int n)
 {
 #ifdef _OPENMP
@@ -795,12 +800,12 @@ static void stage_integrate(const K* k, or_particles* d, uint32_t nthreads, floa
             continue;
         }
         r3 tp = vadd(d->positions[i], vsc(DT, tv));
-        if (tp.x + k->r >= R(1.0f)) { tv.x = -RFABS(tv.x); tv = vsc(k->b_damping, tv); }
-        if (tp.x - k->r <= R(-1.0f)) { tv.x = RFABS(tv.x); tv = vsc(k->b_damping, tv); }
-        if (tp.z + k->r >= R(1.0f)) { tv.z = -RFABS(tv.z); tv = vsc(k->b_damping, tv); }
-        if (tp.z - k->r <= R(-1.0f)) { tv.z = RFABS(tv.z); tv = vsc(k->b_damping, tv); }
-        if (d->positions[i].y - k->r <= R(0.f)) {
-            d->positions[i].y = k->r;
+        if (tp.x + k->r >= R(g_dom[1])) { tv.x = -RFABS(tv.x); tv = vsc(k->b_damping, tv); }
+        if (tp.x - k->r <= R(g_dom[0])) { tv.x = RFABS(tv.x); tv = vsc(k->b_damping, tv); }
+        if (tp.z + k->r >= R(g_dom[3])) { tv.z = -RFABS(tv.z); tv = vsc(k->b_damping, tv); }
+        if (tp.z - k->r <= R(g_dom[2])) { tv.z = RFABS(tv.z); tv = vsc(k->b_damping, tv); }
+        if (d->positions[i].y - k->r <= R(g_dom[4])) {
+            d->positions[i].y = R(g_dom[4]) + k->r;
             tv.y = RFABS(tv.y);
             tv = vsc(k->b_damping, tv);
         }

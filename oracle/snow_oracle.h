@@ -123,5 +123,7 @@ void or_energy_momentum(const or_params* P, const or_particles* sph, uint32_t n_
 
 int or_real_size(void);
 void or_set_threads(int n);
+/* walls at x = x_min, x_max and z = z_min, z_max, floor at y = floor_y (default -1, 1, -1, 1, 0) */
+void or_set_domain(float x_min, float x_max, float z_min, float z_max, float floor_y);
 
 #endif

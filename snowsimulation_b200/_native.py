@@ -38,6 +38,7 @@ EXPORTS = (
     "snowb_batch_snow_simulation",
     "snowb_adjoint_begin", "snowb_adjoint_end", "snowb_adjoint_backward", "snowb_adjoint_release",
     "snowb_autotune", "snowb_autotune_table", "snowb_autotune_load", "snowb_autotune_reset",
+    "snowb_set_domain",
 )
 
 _lib = None
@@ -100,6 +101,7 @@ def load(path=LIB_PATH):
         "snowb_autotune_table": [C.c_char_p, C.c_size_t],
         "snowb_autotune_load": [C.c_char_p],
         "snowb_autotune_reset": [],
+        "snowb_set_domain": [f, f, f, f, f],
     })
     for name, args in sig.items():
         fn = getattr(lib, name)

@@ -51,7 +51,8 @@ def _check_compatible(worlds):
             raise ValueError("batched scenes must share SimParams")
         same = (w.maxc == w0.maxc and w.dt == w0.dt and w.iterations == w0.iterations
                 and w.flags == w0.flags and w.temperature_variation == w0.temperature_variation
-                and list(w.scene) == list(w0.scene) and w.init_links == w0.init_links)
+                and list(w.scene) == list(w0.scene) and w.init_links == w0.init_links
+                and tuple(w.domain) == tuple(w0.domain))
         if not same:
             raise ValueError("batched scenes must share maxc, dt, iterations, flags, scene times and init_links")
 
@@ -111,7 +112,7 @@ def pack(worlds):
     w = HostWorld(w0.params, sph, dem, bnd, buffer, _alloc_cells(full, nc), _alloc_cells(full, nc),
                   _alloc_cells(n_b, nc), int(sum(ns)), int(sum(nd)), n_b, full, maxc, list(w0.scene),
                   w0.dt, w0.iterations, w0.substeps_per_frame, dict(w0.flags), w0.temperature_variation,
-                  "batch of %d scenes" % len(worlds), w0.init_links)
+                  "batch of %d scenes" % len(worlds), w0.init_links, tuple(w0.domain))
     return w, sid
 
 
@@ -189,6 +190,7 @@ class BatchSimulation:
         self._s = [self.sph.struct(), self.dem.struct(), self.bnd.struct(), self.buf.struct()]
         self._c = [self.scd.struct(), self.dcd.struct(), self.bcd.struct()]
         _native.check(self.lib.snowb_set_sim_params(C.byref(w.params)))
+        _native.check(self.lib.snowb_set_domain(*[C.c_float(x) for x in w.domain]))
         _native.check(self.lib.snowb_set_stream(C.c_void_p(torch.cuda.current_stream().cuda_stream)))
         nc = C.c_uint32(0)
         _native.check(self.lib.snowb_batch_num_cells(C.byref(self.batch), C.byref(nc)))
@@ -239,6 +241,6 @@ class BatchSimulation:
                        self.full, w.maxc, [self.scene.fluid_start_time, self.scene.solid_start_time,
                                            self.scene.current_time],
                        w.dt, w.iterations, w.substeps_per_frame, dict(w.flags), w.temperature_variation,
-                       w.name, w.init_links)
+                       w.name, w.init_links, tuple(w.domain))
         sid = {k: _to_host(self.sid[k], self._sid_like[k]) for k in ("sph", "dem", "bnd")}
         return hw, sid

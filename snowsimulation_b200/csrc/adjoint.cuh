@@ -715,15 +715,15 @@ __global__ void ka_integrate_rev(DevParams P, uint32_t n, float dt, int cd_on, c
             int hit[5] = {0, 0, 0, 0, 0};
             const float3 tp = add3(pos, sc3(dt, tv));
             st[0] = tv;
-            if (tp.x + P.r >= 1.0f) { hit[0] = 1; tv.x = -fabsf(tv.x); tv = sc3(P.b_damping, tv); }
+            if (tp.x + P.r >= P.wx1) { hit[0] = 1; tv.x = -fabsf(tv.x); tv = sc3(P.b_damping, tv); }
             st[1] = tv;
-            if (tp.x - P.r <= -1.0f) { hit[1] = 1; tv.x = fabsf(tv.x); tv = sc3(P.b_damping, tv); }
+            if (tp.x - P.r <= P.wx0) { hit[1] = 1; tv.x = fabsf(tv.x); tv = sc3(P.b_damping, tv); }
             st[2] = tv;
-            if (tp.z + P.r >= 1.0f) { hit[2] = 1; tv.z = -fabsf(tv.z); tv = sc3(P.b_damping, tv); }
+            if (tp.z + P.r >= P.wz1) { hit[2] = 1; tv.z = -fabsf(tv.z); tv = sc3(P.b_damping, tv); }
             st[3] = tv;
-            if (tp.z - P.r <= -1.0f) { hit[3] = 1; tv.z = fabsf(tv.z); tv = sc3(P.b_damping, tv); }
+            if (tp.z - P.r <= P.wz0) { hit[3] = 1; tv.z = fabsf(tv.z); tv = sc3(P.b_damping, tv); }
             st[4] = tv;
-            if (pos.y - P.r <= 0.f) { hit[4] = 1; floor_fix = true; tv.y = fabsf(tv.y); tv = sc3(P.b_damping, tv); }
+            if (pos.y - P.r <= P.floor_y) { hit[4] = 1; floor_fix = true; tv.y = fabsf(tv.y); tv = sc3(P.b_damping, tv); }
             const float sp = len3(tv);
             if (sp > P.max_speed) {
                 const float3 th = div3(tv, sp);

@@ -35,6 +35,8 @@ struct DevParams {
     float h2_lt, r2_lt, r2_le;
     // box-culling thresholds: the cut-offs with a relative safety margin
     float h2_cull, r2_cull;
+    // walls at x = wx0, wx1 and z = wz0, wz1, floor at y = floor_y (the reference: +-1, 0)
+    float wx0, wx1, wz0, wz1, floor_y;
     int quirks;
 };
 

@@ -49,6 +49,7 @@ static std::mutex g_mu;
 static bool g_have_params = false;
 static snowb_sim_params g_sim;
 static DevParams g_P;
+static float g_domain[5] = {-1.f, 1.f, -1.f, 1.f, 0.f};   // x_min, x_max, z_min, z_max, floor_y
 static int g_quirks = SNOWB_QUIRKS_REFERENCE;
 static cudaStream_t g_stream = 0;
 static int g_max_blocks = 148 * 16;
@@ -96,6 +97,7 @@ static DevParams derive(const snowb_sim_params& s)
     P.gsx = s.grid_size[0]; P.gsy = s.grid_size[1]; P.gsz = s.grid_size[2];
     P.ncells = s.num_cells; P.maxc = s.maximum_connection;
     P.sgx = P.gsx; P.sgz = P.gsz; P.batch_nx = 1; P.batch_shift = 0; P.scene_mask = 0;
+    P.wx0 = g_domain[0]; P.wx1 = g_domain[1]; P.wz0 = g_domain[2]; P.wz1 = g_domain[3]; P.floor_y = g_domain[4];
     P.h2_lt = smallest_with_sqrt_ge(P.h);
     P.r2_lt = smallest_with_sqrt_ge(P.two_r);
     P.r2_le = smallest_with_sqrt_gt(P.two_r);
@@ -1254,6 +1256,17 @@ int snowb_set_sim_params(const snowb_sim_params* params)
     g_sim = *params;
     g_P = derive(g_sim);
     g_have_params = true;
+    return SNOWB_OK;
+}
+
+int snowb_set_domain(float x_min, float x_max, float z_min, float z_max, float floor_y)
+{
+    if (!(x_min < x_max) || !(z_min < z_max) || !std::isfinite(x_min) || !std::isfinite(x_max) ||
+        !std::isfinite(z_min) || !std::isfinite(z_max) || !std::isfinite(floor_y))
+        return fail(SNOWB_ERR_INVALID, "domain needs finite x_min < x_max, z_min < z_max and floor_y");
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_domain[0] = x_min; g_domain[1] = x_max; g_domain[2] = z_min; g_domain[3] = z_max; g_domain[4] = floor_y;
+    if (g_have_params) g_P = derive(g_sim);
     return SNOWB_OK;
 }
 

@@ -671,13 +671,13 @@ __device__ __forceinline__ void integrate_one(const DevParams& P, const snowb_pa
         return;
     }
     float3 tp = add3(pos, sc3(dt, tv));
-    if (tp.x + P.r >= 1.0f) { tv.x = -fabsf(tv.x); tv = sc3(P.b_damping, tv); }
-    if (tp.x - P.r <= -1.0f) { tv.x = fabsf(tv.x); tv = sc3(P.b_damping, tv); }
-    if (tp.z + P.r >= 1.0f) { tv.z = -fabsf(tv.z); tv = sc3(P.b_damping, tv); }
-    if (tp.z - P.r <= -1.0f) { tv.z = fabsf(tv.z); tv = sc3(P.b_damping, tv); }
-    if (pos.y - P.r <= 0.f) {
-        pos.y = P.r;
-        reinterpret_cast<float*>(D.positions)[3ull * i + 1] = P.r;
+    if (tp.x + P.r >= P.wx1) { tv.x = -fabsf(tv.x); tv = sc3(P.b_damping, tv); }
+    if (tp.x - P.r <= P.wx0) { tv.x = fabsf(tv.x); tv = sc3(P.b_damping, tv); }
+    if (tp.z + P.r >= P.wz1) { tv.z = -fabsf(tv.z); tv = sc3(P.b_damping, tv); }
+    if (tp.z - P.r <= P.wz0) { tv.z = fabsf(tv.z); tv = sc3(P.b_damping, tv); }
+    if (pos.y - P.r <= P.floor_y) {
+        pos.y = P.floor_y + P.r;
+        reinterpret_cast<float*>(D.positions)[3ull * i + 1] = pos.y;
         tv.y = fabsf(tv.y);
         tv = sc3(P.b_damping, tv);
     }

@@ -77,6 +77,7 @@ class HostWorld:
     temperature_variation: float = 0.0
     name: str = ""
     init_links: bool = False
+    domain: tuple = (-1.0, 1.0, -1.0, 1.0, 0.0)   # walls x_min, x_max, z_min, z_max and floor y
 
     def copy(self):
         def cp(d):
@@ -85,7 +86,7 @@ class HostWorld:
                          cp(self.sph_cd), cp(self.dem_cd), cp(self.b_cd), self.n_sph, self.n_dem,
                          self.n_b, self.full, self.maxc, list(self.scene), self.dt, self.iterations,
                          self.substeps_per_frame, dict(self.flags), self.temperature_variation,
-                         self.name, self.init_links)
+                         self.name, self.init_links, tuple(self.domain))
 
 
 def lattice(counts, spacing, origin_min, jitter=0.0, rng=None):
@@ -100,18 +101,19 @@ def lattice(counts, spacing, origin_min, jitter=0.0, rng=None):
     return pos.astype(np.float32)
 
 
-def boundary_box(particle_radius):
-    """InitializeBoundaryParticles (Simulation.cpp:425-556) in float32 arithmetic."""
-    return _boundary_box(float(np.float32(particle_radius))).copy()
+def boundary_box(particle_radius, half_x=1.0, half_y=1.0, half_z=1.0):
+    """InitializeBoundaryParticles (Simulation.cpp:425-556) in float32 arithmetic.  The
+    half extents are the reference's 1 m unless a wider domain asks for more."""
+    return _boundary_box(float(np.float32(particle_radius)), float(half_x), float(half_y), float(half_z)).copy()
 
 
 @functools.lru_cache(maxsize=4)
-def _boundary_box(particle_radius):
+def _boundary_box(particle_radius, half_x, half_y, half_z):
     f = np.float32
     thickness = 1
     d = f(2.0) * f(particle_radius)
     pts = []
-    he1 = (f(1.0), d * f(thickness) / f(2.0), f(1.0))
+    he1 = (f(half_x), d * f(thickness) / f(2.0), f(half_z))
     nx, nz = int(he1[0] / d), int(he1[2] / d)
     bo_y = f(-0.5) * d
     left, right = np.inf, -np.inf
@@ -126,7 +128,7 @@ def _boundary_box(particle_radius):
                 right = max(right, x)
     left = f(left) - d
     right = f(right) + d
-    he2 = (d * f(thickness) / f(2.0), f(1.0), f(1.0))
+    he2 = (d * f(thickness) / f(2.0), f(half_y), f(half_z))
     ny, nz = int(he2[1] / d), int(he2[2] / d)
     lo = (left, f(ny) * d, f(0))
     ro = (right, f(ny) * d, f(0))
@@ -145,7 +147,7 @@ def _boundary_box(particle_radius):
                 front = max(front, p[2])
     back = f(back) - d
     front = f(front) + d
-    he3 = (f(1.0), f(1.0), d * f(thickness) / f(2.0))
+    he3 = (f(half_x), f(half_y), d * f(thickness) / f(2.0))
     nx, ny = int(he3[0] / d), int(he3[1] / d)
     bko = (f(0), f(ny) * d, back)
     fro = (f(0), f(ny) * d, front)
@@ -284,6 +286,29 @@ def config3(seed=0):
     return w
 
 
+def config4(seed=0):
+    """The large scene: a 1,048,576-particle snow block (128 x 64 x 128, jitter +-2 mm, -10 C)
+    with initial interlinks, and 131,072 water particles (100 C) in 8 columns of 16,384
+    (16 x 64 x 16) dropped 0.3 m onto it.  It does not fit the reference's 2 m box, so the
+    walls move to x, z = +-1.5 m (boundary box of the same construction, 3 m tall) and the
+    grid grows to 128^3 cells of h (5.12 m per axis, wrapped)."""
+    rng = np.random.default_rng(seed)
+    p = make_sim_params(grid_size=(128, 128, 128))
+    r, s = float(p.particle_radius), 0.02
+    snow = _block((128, 64, 128), s, (0.0, 0.0), r, 0.002, rng)
+    top = r + s * 63
+    water = []
+    for k in range(8):
+        cx = -0.96 + 0.64 * (k % 4)
+        cz = -0.48 + 0.96 * (k // 4)
+        water.append(_block((16, 64, 16), s, (cx, cz), top + 0.3, 0.002, rng))
+    water = np.concatenate(water)
+    half = 1.5
+    return build_world(water, snow, 100.0, -10.0, params=p, boundary=boundary_box(r, half, half, half),
+                       name="config4: 131072 water + 1048576 snow", init_links=True,
+                       domain=(-half, half, -half, half, 0.0))
+
+
 def adjoint_tiny(seed=0):
     """A small scene for adjoint tests: 27 water particles dropped onto a 6x3x6 snow block
     with interlinks, phase change off."""
@@ -293,4 +318,4 @@ def adjoint_tiny(seed=0):
     return w
 
 
-SCENES = {"config0": config0, "config1": config1, "config3": config3, "tiny": tiny}
+SCENES = {"config0": config0, "config1": config1, "config3": config3, "config4": config4, "tiny": tiny}

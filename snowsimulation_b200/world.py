@@ -86,6 +86,7 @@ class Simulation:
         self._c = [self.scd.struct(), self.dcd.struct(), self.bcd.struct()]
         self.params = world.params
         _native.check(self.lib.snowb_set_sim_params(C.byref(self.params)))
+        _native.check(self.lib.snowb_set_domain(*[C.c_float(x) for x in world.domain]))
         _native.check(self.lib.snowb_set_stream(C.c_void_p(torch.cuda.current_stream().cuda_stream)))
 
     # -- Simulation::InitializeBoundaryCudaData (Simulation.cpp:558-592)
@@ -148,4 +149,4 @@ class Simulation:
                          self.n_b, self.full, w.maxc,
                          [self.scene.fluid_start_time, self.scene.solid_start_time, self.scene.current_time],
                          w.dt, w.iterations, w.substeps_per_frame, dict(w.flags), w.temperature_variation,
-                         w.name, w.init_links)
+                         w.name, w.init_links, tuple(w.domain))

@@ -153,3 +153,23 @@ def test_phase_change_conserves_particles():
     ids = np.sort(np.concatenate([o.w.sph["trackId"][: o.w.n_sph], o.w.dem["trackId"][: o.w.n_dem]]))
     assert np.array_equal(ids, np.arange(1, w.full + 1, dtype=np.uint32))
     assert (o.w.n_sph, o.w.n_dem) != (w.n_sph, w.n_dem)
+
+
+def test_domain_default_is_reference_and_floor_moves():
+    """The default domain of a world is the reference's box (walls +-1 m, floor 0); a raised
+    floor holds the particles above it (the integrate step clamps to floor + r)."""
+    from snowsimulation_b200 import scene
+    from snowsimulation_b200.abi import QUIRKS_FIXED
+    from oracle.oracle import OracleWorld
+    assert tuple(scene.tiny().domain) == (-1.0, 1.0, -1.0, 1.0, 0.0)
+    w = scene.tiny(seed=2)
+    w.domain = (-1.0, 1.0, -1.0, 1.0, 0.03)
+    o = OracleWorld(w, 32, QUIRKS_FIXED).setup()
+    for _ in range(3):
+        o.step()
+    y = o.w.dem["positions"][: o.w.n_dem, 1]
+    assert y.min() >= 0.03 - 1e-6
+    o2 = OracleWorld(scene.tiny(seed=2), 32, QUIRKS_FIXED).setup()
+    for _ in range(3):
+        o2.step()
+    assert o2.w.dem["positions"][: o2.w.n_dem, 1].min() < 0.03
