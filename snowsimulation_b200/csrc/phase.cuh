@@ -221,12 +221,15 @@ __device__ __forceinline__ bool has_free_slot(const uint32_t* rec, uint32_t o, u
         if (rec[q] == SNOWB_UMAX) return true;
     return false;
 }
+// L: the snow-snow candidate lists of the substep's first density pass (L.cnt null: none),
+// replayed instead of the traversal while no phase change re-sorted the sets.
 __global__ void __launch_bounds__(256) k_link_filter(DevParams P, DevState* S, SetView vd,
                                                      snowb_particle_data dem, int dynamic,
-                                                     uint8_t* __restrict__ active)
+                                                     uint8_t* __restrict__ active, NList L)
 {
     const uint32_t nd = S->n_dem, M = P.maxc;
     vd.n = nd;
+    const bool lists = L.cnt != nullptr && S->changed == 0;
     GRID_LOOP(i, nd) {
         const uint32_t o = vd.gi[i];
         const float3 p = vd.pos(i);
@@ -237,7 +240,31 @@ __global__ void __launch_bounds__(256) k_link_filter(DevParams P, DevState* S, S
         const bool fast = M <= SNOWB_MAXC_FAST;
 #pragma unroll
         for (int k = 0; k < SNOWB_MAXC_FAST; ++k) r[k] = fast && (uint32_t)k < M ? dem.connect_record[M * o + k] : 0u;
-        if (count < link_tolerance(P, dem.T[o], dynamic) && has_free_slot(dem.connect_record, o, M)) {
+        const uint32_t lc = lists ? L.cnt[L.cap + i] : NL_OVF;
+        if (!(lc & NL_OVF) && count < link_tolerance(P, dem.T[o], dynamic) &&
+            has_free_slot(dem.connect_record, o, M)) {
+            // the same scan over the listed candidates (cells in order, d < h, j != i)
+            uint32_t skip_cell = 0xFFu;
+            const uint32_t nl = lc & 1023u;
+            for (uint32_t k = 0; k < nl && !act; ++k) {
+                const uint32_t en = L.e[(size_t)k * L.stride + L.cap + i];
+                const uint32_t cell = (en >> 25) & 31u;
+                if (cell == skip_cell) continue;
+                const uint32_t o1 = vd.gi[en & NL_J_MASK];
+                if (o1 == o) { act = 1; break; }
+                bool found = false;
+                if (fast) {
+#pragma unroll
+                    for (int q = 0; q < SNOWB_MAXC_FAST; ++q) found |= (uint32_t)q < M && r[q] == o1;
+                } else {
+                    for (uint32_t q = M * o; q < M * (o + 1); ++q)
+                        if (dem.connect_record[q] == o1) { found = true; break; }
+                }
+                if (found) { skip_cell = cell; continue; }
+                if (dem.iter_end[o1] < (o1 + 1) * M && has_free_slot(dem.connect_record, o1, M)) act = 1;
+            }
+        } else if ((lc & NL_OVF) && count < link_tolerance(P, dem.T[o], dynamic) &&
+                   has_free_slot(dem.connect_record, o, M)) {
             const GCell g = grid_pos(P, p, vd.scene(i));
             FOR27 {
                 uint32_t s, e;
@@ -426,13 +453,98 @@ __device__ void link_particle_warp(const DevParams& P, const SetView& vd, const 
         }
     }
 }
+// link_particle_warp replaying the snow-snow candidate list written by the substep's first
+// density pass at the same sorted positions (entries in traversal order: cells z-y-x, index
+// ascending, all with d < h, tagged with their cell).  The sequential rule is the same; a
+// dup ends the entries of its cell.
+__device__ void link_particle_list(const DevParams& P, const SetView& vd, const snowb_particle_data& d, uint32_t i,
+                                   int dynamic, DevState* S, const NList& L, uint32_t n_list)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t M = P.maxc;
+    const float3 p = vd.pos(i);
+    const uint32_t o = vd.gi[i];
+    const uint32_t tol = link_tolerance(P, d.T[o], dynamic);
+    const uint32_t base = o * M;
+    const uint32_t slot = L.cap + i;
+    uint32_t count = d.iter_end[o] - base;
+    uint32_t rk = lane < M ? d.connect_record[base + lane] : 0u;
+    uint32_t skip_cell = 0xFFu;
+    for (uint32_t k0 = 0; k0 < n_list; k0 += 32u) {
+        const uint32_t k = k0 + lane;
+        uint32_t j = 0, cell = 0xFEu;
+        float d2 = 0.f;
+        if (k < n_list) {
+            const uint32_t en = L.e[(size_t)k * L.stride + slot];
+            j = en & NL_J_MASK;
+            cell = (en >> 25) & 31u;
+            const float3 dv = sub3(p, vd.pos(j));
+            d2 = dot3(dv, dv);
+        }
+        uint32_t mask = __ballot_sync(0xffffffffu, k < n_list);
+        while (mask) {
+            const int kk = __ffs(mask) - 1;
+            mask &= mask - 1u;
+            const uint32_t ck = __shfl_sync(0xffffffffu, cell, kk);
+            const uint32_t jj = __shfl_sync(0xffffffffu, j, kk);
+            const float dk2 = __shfl_sync(0xffffffffu, d2, kk);
+            if (ck == skip_cell) continue;
+            if (!(count < tol)) continue;
+            const uint32_t o1 = vd.gi[jj];
+            const float dist = sqrtf(dk2);
+            const bool dup = __any_sync(0xffffffffu, lane < M && rk == o1);
+            if (dup) { skip_cell = ck; continue; }   // the reference returns from the cell helper
+            const uint32_t freem = __ballot_sync(0xffffffffu, lane < M && rk == SNOWB_UMAX);
+            if (!freem) continue;
+            const int free_k = __ffs(freem) - 1;
+            if (lane == 0) d.connect_record[base + free_k] = o1;
+            if (lane == (uint32_t)free_k) rk = o1;
+            __syncwarp();
+            const uint32_t b1 = o1 * M;
+            bool valid = false;
+            if (d.iter_end[o1] < b1 + M) {
+                const uint32_t q = lane < M ? d.connect_record[b1 + lane] : 0u;
+                const uint32_t pm = __ballot_sync(0xffffffffu, lane < M && q == SNOWB_UMAX);
+                if (pm) {
+                    const int pk = __ffs(pm) - 1;
+                    if (lane == 0) {
+                        d.connect_record[b1 + pk] = o;
+                        d.connect_length[b1 + pk] = dist;
+                        d.iter_end[o1]++;
+                        if (o1 >= vd.n) atomicOr(&S->tail_dirty, 1u);
+                    }
+                    if (o1 == o) {
+                        ++count;
+                        if (lane == (uint32_t)pk) rk = o;
+                    }
+                    valid = true;
+                }
+            }
+            if (valid) {
+                ++count;
+                if (lane == 0) {
+                    d.connect_length[base + free_k] = dist;
+                    d.iter_end[o] = base + count;
+                    atomicAdd(&S->n_links, 1u);
+                }
+            } else {
+                if (lane == 0) d.connect_record[base + free_k] = SNOWB_UMAX;
+                if (lane == (uint32_t)free_k) rk = SNOWB_UMAX;
+            }
+            __syncwarp();
+        }
+    }
+}
 // One colour with one warp per super-cell: the warp walks the super-cell's particles in
 // ascending sorted index and links the active ones with link_particle_warp.
+// L: the snow-snow candidate lists of the substep's first density pass (L.cnt null: none);
+// they are valid while no phase change re-sorted the sets.
 __global__ void k_link_colour_warp(DevParams P, DevState* S, SetView vd, snowb_particle_data dem,
                                    const uint32_t* __restrict__ fs, const uint32_t* __restrict__ fe,
-                                   const uint8_t* __restrict__ active, uint32_t colour, int dynamic)
+                                   const uint8_t* __restrict__ active, uint32_t colour, int dynamic, NList L)
 {
     vd.n = S->n_dem;
+    const bool lists = L.cnt != nullptr && S->changed == 0;
     const uint32_t qx = P.gsx >> 2, qy = P.gsy >> 2, qz = P.gsz >> 2;
     const uint32_t total = qx * qy * qz;
     const uint32_t lane = threadIdx.x & 31u;
@@ -452,7 +564,10 @@ __global__ void k_link_colour_warp(DevParams P, DevState* S, SetView vd, snowb_p
                         while (am) {
                             const int k = __ffs(am) - 1;
                             am &= am - 1u;
-                            link_particle_warp(P, vd, dem, i0 + (uint32_t)k, dynamic, S);
+                            const uint32_t ii = i0 + (uint32_t)k;
+                            const uint32_t lc = lists ? L.cnt[L.cap + ii] : NL_OVF;
+                            if (lc & NL_OVF) link_particle_warp(P, vd, dem, ii, dynamic, S);
+                            else link_particle_list(P, vd, dem, ii, dynamic, S, L, lc & 1023u);
                         }
                     }
                 }

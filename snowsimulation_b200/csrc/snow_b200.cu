@@ -591,12 +591,12 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
     }
     STOP(5);
     if (a.interlink) {
-        TLAUNCH(k_link_filter, 256, full, 128, P, S, vd, *a.dem, a.dynamic, c.active);
+        TLAUNCH(k_link_filter, 256, full, 128, P, S, vd, *a.dem, a.dynamic, c.active, NL);
         const uint32_t nsc = (P.gsx / 4) * (P.gsy / 4) * (P.gsz / 4);   // super-cells per colour
         for (uint32_t col = 0; col < 8; ++col) {
             if (P.maxc <= SNOWB_MAXC_FAST)
                 TLAUNCH(k_link_colour_warp, 256, (uint64_t)nsc * 32, 128, P, S, vd, *a.dem, c.s[1].off,
-                        c.s[1].off + 1, c.active, col, a.dynamic);
+                        c.s[1].off + 1, c.active, col, a.dynamic, NL);
             else
                 TLAUNCH(k_link_colour, 128, nsc, 64, P, S, vd, *a.dem, c.s[1].off, c.s[1].off + 1, c.active, col,
                         a.dynamic);
@@ -1214,11 +1214,12 @@ static int connect_links(const DevParams& P, snowb_particle_data* dem, uint32_t 
     LAUNCH(k_boundary_prep, n, 256, dcd, dem->mass, dem->massInv, dem->mass, n, c.s[1].p4, c.s[1].invm, c.s[1].lambda,
            sid, sid ? c.s[1].sid : nullptr);
     SetView vd = make_view(dcd, c.s[1].p4, dem->mass, sid ? c.s[1].sid : nullptr);
-    LAUNCH(k_link_filter, n, 128, P, c.S, vd, *dem, dynamic, c.active);
+    LAUNCH(k_link_filter, n, 128, P, c.S, vd, *dem, dynamic, c.active, NList{nullptr, nullptr, 0u, 0u});
     const uint32_t nsc = (P.gsx / 4) * (P.gsy / 4) * (P.gsz / 4);
     for (uint32_t col = 0; col < 8; ++col) {
         if (P.maxc <= SNOWB_MAXC_FAST)
-            LAUNCH(k_link_colour_warp, (uint64_t)nsc * 32, 128, P, c.S, vd, *dem, c.fs, c.fe, c.active, col, dynamic);
+            LAUNCH(k_link_colour_warp, (uint64_t)nsc * 32, 128, P, c.S, vd, *dem, c.fs, c.fe, c.active, col, dynamic,
+                   NList{nullptr, nullptr, 0u, 0u});
         else
             LAUNCH(k_link_colour, nsc, 64, P, c.S, vd, *dem, c.fs, c.fe, c.active, col, dynamic);
     }

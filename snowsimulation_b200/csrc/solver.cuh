@@ -346,9 +346,12 @@ __global__ void __launch_bounds__(256) k_density(DevParams P, DevState* __restri
             const Nbhd nb = make_nbhd(P, g, p, P.h2_cull);
             rho = D->mass[o] * P.W0;
             NLWriter wr{L.e, L.stride, (w ? 0u : L.cap) + i, 0u};
-            NLWriter* pw = LAMBDA ? &wr : nullptr;
+            // the density+lambda pass lists all three sets for the PBF and contact passes; the
+            // substep's first density pass lists the snow-snow candidates for link formation
+            NLWriter* pw = (LAMBDA || !w) ? &wr : nullptr;
             acc_WG<LAMBDA>(P, rho, gs, own, p, nb, i, false, 0, 0.f, nullptr, nullptr, pw, 0);
             const uint32_t n_own = wr.n;
+            if (!LAMBDA) pw = nullptr;
             acc_WG<LAMBDA>(P, rho, gs, oth, p, nb, SNOWB_UMAX, false, 0, 0.f, nullptr, nullptr, pw, 1);
             const uint32_t n_oth = wr.n - n_own;
             acc_WG<LAMBDA>(P, rho, gs, vb, p, nb, SNOWB_UMAX, true, 1, D->mass[o], nullptr, nullptr, pw, 2);
@@ -356,6 +359,8 @@ __global__ void __launch_bounds__(256) k_density(DevParams P, DevState* __restri
                 const uint32_t n_bnd = wr.n - n_own - n_oth;
                 L.cnt[wr.slot] = wr.n > NLIST_K ? NL_OVF : (n_own | (n_oth << 10) | (n_bnd << 20));
                 if (wr.n > NLIST_K) atomicAdd(&S->n_nl_ovf, 1u);
+            } else if (!w) {
+                L.cnt[wr.slot] = n_own > NLIST_K ? NL_OVF : n_own;
             }
         } else {
             // boundary: density visits (b, snow, water), lambda (b, water, snow)
@@ -552,9 +557,12 @@ __global__ void k_interlink(DevParams P, const DevState* __restrict__ S, snowb_p
 {
     const uint32_t nd = S->n_dem, M = P.maxc;
     const float3 z = f3(0.f, 0.f, 0.f);
+    // Plain (cached) loads: a record that a partner deletes during the pass is one whose term
+    // is zero at both ends (same length, same distance), so whether this thread still sees it,
+    // or sees its length already zeroed, the term it adds is the same zero.
+    const uint32_t* rec = dem.connect_record;
+    const float* len = dem.connect_length;
     GRID_LOOP(o, nd) {
-        volatile const uint32_t* rec = dem.connect_record;
-        volatile const float* len = dem.connect_length;
         float3 d = z;
         for (uint32_t s = M * o; s < M * (o + 1); ++s) {
             const uint32_t j = rec[s];
