@@ -247,6 +247,24 @@ int snowb_batch_snow_simulation(const snowb_batch* batch,
                                 int dynamic_max_connections, int cd_on, float temperature_variation,
                                 const snowb_step_options* options);
 
+/* ---- frame export (GLFWApp::ExportBgeoFile, GLFWApp.cpp:287-405) -------------------------
+ * One Houdini .bgeo file per set and frame with the reference's point attributes: position,
+ * Cd (rgb, 3 floats), pscale (1 float) and label (1 int; the reference stores the bit
+ * pattern of the float label, float_label = 1, which makes the file identical to its
+ * output; 0 stores the integer).  The reference uses colours (0.7, 0.7, 1) for water and
+ * (0.85, 0.85, 0.85) for snow, pscale = particle radius, label 0 water and 1 snow. */
+int snowb_export_bgeo(const snowb_particle_data* set, uint32_t n, const char* path, const float* rgb, float pscale,
+                      int label, int float_label);
+/* The same, asynchronous: the positions are copied to pinned memory on the library's
+ * stream (ordered after the work already issued) and a host thread writes the file;
+ * snowb_export_wait joins all pending exports and reports the first failure. */
+int snowb_export_bgeo_async(const snowb_particle_data* set, uint32_t n, const char* path, const float* rgb,
+                            float pscale, int label, int float_label);
+int snowb_export_wait(void);
+/* The writer alone, from host memory (n points of 3 floats); needs no GPU. */
+int snowb_write_bgeo_host(const float* positions, uint32_t n, const char* path, const float* rgb, float pscale,
+                          int label, int float_label);
+
 /* ---- autotuner (no reference counterpart) ------------------------------------------------
  * Times the tunable kernels of the substep (neighbour passes, link colouring, apply) under
  * nine launch shapes (64/128/256 threads per block x grid caps of 8/16/64 blocks per SM),

@@ -39,6 +39,7 @@ EXPORTS = (
     "snowb_adjoint_begin", "snowb_adjoint_end", "snowb_adjoint_backward", "snowb_adjoint_release",
     "snowb_autotune", "snowb_autotune_table", "snowb_autotune_load", "snowb_autotune_reset",
     "snowb_set_domain",
+    "snowb_export_bgeo", "snowb_export_bgeo_async", "snowb_export_wait", "snowb_write_bgeo_host",
 )
 
 _lib = None
@@ -102,6 +103,10 @@ def load(path=LIB_PATH):
         "snowb_autotune_load": [C.c_char_p],
         "snowb_autotune_reset": [],
         "snowb_set_domain": [f, f, f, f, f],
+        "snowb_export_bgeo": [PPD, u32, C.c_char_p, C.POINTER(C.c_float), f, i, i],
+        "snowb_export_bgeo_async": [PPD, u32, C.c_char_p, C.POINTER(C.c_float), f, i, i],
+        "snowb_export_wait": [],
+        "snowb_write_bgeo_host": [C.c_void_p, u32, C.c_char_p, C.POINTER(C.c_float), f, i, i],
     })
     for name, args in sig.items():
         fn = getattr(lib, name)

@@ -19,6 +19,7 @@
 #include "solver.cuh"
 #include "phase.cuh"
 #include "adjoint.cuh"
+#include "export.cuh"
 
 namespace snowb {
 
@@ -1637,6 +1638,78 @@ int snowb_autotune_reset(void)
 {
     g_tune.clear();
     ++g_tune_gen;
+    return SNOWB_OK;
+}
+
+// ------------------------------------------------------------------ .bgeo export
+int snowb_write_bgeo_host(const float* positions, uint32_t n, const char* path, const float* rgb, float pscale,
+                          int label, int float_label)
+{
+    if (!path || !rgb || (n && !positions)) return fail(SNOWB_ERR_INVALID, "null pointer");
+    std::string err;
+    if (bgeo_write(path, positions, n, rgb, pscale, label, float_label, err) != 0) return fail(SNOWB_ERR_INVALID, err);
+    return SNOWB_OK;
+}
+
+int snowb_export_bgeo(const snowb_particle_data* set, uint32_t n, const char* path, const float* rgb, float pscale,
+                      int label, int float_label)
+{
+    if (!set || !path || !rgb) return fail(SNOWB_ERR_INVALID, "null pointer");
+    float* h = nullptr;
+    if (n) {
+        CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&h), (size_t)n * 12));
+        cudaError_t e = cudaMemcpyAsync(h, set->positions, (size_t)n * 12, cudaMemcpyDeviceToHost, g_stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(g_stream);
+        if (e != cudaSuccess) { cudaFreeHost(h); return fail(SNOWB_ERR_CUDA, cudaGetErrorString(e)); }
+    }
+    std::string err;
+    const int rc = bgeo_write(path, h, n, rgb, pscale, label, float_label, err);
+    if (h) cudaFreeHost(h);
+    if (rc != 0) return fail(SNOWB_ERR_INVALID, err);
+    return SNOWB_OK;
+}
+
+int snowb_export_bgeo_async(const snowb_particle_data* set, uint32_t n, const char* path, const float* rgb,
+                            float pscale, int label, int float_label)
+{
+    if (!set || !path || !rgb) return fail(SNOWB_ERR_INVALID, "null pointer");
+    ExportJob* job = new ExportJob();
+    if (n) {
+        cudaError_t e = cudaMallocHost(reinterpret_cast<void**>(&job->staging), (size_t)n * 12);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&job->ev, cudaEventDisableTiming);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(job->staging, set->positions, (size_t)n * 12, cudaMemcpyDeviceToHost, g_stream);
+        if (e == cudaSuccess) e = cudaEventRecord(job->ev, g_stream);
+        if (e != cudaSuccess) {
+            if (job->staging) cudaFreeHost(job->staging);
+            if (job->ev) cudaEventDestroy(job->ev);
+            delete job;
+            return fail(SNOWB_ERR_CUDA, cudaGetErrorString(e));
+        }
+    }
+    const std::string file(path);
+    const float col[3] = {rgb[0], rgb[1], rgb[2]};
+    job->th = std::thread([job, file, n, col, pscale, label, float_label]() {
+        if (job->ev && cudaEventSynchronize(job->ev) != cudaSuccess) { job->rc = -1; job->err = "copy failed"; return; }
+        job->rc = bgeo_write(file.c_str(), job->staging, n, col, pscale, label, float_label, job->err);
+    });
+    g_exports.push_back(job);
+    return SNOWB_OK;
+}
+
+int snowb_export_wait(void)
+{
+    int rc = SNOWB_OK;
+    std::string err;
+    for (ExportJob* job : g_exports) {
+        job->th.join();
+        if (job->rc != 0 && rc == SNOWB_OK) { rc = SNOWB_ERR_INVALID; err = job->err; }
+        if (job->staging) cudaFreeHost(job->staging);
+        if (job->ev) cudaEventDestroy(job->ev);
+        delete job;
+    }
+    g_exports.clear();
+    if (rc != SNOWB_OK) return fail(rc, err);
     return SNOWB_OK;
 }
 
