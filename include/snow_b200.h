@@ -247,6 +247,33 @@ int snowb_batch_snow_simulation(const snowb_batch* batch,
                                 int dynamic_max_connections, int cd_on, float temperature_variation,
                                 const snowb_step_options* options);
 
+/* ---- point-sprite rendering (point_sprite_vs.glsl, point_sprite_temperature_vs.glsl,
+ * point_sprite_fs.glsl; Renderer.cpp draws with them) --------------------------------------
+ * The reference shades its particles with these OpenGL shaders.  The same vertex and
+ * fragment arithmetic runs here as CUDA kernels into a device image (RGBA float,
+ * width x height, row 0 at the bottom like a GL framebuffer) with a 64-bit depth/id buffer,
+ * no graphics API involved.  Depth test LESS in draw order; up to 32 draws (sets) between
+ * clears, `draw` numbering them in drawing order. */
+typedef struct snowb_camera {
+    float view[16];          /* column-major, as the reference's glm matrices */
+    float projection[16];
+    float camera_pos[3];
+    float light_pos[3];      /* view space, like the shaders' light_pos uniform */
+    float point_size;        /* sprite side in pixels at distance 1 (Renderer::m_point_size) */
+    uint32_t width, height;
+} snowb_camera;
+typedef struct snowb_point_colour {
+    float rgb[3];            /* point_color */
+    int use_temperature;     /* 1: the temperature shader (colour from the set's T) */
+    float coolest_rgb[3], hottest_rgb[3];
+    float coolest_T, hottest_T;
+} snowb_point_colour;
+/* Clear the image to (0, 0, 0, 0) and the depth buffer to far. */
+int snowb_render_clear(const snowb_camera* cam, float* rgba, unsigned long long* zbuf);
+/* Draw the first n particles of a set (positions, and T for the temperature colours). */
+int snowb_render_points(const snowb_particle_data* set, uint32_t n, const snowb_camera* cam,
+                        const snowb_point_colour* colour, uint32_t draw, float* rgba, unsigned long long* zbuf);
+
 /* ---- frame export (GLFWApp::ExportBgeoFile, GLFWApp.cpp:287-405) -------------------------
  * One Houdini .bgeo file per set and frame with the reference's point attributes: position,
  * Cd (rgb, 3 floats), pscale (1 float) and label (1 int; the reference stores the bit

@@ -40,6 +40,7 @@ EXPORTS = (
     "snowb_autotune", "snowb_autotune_table", "snowb_autotune_load", "snowb_autotune_reset",
     "snowb_set_domain",
     "snowb_export_bgeo", "snowb_export_bgeo_async", "snowb_export_wait", "snowb_write_bgeo_host",
+    "snowb_render_clear", "snowb_render_points",
 )
 
 _lib = None
@@ -107,6 +108,9 @@ def load(path=LIB_PATH):
         "snowb_export_bgeo_async": [PPD, u32, C.c_char_p, C.POINTER(C.c_float), f, i, i],
         "snowb_export_wait": [],
         "snowb_write_bgeo_host": [C.c_void_p, u32, C.c_char_p, C.POINTER(C.c_float), f, i, i],
+        # camera and colour structs (render.py) are passed by address
+        "snowb_render_clear": [C.c_void_p, C.c_void_p, C.c_void_p],
+        "snowb_render_points": [PPD, u32, C.c_void_p, C.c_void_p, u32, C.c_void_p, C.c_void_p],
     })
     for name, args in sig.items():
         fn = getattr(lib, name)

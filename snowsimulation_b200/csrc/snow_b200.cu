@@ -20,6 +20,7 @@
 #include "phase.cuh"
 #include "adjoint.cuh"
 #include "export.cuh"
+#include "render.cuh"
 
 namespace snowb {
 
@@ -1638,6 +1639,53 @@ int snowb_autotune_reset(void)
 {
     g_tune.clear();
     ++g_tune_gen;
+    return SNOWB_OK;
+}
+
+// ------------------------------------------------------------------ point-sprite rendering
+static int render_cam(const snowb_camera* cam, RenderCam& c)
+{
+    if (!cam) return fail(SNOWB_ERR_INVALID, "null camera");
+    if (cam->width == 0 || cam->height == 0 || (uint64_t)cam->width * cam->height > (1ull << 28))
+        return fail(SNOWB_ERR_INVALID, "image size out of range");
+    std::memcpy(c.V, cam->view, sizeof(c.V));
+    std::memcpy(c.Pm, cam->projection, sizeof(c.Pm));
+    std::memcpy(c.cam, cam->camera_pos, sizeof(c.cam));
+    std::memcpy(c.light, cam->light_pos, sizeof(c.light));
+    c.point_size = cam->point_size;
+    c.W = cam->width;
+    c.H = cam->height;
+    return SNOWB_OK;
+}
+
+int snowb_render_clear(const snowb_camera* cam, float* rgba, unsigned long long* zbuf)
+{
+    RenderCam c;
+    TRY(render_cam(cam, c));
+    if (!rgba || !zbuf) return fail(SNOWB_ERR_INVALID, "null image");
+    LAUNCH(kr_clear, (uint64_t)c.W * c.H, 256, c.W * c.H, zbuf, rgba);
+    return SNOWB_OK;
+}
+
+int snowb_render_points(const snowb_particle_data* set, uint32_t n, const snowb_camera* cam,
+                        const snowb_point_colour* colour, uint32_t draw, float* rgba, unsigned long long* zbuf)
+{
+    RenderCam c;
+    TRY(render_cam(cam, c));
+    if (!set || !colour || !rgba || !zbuf) return fail(SNOWB_ERR_INVALID, "null pointer");
+    if (draw > 31) return fail(SNOWB_ERR_INVALID, "at most 32 draws between clears");
+    if (n >= (1u << 27)) return fail(SNOWB_ERR_INVALID, "more than 2^27 particles in one draw");
+    if (n == 0) return SNOWB_OK;
+    RenderColour rc;
+    std::memcpy(rc.rgb, colour->rgb, sizeof(rc.rgb));
+    rc.temp = colour->use_temperature ? 1 : 0;
+    std::memcpy(rc.cool, colour->coolest_rgb, sizeof(rc.cool));
+    std::memcpy(rc.hot, colour->hottest_rgb, sizeof(rc.hot));
+    rc.t_cool = colour->coolest_T;
+    rc.t_hot = colour->hottest_T;
+    const float* T = rc.temp ? set->T : nullptr;
+    LAUNCH(kr_depth, n, 128, c, rc, set->positions, T, n, draw, zbuf);
+    LAUNCH(kr_shade, (uint64_t)c.W * c.H, 256, c, rc, set->positions, T, draw, zbuf, rgba);
     return SNOWB_OK;
 }
 
