@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-large", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--profile-out", default="")
     return ap.parse_args()
 
@@ -146,6 +147,44 @@ def cpu_baseline(scene_name, max_seconds=25.0, max_substeps=None):
     return {"value": n * done / el, "unit": UNIT, "cores": cores, "kind": "port",
             "sample": "%d substep(s) of %s (%d particles), FP32 C oracle, OpenMP %d threads, %.1f s"
                       % (done, scene_name, n, cores, el)}
+
+
+# ----------------------------------------------------------------- error vs FP64
+def fp64_error(scene_name, dev, frames=2):
+    """The GPU run of the timed scene against the FP64 oracle from the same start, frame by
+    frame (particles matched by track id): maximum position and temperature differences."""
+    import numpy as np
+    from snowsimulation_b200 import scene
+    from snowsimulation_b200.world import Simulation
+    from oracle.oracle import OracleWorld
+    w = getattr(scene, scene_name)()
+    sim = Simulation(w, device=dev).setup()
+    o = OracleWorld(w, 64, threads=os.cpu_count() or 1).setup()
+    out = []
+
+    def by_id(world_sets):
+        ids, xs, ts = [], [], []
+        for d, n in world_sets:
+            ids.append(d["trackId"][:n]); xs.append(d["positions"][:n]); ts.append(d["T"][:n])
+        ids = np.concatenate(ids)
+        order = np.argsort(ids)
+        return ids[order], np.concatenate(xs)[order].astype(np.float64), np.concatenate(ts)[order].astype(np.float64)
+
+    for f in range(frames):
+        sim.step(substeps=SUBSTEPS)
+        for _ in range(SUBSTEPS):
+            o.step()
+        H = sim.to_host()
+        ig, xg, tg = by_id(((H.sph, H.n_sph), (H.dem, H.n_dem)))
+        io, xo, to = by_id(((o.w.sph, o.w.n_sph), (o.w.dem, o.w.n_dem)))
+        same = np.array_equal(ig, io)
+        rec = {"frame": f, "same_particles": bool(same), "sizes": [H.n_sph, H.n_dem]}
+        if same:
+            rec["pos_max_m"] = float(np.abs(xg - xo).max())
+            rec["T_max_C"] = float(np.abs(tg - to).max())
+        out.append(rec)
+    return {"workload": "%s from rest, %d frames of %d substeps" % (scene_name, frames, SUBSTEPS),
+            "oracle": "FP64 C restatement of the substep (oracle/), reference quirks", "per_frame": out}
 
 
 # ----------------------------------------------------------------- reference arm
@@ -539,6 +578,8 @@ def main():
         line["large"] = large_res
     if ws == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.scene)
+    if ws == 1 and not args.no_fp64:
+        line["fp64_error"] = fp64_error(args.scene, dev)
     print(json.dumps(line))
     if ws > 1:
         dist.destroy_process_group()
