@@ -149,6 +149,38 @@ def cpu_baseline(scene_name, max_seconds=25.0, max_substeps=None):
                       % (done, scene_name, n, cores, el)}
 
 
+def reference_cpu_baselines(water_pos, snow_pos, links, snow_mass, h, dt, iters=3, max_seconds=4.0):
+    """The reference's own CPU code near this path, timed on the host (reported baselines;
+    neither routine is the substep): NeighborSearch::SpatialSearch over the water set, and
+    ConstraintSolver::SolveXPBDConstraints over one distance constraint per interlink of the
+    scene at rest, `iters` iterations (the interlink stage of one substep)."""
+    from oracle import cpu_ref
+    if not cpu_ref.available():
+        return {"unavailable": "oracle/_ref/libsnowcpuref.so not built (needs the reference sources)"}
+    out = {}
+    nw = len(water_pos)
+    _, t1 = cpu_ref.spatial_search(water_pos, h, calls=1)
+    calls = int(max(1, min(500, max_seconds / max(t1, 1e-6))))
+    pairs, sec = cpu_ref.spatial_search(water_pos, h, calls=calls)
+    out["spatial_search"] = {
+        "value": nw / sec, "unit": "particles searched/s", "cores": cpu_ref.SPATIAL_SEARCH_THREADS,
+        "kind": "reference",
+        "sample": "NeighborSearch::SpatialSearch (NeighborSearch.cpp:154-259) on the %d water particles, "
+                  "radius %.3f m, its fixed 1 m hash grid; %d calls, %.3f ms per call, %d neighbour pairs"
+                  % (nw, h, calls, sec * 1e3, pairs)}
+    a, b, rest = links
+    _, t1 = cpu_ref.xpbd_links(snow_pos, a, b, rest, snow_mass, dt, iters=iters, calls=1)
+    calls = int(max(1, min(20, max_seconds / max(t1, 1e-6))))
+    _, sec = cpu_ref.xpbd_links(snow_pos, a, b, rest, snow_mass, dt, iters=iters, calls=calls)
+    out["xpbd_links"] = {
+        "value": len(a) * iters / sec, "unit": "constraint projections/s", "cores": cpu_ref.XPBD_THREADS,
+        "kind": "reference",
+        "sample": "ConstraintSolver::SolveXPBDConstraints (ConstraintSolver.cpp:51-72) over %d DistanceConstraints "
+                  "(the scene's interlinks at rest) on %d snow particles, %d iterations; %d solves, %.1f ms per solve"
+                  % (len(a), len(snow_pos), iters, calls, sec * 1e3)}
+    return out
+
+
 # ----------------------------------------------------------------- error vs FP64
 def fp64_error(scene_name, dev, frames=2):
     """The GPU run of the timed scene against the FP64 oracle from the same start, frame by
@@ -401,6 +433,14 @@ def main():
     sim = Simulation(w, device=dev).setup()
     lib = sim.lib
     n_part = w.n_sph + w.n_dem
+    rest_state = None
+    if ws == 1 and not args.no_cpu_baseline:
+        from oracle import cpu_ref
+        H0 = sim.to_host()
+        rest_state = (H0.sph["positions"][: H0.n_sph].copy(), H0.dem["positions"][: H0.n_dem].copy(),
+                      cpu_ref.link_pairs(H0.dem["connect_record"], H0.dem["connect_length"], H0.n_dem, H0.maxc),
+                      float(H0.dem["mass"][0]))
+        del H0
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)   # > 126 MB L2
 
@@ -578,6 +618,9 @@ def main():
         line["large"] = large_res
     if ws == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.scene)
+        line["cpu_baseline"]["reference_cpu"] = reference_cpu_baselines(
+            rest_state[0], rest_state[1], rest_state[2], rest_state[3], h=float(w.params.effective_radius),
+            dt=1.0 / (60.0 * SUBSTEPS))
     if ws == 1 and not args.no_fp64:
         line["fp64_error"] = fp64_error(args.scene, dev)
     print(json.dumps(line))
