@@ -273,6 +273,50 @@ int snowb_render_clear(const snowb_camera* cam, float* rgba, unsigned long long*
 /* Draw the first n particles of a set (positions, and T for the temperature colours). */
 int snowb_render_points(const snowb_particle_data* set, uint32_t n, const snowb_camera* cam,
                         const snowb_point_colour* colour, uint32_t draw, float* rgba, unsigned long long* zbuf);
+/* The same clear with a clear colour (Renderer::ClearBuffer, m_clear_color). */
+int snowb_render_clear_colour(const snowb_camera* cam, const float* clear_rgba, float* rgba, unsigned long long* zbuf);
+
+/* ---- screen-space fluid (the reference's default view: Renderer::Render with
+ * m_b_render_fluid, Renderer.cpp:92-109, through RenderSceneDepth, RenderFluidDepth,
+ * SmoothDepth, RenderThickness and RenderFluid :404-690; shaders point_depth_*.glsl,
+ * bilateral_fs.glsl, ssfr_thickness_*.glsl, ssfr_fluid_fs.glsl) ----------------------------
+ * The snow is drawn as point sprites into a scene image and as sphere depth; the water as
+ * sphere depth (smoothed by a separable bilateral filter) and additive thickness; a
+ * full-screen composite refracts the scene through the water surface.  Images are
+ * width x height, row 0 at the bottom; depth maps hold the clip depth z/w clamped to 0..1
+ * (1 = empty), thickness is 32.32 fixed point (sum of n.z * 0.005 per covered pixel). */
+typedef struct snowb_ssfr {
+    float sphere_radius;       /* point_depth_fs sphere_radius (the particle radius) */
+    float filter_radius;       /* bilateral half-width in texels (SmoothDepth: 10) */
+    float blur_scale;          /* SmoothDepth: 0.1 */
+    float blur_depth_falloff;  /* bilateral_fs.glsl: 65 */
+    float light_color[4];      /* RenderFluid: (1, 1, 1, 0.8) */
+    float clear_color[4];      /* Renderer::m_clear_color: (0.15, 0.15, 0.15, 0) */
+} snowb_ssfr;
+/* Device workspace of snowb_render_fluid for the camera's image size (48 bytes a pixel). */
+int snowb_ssfr_workspace_bytes(const snowb_camera* cam, uint64_t* bytes);
+/* The whole view into rgba (width x height x 4 floats): n_dem snow particles in
+ * snow_colour, n_sph water particles as the fluid surface.  workspace: 16-byte aligned,
+ * snowb_ssfr_workspace_bytes long. */
+int snowb_render_fluid(const snowb_particle_data* sph, uint32_t n_sph, const snowb_particle_data* dem, uint32_t n_dem,
+                       const snowb_camera* cam, const snowb_point_colour* snow_colour, const snowb_ssfr* ssfr,
+                       void* workspace, float* rgba);
+/* Its stages.  depth := 1 and thick := 0 (either may be NULL). */
+int snowb_ssfr_clear(const snowb_camera* cam, float* depth, unsigned long long* thick);
+/* Sphere depth of the first n particles of a set (minimum into depth). */
+int snowb_ssfr_sphere_depth(const snowb_particle_data* set, uint32_t n, const snowb_camera* cam, const snowb_ssfr* ssfr,
+                            float* depth);
+/* Thickness of the first n particles (added into thick). */
+int snowb_ssfr_thickness(const snowb_particle_data* set, uint32_t n, const snowb_camera* cam, unsigned long long* thick);
+/* Bilateral smoothing, along y into tmp, then along x into out. */
+int snowb_ssfr_smooth(const snowb_camera* cam, const snowb_ssfr* ssfr, const float* depth, float* tmp, float* out);
+/* Full-screen composite of the smoothed water depth, its thickness, the scene image and the
+ * scene depth into rgba. */
+int snowb_ssfr_compose(const snowb_camera* cam, const snowb_ssfr* ssfr, const float* depth,
+                       const unsigned long long* thick, const float* scene_rgba, const float* scene_depth, float* rgba);
+/* The matrices the kernels use: projection * view, view, projection, inverse projection,
+ * inverse view (5 x 16 floats, column-major). */
+int snowb_ssfr_matrices(const snowb_camera* cam, float* out80);
 
 /* ---- frame export (GLFWApp::ExportBgeoFile, GLFWApp.cpp:287-405) -------------------------
  * One Houdini .bgeo file per set and frame with the reference's point attributes: position,

@@ -40,7 +40,9 @@ EXPORTS = (
     "snowb_autotune", "snowb_autotune_table", "snowb_autotune_load", "snowb_autotune_reset",
     "snowb_set_domain",
     "snowb_export_bgeo", "snowb_export_bgeo_async", "snowb_export_wait", "snowb_write_bgeo_host",
-    "snowb_render_clear", "snowb_render_points",
+    "snowb_render_clear", "snowb_render_points", "snowb_render_clear_colour",
+    "snowb_ssfr_workspace_bytes", "snowb_render_fluid", "snowb_ssfr_clear", "snowb_ssfr_sphere_depth",
+    "snowb_ssfr_thickness", "snowb_ssfr_smooth", "snowb_ssfr_compose", "snowb_ssfr_matrices",
 )
 
 _lib = None
@@ -111,6 +113,15 @@ def load(path=LIB_PATH):
         # camera and colour structs (render.py) are passed by address
         "snowb_render_clear": [C.c_void_p, C.c_void_p, C.c_void_p],
         "snowb_render_points": [PPD, u32, C.c_void_p, C.c_void_p, u32, C.c_void_p, C.c_void_p],
+        "snowb_render_clear_colour": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
+        "snowb_ssfr_workspace_bytes": [C.c_void_p, C.POINTER(C.c_uint64)],
+        "snowb_render_fluid": [PPD, u32, PPD, u32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
+        "snowb_ssfr_clear": [C.c_void_p, C.c_void_p, C.c_void_p],
+        "snowb_ssfr_sphere_depth": [PPD, u32, C.c_void_p, C.c_void_p, C.c_void_p],
+        "snowb_ssfr_thickness": [PPD, u32, C.c_void_p, C.c_void_p],
+        "snowb_ssfr_smooth": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
+        "snowb_ssfr_compose": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
+        "snowb_ssfr_matrices": [C.c_void_p, C.c_void_p],
     })
     for name, args in sig.items():
         fn = getattr(lib, name)

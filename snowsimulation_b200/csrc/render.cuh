@@ -79,12 +79,20 @@ __device__ __forceinline__ void sprite_span(float c, float side, uint32_t lim, i
     if (a < 0) a = 0;
     if (b > (int)lim) b = (int)lim;
 }
+// gl_PointCoord * 2 - 1 of pixel (px, py) in a sprite of side `side` centred at (xw, yw)
+// (upper-left point-coordinate origin)
+__device__ __forceinline__ void point_coord(float xw, float yw, float side, int px, int py, float& nx, float& ny)
+{
+    const float pcx = (((float)px + 0.5f) - (xw - 0.5f * side)) / side;
+    const float pcy = ((yw + 0.5f * side) - ((float)py + 0.5f)) / side;
+    nx = pcx * 2.f - 1.f;
+    ny = pcy * 2.f - 1.f;
+}
 // fragment: false when discarded; shaded colour in rgb
 __device__ __forceinline__ bool sprite_fragment(const SpriteVtx& v, int px, int py, float3& rgb)
 {
-    const float pcx = (((float)px + 0.5f) - (v.xw - 0.5f * v.side)) / v.side;
-    const float pcy = ((v.yw + 0.5f * v.side) - ((float)py + 0.5f)) / v.side;
-    const float nx = pcx * 2.f - 1.f, ny = pcy * 2.f - 1.f;
+    float nx, ny;
+    point_coord(v.xw, v.yw, v.side, px, py, nx, ny);
     float nz = 1.f - (nx * nx + ny * ny);
     if (nz < 0.f) return false;
     nz = sqrtf(nz);
@@ -130,12 +138,12 @@ __global__ void kr_shade(RenderCam c, RenderColour rc, const snowb_float3* __res
         rgba[4 * (size_t)k + 3] = 1.f;
     }
 }
-__global__ void kr_clear(uint32_t npix, unsigned long long* zbuf, float* rgba)
+__global__ void kr_clear(uint32_t npix, unsigned long long* zbuf, float* rgba, float4 clear)
 {
     GRID_LOOP(k, npix) {
         zbuf[k] = ~0ull;
-        rgba[4 * (size_t)k] = 0.f; rgba[4 * (size_t)k + 1] = 0.f; rgba[4 * (size_t)k + 2] = 0.f;
-        rgba[4 * (size_t)k + 3] = 0.f;
+        rgba[4 * (size_t)k] = clear.x; rgba[4 * (size_t)k + 1] = clear.y; rgba[4 * (size_t)k + 2] = clear.z;
+        rgba[4 * (size_t)k + 3] = clear.w;
     }
 }
 

@@ -21,6 +21,7 @@
 #include "adjoint.cuh"
 #include "export.cuh"
 #include "render.cuh"
+#include "ssfr.cuh"
 
 namespace snowb {
 
@@ -1663,7 +1664,17 @@ int snowb_render_clear(const snowb_camera* cam, float* rgba, unsigned long long*
     RenderCam c;
     TRY(render_cam(cam, c));
     if (!rgba || !zbuf) return fail(SNOWB_ERR_INVALID, "null image");
-    LAUNCH(kr_clear, (uint64_t)c.W * c.H, 256, c.W * c.H, zbuf, rgba);
+    LAUNCH(kr_clear, (uint64_t)c.W * c.H, 256, c.W * c.H, zbuf, rgba, make_float4(0.f, 0.f, 0.f, 0.f));
+    return SNOWB_OK;
+}
+
+int snowb_render_clear_colour(const snowb_camera* cam, const float* clear_rgba, float* rgba, unsigned long long* zbuf)
+{
+    RenderCam c;
+    TRY(render_cam(cam, c));
+    if (!rgba || !zbuf || !clear_rgba) return fail(SNOWB_ERR_INVALID, "null pointer");
+    LAUNCH(kr_clear, (uint64_t)c.W * c.H, 256, c.W * c.H, zbuf, rgba,
+           make_float4(clear_rgba[0], clear_rgba[1], clear_rgba[2], clear_rgba[3]));
     return SNOWB_OK;
 }
 
@@ -1686,6 +1697,179 @@ int snowb_render_points(const snowb_particle_data* set, uint32_t n, const snowb_
     const float* T = rc.temp ? set->T : nullptr;
     LAUNCH(kr_depth, n, 128, c, rc, set->positions, T, n, draw, zbuf);
     LAUNCH(kr_shade, (uint64_t)c.W * c.H, 256, c, rc, set->positions, T, draw, zbuf, rgba);
+    return SNOWB_OK;
+}
+
+// ------------------------------------------------------------------ screen-space fluid
+// 4x4 column-major product A * B in glm's order: column c = ((A0 b0 + A1 b1) + A2 b2) + A3 b3
+static void mat_mul(const float* A, const float* B, float* out)
+{
+    for (int c = 0; c < 4; ++c)
+        for (int r = 0; r < 4; ++r)
+            out[c * 4 + r] = ((A[r] * B[c * 4] + A[4 + r] * B[c * 4 + 1]) + A[8 + r] * B[c * 4 + 2]) +
+                             A[12 + r] * B[c * 4 + 3];
+}
+// inverse of a column-major 4x4 (Gauss-Jordan with partial pivoting in double, rounded to
+// float); false when singular
+static bool mat_inv(const float* M, float* out)
+{
+    double a[4][8];
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c) {
+            a[r][c] = M[c * 4 + r];
+            a[r][4 + c] = r == c ? 1.0 : 0.0;
+        }
+    for (int k = 0; k < 4; ++k) {
+        int piv = k;
+        for (int r = k + 1; r < 4; ++r)
+            if (std::fabs(a[r][k]) > std::fabs(a[piv][k])) piv = r;
+        if (a[piv][k] == 0.0) return false;
+        if (piv != k)
+            for (int c = 0; c < 8; ++c) std::swap(a[k][c], a[piv][c]);
+        const double d = a[k][k];
+        for (int c = 0; c < 8; ++c) a[k][c] /= d;
+        for (int r = 0; r < 4; ++r) {
+            if (r == k) continue;
+            const double f = a[r][k];
+            if (f != 0.0)
+                for (int c = 0; c < 8; ++c) a[r][c] -= f * a[k][c];
+        }
+    }
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c) out[c * 4 + r] = (float)a[r][4 + c];
+    return true;
+}
+static int ssfr_cam(const snowb_camera* cam, const snowb_ssfr* ss, SsfrCam& c)
+{
+    RenderCam rc;
+    TRY(render_cam(cam, rc));
+    std::memcpy(c.V, cam->view, sizeof(c.V));
+    std::memcpy(c.P, cam->projection, sizeof(c.P));
+    mat_mul(c.P, c.V, c.PV);
+    if (!mat_inv(c.P, c.Pinv) || !mat_inv(c.V, c.Vinv)) return fail(SNOWB_ERR_INVALID, "singular camera matrix");
+    c.point_size = cam->point_size;
+    c.radius = ss ? ss->sphere_radius : 0.f;
+    c.W = cam->width;
+    c.H = cam->height;
+    return SNOWB_OK;
+}
+static int ssfr_shade(const snowb_ssfr* ss, SsfrShade& s)
+{
+    if (!ss) return fail(SNOWB_ERR_INVALID, "null ssfr parameters");
+    if (!(ss->filter_radius >= 0.f && ss->filter_radius <= 256.f)) return fail(SNOWB_ERR_INVALID, "filter radius out of 0..256");
+    s.filter_radius = ss->filter_radius;
+    s.blur_scale = ss->blur_scale;
+    s.falloff = ss->blur_depth_falloff;
+    std::memcpy(s.light, ss->light_color, sizeof(s.light));
+    std::memcpy(s.clear, ss->clear_color, sizeof(s.clear));
+    return SNOWB_OK;
+}
+
+int snowb_ssfr_matrices(const snowb_camera* cam, float* out80)
+{
+    SsfrCam c;
+    TRY(ssfr_cam(cam, nullptr, c));
+    if (!out80) return fail(SNOWB_ERR_INVALID, "null output");
+    std::memcpy(out80, c.PV, 64);
+    std::memcpy(out80 + 16, c.V, 64);
+    std::memcpy(out80 + 32, c.P, 64);
+    std::memcpy(out80 + 48, c.Pinv, 64);
+    std::memcpy(out80 + 64, c.Vinv, 64);
+    return SNOWB_OK;
+}
+
+int snowb_ssfr_clear(const snowb_camera* cam, float* depth, unsigned long long* thick)
+{
+    SsfrCam c;
+    TRY(ssfr_cam(cam, nullptr, c));
+    if (!depth && !thick) return SNOWB_OK;
+    LAUNCH(ks_fill, (uint64_t)c.W * c.H, 256, c.W * c.H, reinterpret_cast<uint32_t*>(depth), 0x3f800000u, thick);
+    return SNOWB_OK;
+}
+
+int snowb_ssfr_sphere_depth(const snowb_particle_data* set, uint32_t n, const snowb_camera* cam, const snowb_ssfr* ssfr,
+                            float* depth)
+{
+    SsfrCam c;
+    TRY(ssfr_cam(cam, ssfr, c));
+    if (!set || !ssfr || !depth) return fail(SNOWB_ERR_INVALID, "null pointer");
+    if (n == 0) return SNOWB_OK;
+    LAUNCH(ks_sphere_depth, n, 128, c, set->positions, n, reinterpret_cast<uint32_t*>(depth));
+    return SNOWB_OK;
+}
+
+int snowb_ssfr_thickness(const snowb_particle_data* set, uint32_t n, const snowb_camera* cam, unsigned long long* thick)
+{
+    SsfrCam c;
+    TRY(ssfr_cam(cam, nullptr, c));
+    if (!set || !thick) return fail(SNOWB_ERR_INVALID, "null pointer");
+    if (n == 0) return SNOWB_OK;
+    LAUNCH(ks_thickness, n, 128, c, set->positions, n, thick);
+    return SNOWB_OK;
+}
+
+int snowb_ssfr_smooth(const snowb_camera* cam, const snowb_ssfr* ssfr, const float* depth, float* tmp, float* out)
+{
+    SsfrCam c;
+    SsfrShade s;
+    TRY(ssfr_cam(cam, ssfr, c));
+    TRY(ssfr_shade(ssfr, s));
+    if (!depth || !tmp || !out || tmp == depth || tmp == out) return fail(SNOWB_ERR_INVALID, "bad buffers");
+    const uint64_t np = (uint64_t)c.W * c.H;
+    LAUNCH(ks_bilateral, np, 256, c, s, depth, tmp, 0);
+    LAUNCH(ks_bilateral, np, 256, c, s, tmp, out, 1);
+    return SNOWB_OK;
+}
+
+int snowb_ssfr_compose(const snowb_camera* cam, const snowb_ssfr* ssfr, const float* depth,
+                       const unsigned long long* thick, const float* scene_rgba, const float* scene_depth, float* rgba)
+{
+    SsfrCam c;
+    SsfrShade s;
+    TRY(ssfr_cam(cam, ssfr, c));
+    TRY(ssfr_shade(ssfr, s));
+    if (!depth || !thick || !scene_rgba || !scene_depth || !rgba) return fail(SNOWB_ERR_INVALID, "null pointer");
+    LAUNCH(ks_compose, (uint64_t)c.W * c.H, 256, c, s, depth, thick, scene_rgba, scene_depth, rgba);
+    return SNOWB_OK;
+}
+
+int snowb_ssfr_workspace_bytes(const snowb_camera* cam, uint64_t* bytes)
+{
+    RenderCam c;
+    TRY(render_cam(cam, c));
+    if (!bytes) return fail(SNOWB_ERR_INVALID, "null output");
+    *bytes = (uint64_t)c.W * c.H * 48u;
+    return SNOWB_OK;
+}
+
+int snowb_render_fluid(const snowb_particle_data* sph, uint32_t n_sph, const snowb_particle_data* dem, uint32_t n_dem,
+                       const snowb_camera* cam, const snowb_point_colour* snow_colour, const snowb_ssfr* ssfr,
+                       void* workspace, float* rgba)
+{
+    if (!sph || !dem || !snow_colour || !ssfr || !workspace || !rgba) return fail(SNOWB_ERR_INVALID, "null pointer");
+    if ((reinterpret_cast<uintptr_t>(workspace) & 15u) != 0) return fail(SNOWB_ERR_INVALID, "workspace not 16-byte aligned");
+    RenderCam rc;
+    TRY(render_cam(cam, rc));
+    const uint64_t np = (uint64_t)rc.W * rc.H;
+    char* w = static_cast<char*>(workspace);
+    unsigned long long* zbuf = reinterpret_cast<unsigned long long*>(w);
+    unsigned long long* thick = zbuf + np;
+    float* scene = reinterpret_cast<float*>(thick + np);
+    float* scene_depth = scene + 4 * np;
+    float* fdepth = scene_depth + np;
+    float* tmp = fdepth + np;
+    float* smooth = tmp + np;
+    // scene: the snow as point sprites over the clear colour, and its sphere depth
+    TRY(snowb_render_clear_colour(cam, ssfr->clear_color, scene, zbuf));
+    TRY(snowb_render_points(dem, n_dem, cam, snow_colour, 0, scene, zbuf));
+    TRY(snowb_ssfr_clear(cam, scene_depth, thick));
+    TRY(snowb_ssfr_clear(cam, fdepth, nullptr));
+    TRY(snowb_ssfr_sphere_depth(dem, n_dem, cam, ssfr, scene_depth));
+    // water: sphere depth, smoothed, thickness, composite
+    TRY(snowb_ssfr_sphere_depth(sph, n_sph, cam, ssfr, fdepth));
+    TRY(snowb_ssfr_smooth(cam, ssfr, fdepth, tmp, smooth));
+    TRY(snowb_ssfr_thickness(sph, n_sph, cam, thick));
+    TRY(snowb_ssfr_compose(cam, ssfr, smooth, thick, scene, scene_depth, rgba));
     return SNOWB_OK;
 }
 

@@ -85,6 +85,62 @@ def colour(rgb, temperature=None):
     return pc
 
 
+class SsfrParams(C.Structure):
+    _fields_ = [("sphere_radius", C.c_float), ("filter_radius", C.c_float), ("blur_scale", C.c_float),
+                ("blur_depth_falloff", C.c_float), ("light_color", C.c_float * 4), ("clear_color", C.c_float * 4)]
+
+
+def ssfr_params(sphere_radius=0.01, filter_radius=10.0, blur_scale=0.1, blur_depth_falloff=65.0,
+                light_color=(1.0, 1.0, 1.0, 0.8), clear_color=(0.15, 0.15, 0.15, 0.0)):
+    """The reference Renderer's values (Renderer.cpp:10, :485-690; bilateral_fs.glsl)."""
+    p = SsfrParams()
+    p.sphere_radius, p.filter_radius, p.blur_scale = sphere_radius, filter_radius, blur_scale
+    p.blur_depth_falloff = blur_depth_falloff
+    p.light_color[:] = light_color
+    p.clear_color[:] = clear_color
+    return p
+
+
+def reference_camera(width=1600, height=900):
+    """The reference application's view: CameraDesc of GLFWApp.cpp:176-185 (eye (0, 0, 5)
+    looking at the origin, fov 45 handed to glm::perspective as radians, near 0.001, far
+    1000), a 1600 x 900 viewport, point size 30 (Renderer.cpp:8-11) and the light at the
+    camera (Renderer.cpp:308-309)."""
+    c = Camera()
+    eye = (0.0, 0.0, 5.0)
+    c.view[:] = look_at(eye, (0.0, 0.0, 0.0), (0.0, 1.0, 0.0))
+    c.projection[:] = perspective(45.0, f32(width) / f32(height), 0.001, 1000.0)
+    c.camera_pos[:] = eye
+    c.light_pos[:] = eye
+    c.point_size = 30.0
+    c.width, c.height = width, height
+    return c
+
+
+def ssfr_matrices(lib, cam):
+    """The library's camera matrices: dict of PV, V, P, Pinv, Vinv (16 floats each)."""
+    out = (C.c_float * 80)()
+    _native.check(lib.snowb_ssfr_matrices(C.addressof(cam), C.addressof(out)))
+    a = np.frombuffer(out, np.float32).copy()
+    return {k: a[16 * i:16 * i + 16] for i, k in enumerate(("PV", "V", "P", "Pinv", "Vinv"))}
+
+
+def render_fluid(sim, cam, ssfr=None, snow_colour=None):
+    """The reference's default view of `sim` (snow as point sprites, water as a smoothed,
+    refracting surface) into a new device image (H x W x 4 float32)."""
+    lib = sim.lib
+    ss = ssfr if ssfr is not None else ssfr_params(sphere_radius=float(sim.w.params.particle_radius))
+    pc = snow_colour if snow_colour is not None else colour(SNOW_RGB)
+    nbytes = C.c_uint64(0)
+    _native.check(lib.snowb_ssfr_workspace_bytes(C.addressof(cam), C.byref(nbytes)))
+    ws = torch.empty(int(nbytes.value) // 4, dtype=torch.float32, device=sim.device)
+    img = torch.empty((cam.height, cam.width, 4), dtype=torch.float32, device=sim.device)
+    _native.check(lib.snowb_render_fluid(C.byref(sim._s[0]), sim.n_sph, C.byref(sim._s[1]), sim.n_dem,
+                                         C.addressof(cam), C.addressof(pc), C.addressof(ss), ws.data_ptr(),
+                                         img.data_ptr()))
+    return img
+
+
 def render(sim, cam, temperature=None):
     """Water then snow of `sim` into a new device image (H x W x 4 float32)."""
     lib = sim.lib
