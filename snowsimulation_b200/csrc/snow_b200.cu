@@ -145,6 +145,8 @@ struct Ctx {
     DevState* S = nullptr;
     DevState* S_host = nullptr;
     uint32_t* err_dev = nullptr;
+    cudaStream_t side = nullptr;          // second stream for the water sort (see sort_pair)
+    cudaEvent_t fork = nullptr, join = nullptr;
 };
 static Ctx g_ctx;
 static uint64_t g_ctx_gen = 0;   // bumped whenever the scratch buffers are (re)allocated
@@ -167,6 +169,9 @@ static void free_ctx(Ctx& c)
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c.S_host) cudaFreeHost(c.S_host);
+    if (c.side) cudaStreamDestroy(c.side);
+    if (c.fork) cudaEventDestroy(c.fork);
+    if (c.join) cudaEventDestroy(c.join);
     c = Ctx();
 }
 static int alloc_sort(SetBufs& s, uint32_t cap, uint32_t ncells, bool attrs)
@@ -211,6 +216,9 @@ static int ensure_ctx(uint32_t full, uint32_t nb, uint32_t ncells)
     CUDA_TRY(cudaMemset(c.S, 0, sizeof(DevState)));
     CUDA_TRY(cudaMemset(c.err_dev, 0, sizeof(uint32_t)));
     CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&c.S_host), sizeof(DevState)));
+    CUDA_TRY(cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking));
+    CUDA_TRY(cudaEventCreateWithFlags(&c.fork, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventCreateWithFlags(&c.join, cudaEventDisableTiming));
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     g_max_blocks = sms * 16;
@@ -552,12 +560,27 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
         if (!cond) dirty = false;
         return SNOWB_OK;
     };
+    // The two sets' sorts share no buffer: the water sort runs on a side stream beside the
+    // snow sort (a fork and a join of the captured graph), so the small set's chain of
+    // latency-bound launches overlaps the large one's.
+    auto sort_pair = [&](const uint32_t* cond) -> int {
+        const cudaStream_t main_stream = g_stream;
+        CUDA_TRY(cudaEventRecord(c.fork, main_stream));
+        CUDA_TRY(cudaStreamWaitEvent(c.side, c.fork, 0));
+        g_stream = c.side;
+        const int rc = sort_if(0, cond);
+        g_stream = main_stream;
+        TRY(rc);
+        TRY(sort_if(1, cond));
+        CUDA_TRY(cudaEventRecord(c.join, c.side));
+        CUDA_TRY(cudaStreamWaitEvent(main_stream, c.join, 0));
+        return SNOWB_OK;
+    };
 #define STOP(k) do { if (a.stop_after == (k)) return SNOWB_OK; } while (0)
 
     TAPE_HOOK(0, 0);
     LAUNCH1(k_begin_substep, S);
-    TRY(sort_if(1, nullptr));
-    TRY(sort_if(0, nullptr));
+    TRY(sort_pair(nullptr));
     STOP(1);
     TLAUNCH(k_density<false>, 256, work3, 128, P, S, vs, vd, vb, X, ss, sd, sb, NL);
     STOP(2);
@@ -589,8 +612,7 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
     }
     STOP(4);
     if (a.change_phase) {   // the reference sorts again; only a phase change alters the result
-        TRY(sort_if(1, &S->changed));
-        TRY(sort_if(0, &S->changed));
+        TRY(sort_pair(&S->changed));
     }
     STOP(5);
     if (a.interlink) {
@@ -616,8 +638,7 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
     STOP(7);
     for (int it = 0; it < a.iterations; ++it) {
         const int base = 10 + 10 * it;
-        TRY(sort_if(1, nullptr));
-        TRY(sort_if(0, nullptr));
+        TRY(sort_pair(nullptr));
         TAPE_HOOK(2, it);
         STOP(base + 0);
         // density + lambda in one pass (stage boundaries base+1 and base+2 coincide)
@@ -638,8 +659,7 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
         TAPE_HOOK(3, it);
         STOP(base + 6);
         if (a.friction && step_dem) {
-            TRY(sort_if(1, nullptr));
-            TRY(sort_if(0, nullptr));
+            TRY(sort_pair(nullptr));
             TLAUNCH(k_friction, 256, full, 128, P, S, vd, vb, X, sd, sb);
             TLAUNCH(k_apply, 1024, full, 256, P, S, vs, vd, X, 0, 1);
             dirty_d = true;
