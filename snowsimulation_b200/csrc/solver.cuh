@@ -614,9 +614,19 @@ __device__ __forceinline__ float3 friction_term(const DevParams& P, float3 dx, f
     }
     return sc3(-(w0 / ws), dxt);
 }
+// Two phases per set: the candidate scan records the contacts (d <= 2r, a few per
+// particle) with their cell in shared memory, then the friction terms are evaluated over
+// the record with the per-cell partial sums closed where the cell changes (cells without
+// contacts add +0 in the traversal, which leaves the sum unchanged).  The lanes of a warp
+// then evaluate the costly term together instead of once per lane that found a contact.
+// More than FR_K contacts fall back to the single traversal.
+constexpr uint32_t FR_K = 16;
 __global__ void __launch_bounds__(256) k_friction(DevParams P, const DevState* __restrict__ S, SetView vd, SetView vb,
                                                   Sets X, Sorted sd, Sorted sb)
 {
+    __shared__ uint32_t rec_sh[FR_K * 256];
+    uint32_t* const rec = rec_sh + threadIdx.x;     // entry k at rec[k * blockDim.x]
+    const uint32_t bd = blockDim.x;
     vd.n = S->n_dem; vb.n = S->n_b;
     const uint32_t ld = launch_limit(P, S->n0_dem, S->n_dem);
     GRID_LOOP(i, ld) {
@@ -627,35 +637,92 @@ __global__ void __launch_bounds__(256) k_friction(DevParams P, const DevState* _
         GCell g = grid_pos(P, p, vd.scene(i));
         const Nbhd nb = make_nbhd(P, g, p, P.r2_cull);
         float3 c = f3(0.f, 0.f, 0.f);
+        // snow-snow contacts
+        uint32_t n = 0;
         FOR27 {
-            float3 cs = f3(0.f, 0.f, 0.f);
             uint32_t s, e;
             if (vd.range_nb(nb, ox, oy, oz, s, e))
                 for (uint32_t j = s; j < e; ++j) {
                     if (j == i) continue;
-                    float3 pp1 = vd.pos(j);
-                    float3 v = sub3(p, pp1);
-                    float d2 = dot3(v, v);
-                    if (d2 < P.r2_le) {
-                        const uint32_t oj = vd.gi[j];
-                        float3 op1 = ldv3(X.dem.positions, oj);
-                        float3 dx = add3(sub3(p, op0), sub3(pp1, op1));
-                        cs = add3(cs, friction_term(P, dx, w0, vd.attr(sd.invm, X.dem.massInv, j), sqrtf(d2), v));
+                    const float3 v = sub3(p, vd.pos(j));
+                    if (dot3(v, v) < P.r2_le) {
+                        if (n < FR_K) rec[n * bd] = j | ((uint32_t)CELL27 << 25);
+                        ++n;
                     }
                 }
-            c = add3(c, cs);
         }
-        FOR27 {
+        if (n <= FR_K) {
             float3 cs = f3(0.f, 0.f, 0.f);
+            uint32_t cur = 0xFFu;
+            for (uint32_t k = 0; k < n; ++k) {
+                const uint32_t en = rec[k * bd], j = en & NL_J_MASK, cell = en >> 25;
+                if (cell != cur) { if (cur != 0xFFu) c = add3(c, cs); cs = f3(0.f, 0.f, 0.f); cur = cell; }
+                const float3 pp1 = vd.pos(j);
+                const float3 v = sub3(p, pp1);
+                const float d2 = dot3(v, v);
+                const float3 op1 = ldv3(X.dem.positions, vd.gi[j]);
+                const float3 dx = add3(sub3(p, op0), sub3(pp1, op1));
+                cs = add3(cs, friction_term(P, dx, w0, vd.attr(sd.invm, X.dem.massInv, j), sqrtf(d2), v));
+            }
+            if (cur != 0xFFu) c = add3(c, cs);
+        } else {
+            FOR27 {
+                float3 cs = f3(0.f, 0.f, 0.f);
+                uint32_t s, e;
+                if (vd.range_nb(nb, ox, oy, oz, s, e))
+                    for (uint32_t j = s; j < e; ++j) {
+                        if (j == i) continue;
+                        float3 pp1 = vd.pos(j);
+                        float3 v = sub3(p, pp1);
+                        float d2 = dot3(v, v);
+                        if (d2 < P.r2_le) {
+                            const uint32_t oj = vd.gi[j];
+                            float3 op1 = ldv3(X.dem.positions, oj);
+                            float3 dx = add3(sub3(p, op0), sub3(pp1, op1));
+                            cs = add3(cs, friction_term(P, dx, w0, vd.attr(sd.invm, X.dem.massInv, j), sqrtf(d2), v));
+                        }
+                    }
+                c = add3(c, cs);
+            }
+        }
+        // snow-boundary contacts
+        n = 0;
+        FOR27 {
             uint32_t s, e;
             if (vb.range_nb(nb, ox, oy, oz, s, e))
                 for (uint32_t j = s; j < e; ++j) {
-                    float3 v = sub3(p, vb.pos(j));
-                    float d2 = dot3(v, v);
-                    if (d2 < P.r2_le)
-                        cs = add3(cs, friction_term(P, sub3(p, op0), w0, vb.attr(sb.invm, X.bnd.massInv, j), sqrtf(d2), v));
+                    const float3 v = sub3(p, vb.pos(j));
+                    if (dot3(v, v) < P.r2_le) {
+                        if (n < FR_K) rec[n * bd] = j | ((uint32_t)CELL27 << 25);
+                        ++n;
+                    }
                 }
-            c = add3(c, cs);
+        }
+        const float3 dx0 = sub3(p, op0);
+        if (n <= FR_K) {
+            float3 cs = f3(0.f, 0.f, 0.f);
+            uint32_t cur = 0xFFu;
+            for (uint32_t k = 0; k < n; ++k) {
+                const uint32_t en = rec[k * bd], j = en & NL_J_MASK, cell = en >> 25;
+                if (cell != cur) { if (cur != 0xFFu) c = add3(c, cs); cs = f3(0.f, 0.f, 0.f); cur = cell; }
+                const float3 v = sub3(p, vb.pos(j));
+                const float d2 = dot3(v, v);
+                cs = add3(cs, friction_term(P, dx0, w0, vb.attr(sb.invm, X.bnd.massInv, j), sqrtf(d2), v));
+            }
+            if (cur != 0xFFu) c = add3(c, cs);
+        } else {
+            FOR27 {
+                float3 cs = f3(0.f, 0.f, 0.f);
+                uint32_t s, e;
+                if (vb.range_nb(nb, ox, oy, oz, s, e))
+                    for (uint32_t j = s; j < e; ++j) {
+                        float3 v = sub3(p, vb.pos(j));
+                        float d2 = dot3(v, v);
+                        if (d2 < P.r2_le)
+                            cs = add3(cs, friction_term(P, dx0, w0, vb.attr(sb.invm, X.bnd.massInv, j), sqrtf(d2), v));
+                    }
+                c = add3(c, cs);
+            }
         }
         if (nan3(c)) c = f3(0.f, 0.f, 0.f);
         st3(X.dem.correction, o, c);
