@@ -29,7 +29,10 @@ struct Sorted {
 // (their supports are d < h or smaller) instead of re-testing ~300 candidates over 81
 // cells, keeping the per-cell partial sums.  A particle with more than NLIST_K entries is
 // marked overflowed and its consumers traverse the cells as before.
-constexpr uint32_t NLIST_K = 192;
+#ifndef SNOWB_NLIST_K
+#define SNOWB_NLIST_K 384
+#endif
+constexpr uint32_t NLIST_K = SNOWB_NLIST_K;
 constexpr uint32_t NL_J_MASK = (1u << 25) - 1u;
 constexpr uint32_t NL_OVF = 1u << 31;
 struct NList {
