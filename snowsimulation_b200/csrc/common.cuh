@@ -64,6 +64,56 @@ __device__ __forceinline__ float3 sub3(float3 a, float3 b) { return f3(a.x - b.x
 __device__ __forceinline__ float3 sc3(float s, float3 a) { return f3(s * a.x, s * a.y, s * a.z); }
 __device__ __forceinline__ float3 div3(float3 a, float s) { return f3(a.x / s, a.y / s, a.z / s); }
 __device__ __forceinline__ float dot3(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+// Packed two-lane FP32 arithmetic of sm_100 (add/sub/mul.rn.f32x2).  Each instruction alone
+// rounds each lane as the scalar operation does, but ptxas contracts a packed multiply
+// feeding a packed add into a fused multiply-add even with .rn and -fmad=false (measured:
+// about 21% of d2_pair results differ from the separately rounded ones in the last bits),
+// so packed results serve only as screens with a margin, never as values.
+__device__ __forceinline__ uint64_t pk2(float a, float b)
+{
+    uint64_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ float2 upk2(uint64_t v)
+{
+    float a, b;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+    return make_float2(a, b);
+}
+__device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b)
+{
+    uint64_t d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ uint64_t sub2(uint64_t a, uint64_t b)
+{
+    uint64_t d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ uint64_t mul2(uint64_t a, uint64_t b)
+{
+    uint64_t d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+// p broadcast to both lanes, per coordinate
+struct P2 {
+    uint64_t x, y, z;
+};
+__device__ __forceinline__ P2 bcast2(float3 p) { return P2{pk2(p.x, p.x), pk2(p.y, p.y), pk2(p.z, p.z)}; }
+// dot3(sub3(p, q0), sub3(p, q0)) and the same for q1, two candidates per instruction, to
+// within a few ulps (see above)
+__device__ __forceinline__ float2 d2_pair(const P2& p, float4 q0, float4 q1)
+{
+    const uint64_t dx = sub2(p.x, pk2(q0.x, q1.x));
+    const uint64_t dy = sub2(p.y, pk2(q0.y, q1.y));
+    const uint64_t dz = sub2(p.z, pk2(q0.z, q1.z));
+    return upk2(add2(add2(mul2(dx, dx), mul2(dy, dy)), mul2(dz, dz)));
+}
 __device__ __forceinline__ float len3(float3 a) { return sqrtf(dot3(a, a)); }
 __device__ __forceinline__ bool nan3(float3 a) { return isnan(a.x) || isnan(a.y) || isnan(a.z); }
 __device__ __forceinline__ bool inf3(float3 a) { return isinf(a.x) || isinf(a.y) || isinf(a.z); }

@@ -301,15 +301,31 @@ __device__ __forceinline__ void acc_WG(const DevParams& P, float& rho, float& gs
                                        const Nbhd& nb, uint32_t skip, bool vol, int mode, float m_self,
                                        const float* mass_s, const float* mass_o, NLWriter* wr = nullptr, int set = 0)
 {
+    const P2 pp = bcast2(p);
     FOR27 {
         float cs = 0.f, cg = 0.f;
         uint32_t s, e;
         if (v.range_nb(nb, ox, oy, oz, s, e)) {
             const int cell = CELL27;
             if (e <= v.n) {
-                // current entries only: the compact sorted copies
-                for (uint32_t j = s; j < e; ++j) {
-                    if (j == skip) continue;
+                // current entries only: the compact sorted copies.  Candidates are screened
+                // two at a time with packed arithmetic; ptxas may contract its multiply-adds,
+                // so the screen is a superset test against the slightly larger h2_cull, and
+                // every candidate that passes goes through the exact scalar test and terms.
+                uint32_t j = s;
+                for (; j + 1 < e; j += 2) {
+                    const float4 q0 = __ldg(v.p4 + j), q1 = __ldg(v.p4 + j + 1);
+                    const float2 dd = d2_pair(pp, q0, q1);
+                    if (dd.x < P.h2_cull && j != skip) {
+                        const float mj = (LAMBDA && mode == 2) ? __ldg(mass_s + j) : 0.f;
+                        wg_term<LAMBDA>(P, cs, cg, q0, p, j, vol, mode, m_self, mj, wr, cell, set);
+                    }
+                    if (dd.y < P.h2_cull && j + 1 != skip) {
+                        const float mj = (LAMBDA && mode == 2) ? __ldg(mass_s + j + 1) : 0.f;
+                        wg_term<LAMBDA>(P, cs, cg, q1, p, j + 1, vol, mode, m_self, mj, wr, cell, set);
+                    }
+                }
+                if (j < e && j != skip) {
                     const float mj = (LAMBDA && mode == 2) ? __ldg(mass_s + j) : 0.f;
                     wg_term<LAMBDA>(P, cs, cg, __ldg(v.p4 + j), p, j, vol, mode, m_self, mj, wr, cell, set);
                 }
