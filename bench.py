@@ -93,6 +93,13 @@ class Clocks:
                                        "-lms", "50", "-i", str(dev)], stdout=self.f, stderr=subprocess.DEVNULL)
         except OSError:
             self.p = None
+        # nvidia-smi takes a moment to start: wait (at most 2 s) for its first row, so that
+        # the timed region that follows is sampled from its start
+        t0 = time.perf_counter()
+        while self.p is not None and time.perf_counter() - t0 < 2.0:
+            if os.path.getsize(self.f.name) > 0 or self.p.poll() is not None:
+                break
+            time.sleep(0.01)
 
     def stop(self):
         if self.p is None:
