@@ -235,14 +235,16 @@ __global__ void __launch_bounds__(256) k_link_filter(DevParams P, DevState* S, S
         const float3 p = vd.pos(i);
         const uint32_t count = dem.iter_end[o] - o * M;
         uint8_t act = 0;
+        // a particle at its cap stays inactive: its slots are not even read
+        const bool below = count < link_tolerance(P, dem.T[o], dynamic);
         // own slots in registers (M <= SNOWB_MAXC_FAST), else read from memory
         uint32_t r[SNOWB_MAXC_FAST];
         const bool fast = M <= SNOWB_MAXC_FAST;
 #pragma unroll
-        for (int k = 0; k < SNOWB_MAXC_FAST; ++k) r[k] = fast && (uint32_t)k < M ? dem.connect_record[M * o + k] : 0u;
+        for (int k = 0; k < SNOWB_MAXC_FAST; ++k)
+            r[k] = below && fast && (uint32_t)k < M ? dem.connect_record[M * o + k] : 0u;
         const uint32_t lc = lists ? L.cnt[L.cap + i] : NL_OVF;
-        if (!(lc & NL_OVF) && count < link_tolerance(P, dem.T[o], dynamic) &&
-            has_free_slot(dem.connect_record, o, M)) {
+        if (!(lc & NL_OVF) && below && has_free_slot(dem.connect_record, o, M)) {
             // the same scan over the listed candidates (cells in order, d < h, j != i)
             uint32_t skip_cell = 0xFFu;
             const uint32_t nl = lc & 1023u;
@@ -263,8 +265,7 @@ __global__ void __launch_bounds__(256) k_link_filter(DevParams P, DevState* S, S
                 if (found) { skip_cell = cell; continue; }
                 if (dem.iter_end[o1] < (o1 + 1) * M && has_free_slot(dem.connect_record, o1, M)) act = 1;
             }
-        } else if ((lc & NL_OVF) && count < link_tolerance(P, dem.T[o], dynamic) &&
-                   has_free_slot(dem.connect_record, o, M)) {
+        } else if ((lc & NL_OVF) && below && has_free_slot(dem.connect_record, o, M)) {
             const GCell g = grid_pos(P, p, vd.scene(i));
             FOR27 {
                 uint32_t s, e;
@@ -472,7 +473,7 @@ __device__ void link_particle_list(const DevParams& P, const SetView& vd, const 
     uint32_t skip_cell = 0xFFu;
     for (uint32_t k0 = 0; k0 < n_list; k0 += 32u) {
         const uint32_t k = k0 + lane;
-        uint32_t j = 0, cell = 0xFEu;
+        uint32_t j = 0, cell = 0xFEu, og = 0;
         float d2 = 0.f;
         if (k < n_list) {
             const uint32_t en = L.e[(size_t)k * L.stride + slot];
@@ -480,17 +481,19 @@ __device__ void link_particle_list(const DevParams& P, const SetView& vd, const 
             cell = (en >> 25) & 31u;
             const float3 dv = sub3(p, vd.pos(j));
             d2 = dot3(dv, dv);
+            // the partner's index, fetched side by side for the 32 candidates (it never
+            // changes in this pass), so the walk below needs no load for a duplicate
+            og = vd.gi[j];
         }
         uint32_t mask = __ballot_sync(0xffffffffu, k < n_list);
         while (mask) {
             const int kk = __ffs(mask) - 1;
             mask &= mask - 1u;
             const uint32_t ck = __shfl_sync(0xffffffffu, cell, kk);
-            const uint32_t jj = __shfl_sync(0xffffffffu, j, kk);
             const float dk2 = __shfl_sync(0xffffffffu, d2, kk);
             if (ck == skip_cell) continue;
             if (!(count < tol)) continue;
-            const uint32_t o1 = vd.gi[jj];
+            const uint32_t o1 = __shfl_sync(0xffffffffu, og, kk);
             const float dist = sqrtf(dk2);
             const bool dup = __any_sync(0xffffffffu, lane < M && rk == o1);
             if (dup) { skip_cell = ck; continue; }   // the reference returns from the cell helper
