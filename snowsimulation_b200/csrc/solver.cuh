@@ -889,57 +889,13 @@ __global__ void k_heat_commit(const DevState* __restrict__ S, Sets X, float dTe,
 }
 
 // ======================================================================== XSPH
-// xsph_viscosity_cell{,_coupling} (:3419-3502): sum of (m_j/rho_j) (v_j - v_i) W
-__device__ __forceinline__ float3 acc_xsph(const DevParams& P, float3 acc, const SetView& v,
-                                           const snowb_particle_data& O, const snowb_float3* vel, float3 p,
-                                           GCell g, uint32_t skip, float3 vi)
-{
-    FOR27 {
-        float3 cs = f3(0.f, 0.f, 0.f);
-        uint32_t s, e;
-        if (v.range(P, g, ox, oy, oz, s, e))
-            for (uint32_t j = s; j < e; ++j) {
-                if (j == skip) continue;
-                float3 dv = sub3(p, v.pos(j));
-                float d2 = dot3(dv, dv);
-                if (d2 < P.h2_lt) {
-                    const uint32_t oj = v.gi[j];
-                    float3 vij = sub3(ldv3(vel, oj), vi);
-                    float a = O.mass[oj] / O.density[oj];
-                    float wgt = W_poly6(P, sqrtf(d2));
-                    cs = add3(cs, f3((a * vij.x) * wgt, (a * vij.y) * wgt, (a * vij.z) * wgt));
-                }
-            }
-        acc = add3(acc, cs);
-    }
-    return acc;
-}
-// xsph_sph_viscosity / xsph_dem_viscosity (:3504-3660), Jacobi: results go to out_vel.
-// `limit` is the number of sorted particles processed (Q6 for the snow set).
-__global__ void __launch_bounds__(128) k_xsph(DevParams P, const DevState* __restrict__ S, SetView vown, SetView voth,
-                                              snowb_particle_data A, snowb_particle_data B, int own_is_sph,
-                                              float visc, snowb_float3* __restrict__ out_vel)
-{
-    const uint32_t ns = S->n_sph, nd = S->n_dem;
-    vown.n = own_is_sph ? ns : nd;
-    voth.n = own_is_sph ? nd : ns;
-    const uint32_t limit = own_is_sph ? ns
-                         : (P.quirks == SNOWB_QUIRKS_REFERENCE ? umin32(coverage(ns), nd) : nd);
-    GRID_LOOP(i, limit) {
-        const uint32_t o = vown.gi[i];
-        float3 p = xyz(vown.p4[i]); GCell g = grid_pos(P, p, vown.scene(i));
-        float3 vi = ldv3(A.velocity, o);
-        float3 c = f3(0.f, 0.f, 0.f);
-        c = acc_xsph(P, c, vown, A, A.velocity, p, g, i, vi);
-        c = acc_xsph(P, c, voth, B, B.velocity, p, g, SNOWB_UMAX, vi);
-        c = sc3(visc, c);
-        st3(out_vel, o, add3(vi, c));
-    }
-}
-// Warp-per-particle variant: lane k < 27 computes the partial sum of cell k (the
-// reference's per-cell helper), then the partials are added to the running total in cell
-// order with shuffles -- the same operations in the same order as one thread would do,
-// with 27-way parallelism for the small sets XSPH works on.
+// xsph_viscosity_cell{,_coupling} (:3419-3502): sum of (m_j/rho_j) (v_j - v_i) W, and
+// xsph_sph_viscosity / xsph_dem_viscosity (:3504-3660), Jacobi: results go to out_vel
+// (`limit`, the number of sorted particles processed, carries Q6 for the snow set).
+// One warp per particle: lane k < 27 computes the partial sum of cell k (the reference's
+// per-cell helper), then the partials are added to the running total in cell order with
+// shuffles -- the same operations in the same order as one thread would do, with 27-way
+// parallelism for the small sets XSPH works on.
 __device__ __forceinline__ float3 warp_ordered_sum(float3 acc, float3 part)
 {
 #pragma unroll 1
