@@ -299,7 +299,8 @@ __device__ __forceinline__ void wg_term(const DevParams& P, float& cs, float& cg
 template <bool LAMBDA>
 __device__ __forceinline__ void acc_WG(const DevParams& P, float& rho, float& gs, const SetView& v, float3 p,
                                        const Nbhd& nb, uint32_t skip, bool vol, int mode, float m_self,
-                                       const float* mass_s, const float* mass_o, NLWriter* wr = nullptr, int set = 0)
+                                       const float* mass_s, const float* mass_o, NLWriter* wr = nullptr, int set = 0,
+                                       float* dpart = nullptr, uint32_t* dmask = nullptr)
 {
     const P2 pp = bcast2(p);
     FOR27 {
@@ -337,7 +338,13 @@ __device__ __forceinline__ void acc_WG(const DevParams& P, float& rho, float& gs
                 }
             }
         }
-        rho += cs;
+        // dpart: keep the cell's density partial aside instead of adding it now (a partial
+        // of +0, which adds nothing, is not kept)
+        if (dpart) {
+            if (cs != 0.f) { dpart[CELL27] = cs; *dmask |= 1u << CELL27; }
+        } else {
+            rho += cs;
+        }
         if (LAMBDA) gs += cg;
     }
 }
@@ -382,19 +389,30 @@ __global__ void __launch_bounds__(256) k_density(DevParams P, DevState* __restri
                 L.cnt[wr.slot] = n_own > NLIST_K ? NL_OVF : n_own;
             }
         } else {
-            // boundary: density visits (b, snow, water), lambda (b, water, snow)
+            // boundary: density sums the sets in the order (b, snow, water), lambda (b, water, snow)
             i = t - ns - nd; o = vb.gi[i];
             float3 p = xyz(vb.p4[i]); GCell g = grid_pos(P, p, vb.scene(i));
             const Nbhd nb = make_nbhd(P, g, p, P.h2_cull);
             rho = (P.rho0 * X.bnd.volume[o]) * P.W0;
             acc_WG<LAMBDA>(P, rho, gs, vb, p, nb, i, true, 2, 0.f, sb.mass, X.bnd.mass);
-            float unused = 0.f;
-            acc_WG<false>(P, rho, unused, vd, p, nb, SNOWB_UMAX, false, 0, 0.f, nullptr, nullptr);
-            acc_WG<false>(P, rho, unused, vs, p, nb, SNOWB_UMAX, false, 0, 0.f, nullptr, nullptr);
             if (LAMBDA) {
-                float r2 = 0.f;
-                acc_WG<true>(P, r2, gs, vs, p, nb, SNOWB_UMAX, false, 0, 0.f, nullptr, nullptr);
-                acc_WG<true>(P, r2, gs, vd, p, nb, SNOWB_UMAX, false, 0, 0.f, nullptr, nullptr);
+                // one traversal per set for both sums: water first (its lambda terms come
+                // before the snow's), its density partials kept aside and added after the
+                // snow's, cell by cell in order -- the two orders of the separate passes
+                float wpart[27];
+                uint32_t wmask = 0;
+                acc_WG<true>(P, rho, gs, vs, p, nb, SNOWB_UMAX, false, 0, 0.f, nullptr, nullptr, nullptr, 0, wpart,
+                             &wmask);
+                acc_WG<true>(P, rho, gs, vd, p, nb, SNOWB_UMAX, false, 0, 0.f, nullptr, nullptr);
+                while (wmask) {
+                    const int c = __ffs(wmask) - 1;
+                    wmask &= wmask - 1u;
+                    rho += wpart[c];
+                }
+            } else {
+                float unused = 0.f;
+                acc_WG<false>(P, rho, unused, vd, p, nb, SNOWB_UMAX, false, 0, 0.f, nullptr, nullptr);
+                acc_WG<false>(P, rho, unused, vs, p, nb, SNOWB_UMAX, false, 0, 0.f, nullptr, nullptr);
             }
             D = &X.bnd; lam_s = sb.lambda;
         }
