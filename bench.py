@@ -554,14 +554,30 @@ def main():
     if base(top) == "k_density" and "true" in top:     # density + lambda in one pass
         kb += bytes_model.PASS["L"] * (sim.n_sph + sim.n_dem + sim.n_b)
     traffic = None
+    winst = None
     tfile = os.path.join(ROOT, "profiles", "dram_traffic_config1.txt")
-    if os.path.exists(tfile):   # per-launch DRAM bytes of the kernel from an ncu capture
+    if os.path.exists(tfile):   # per-launch DRAM bytes (and warp instructions) from an ncu capture
         for line in open(tfile):
             parts = line.split()
             if len(parts) >= 2 and parts[0] == top:
                 traffic = float(parts[1])
+                if len(parts) >= 3:
+                    winst = float(parts[2])
     peak, peak_kind = peaks()
     achieved = kb / per_launch_s / 1e9
+    # The dominant kernel issues instructions (IEEE divisions and square roots of the
+    # bit-exact arithmetic) far more than it moves bytes: its warp instructions per launch
+    # (ncu) over the live launch time, against the issue peak of 4 schedulers per SM at the
+    # sampled SM clock.
+    issue = None
+    if winst:
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        mhz = clk.get("sm_mhz") or clk.get("sm_max_mhz") or 1965.0
+        peak_issue = sms * 4 * mhz * 1e6 / 1e9
+        issue = {"kernel": top, "warp_instructions_per_launch": winst, "source": "ncu (profiles/)",
+                 "achieved": winst / per_launch_s / 1e9, "peak": peak_issue, "unit": "G warp-instructions/s",
+                 "frac": winst / per_launch_s / 1e9 / peak_issue,
+                 "peak_basis": "%d SMs x 4 schedulers x %.0f MHz (sampled)" % (sms, mhz)}
     sub_bytes = bytes_model.substep_bytes(sim.n_sph, sim.n_dem, sim.n_b, w.iterations)
     sub_gbs = sub_bytes * SUBSTEPS / (ms_per_step / 1000.0) / 1e9
 
@@ -613,6 +629,7 @@ def main():
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "algorithmic_bytes_per_launch": kb, "avg_launch_ms": per_launch_s * 1000.0,
                      "launches_per_step": c / c_frames},
+        "issue_roofline": issue,
         "substep_roofline": {"algorithmic_bytes": sub_bytes, "achieved_GBs": sub_gbs,
                              "frac": sub_gbs / peak},
         "kernel_ms_per_step": {nm: t / prof_frames for nm, (c, t) in sorted(prof.items(), key=lambda x: -x[1][1])},
