@@ -7,8 +7,8 @@ particles, seeded synthetic lattice), one step = one frame = 4 substeps of dt = 
 with 3 solver iterations.  `value` is timed on the device with CUDA events around each
 frame (state resident in HBM, L2 flushed between frames); `e2e` goes through the C-ABI
 call with the per-frame host I/O of the reference (positions, velocities and temperatures
-of both sets copied from pinned host memory before the frame and back after it, the
-buffers the reference maps from GL each frame).  Multi-GPU runs are independent replicas
+of the live particles of both sets copied from pinned host memory before the frame and
+back after it, the buffers the reference maps from GL each frame).  Multi-GPU runs are independent replicas
 (one scene per rank, no collective in the step); `value` is the sum over ranks divided by
 the slowest rank's time.
 
@@ -498,23 +498,32 @@ def main():
             for s in ("sph", "dem") for f in fields}
     for (s, f), hb in host.items():
         hb.copy_(getattr(sim, s).t[f])
-    h2d = sum(hb.numel() * hb.element_size() for hb in host.values())
-    d2h = h2d
-    e_ms = []
+    sim.read_sizes()
+
+    def live(s):   # particles of the set (the slots beyond are padding)
+        return sim.n_sph if s == "sph" else sim.n_dem
+
+    e_ms, h2d_tot, d2h_tot = [], 0, 0
     if ws > 1:
         dist.barrier()
     for k in range(args.steps):
         flush.zero_()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
-        for (s, f), hb in host.items():
-            getattr(sim, s).t[f].copy_(hb, non_blocking=True)
+        for (s, f), hb in host.items():   # this step's inputs: the live particles of each set
+            n = live(s)
+            getattr(sim, s).t[f][:n].copy_(hb[:n], non_blocking=True)
+            h2d_tot += hb[:n].numel() * hb.element_size()
         frame(sync=True)                       # the reference contract: sizes back on the host
-        for (s, f), hb in host.items():
-            hb.copy_(getattr(sim, s).t[f], non_blocking=True)
+        for (s, f), hb in host.items():   # its results, for the sizes after the step
+            n = live(s)
+            hb[:n].copy_(getattr(sim, s).t[f][:n], non_blocking=True)
+            d2h_tot += hb[:n].numel() * hb.element_size()
         b.record(stream)
         b.synchronize()
         e_ms.append(a.elapsed_time(b))
+    h2d = h2d_tot // args.steps
+    d2h = d2h_tot // args.steps
     e_tot = sum(e_ms)
     e_tot = slowest([e_tot], ws, dev)[0]
     e2e = job_rate(n_part * SUBSTEPS * args.steps, ws, e_tot)
