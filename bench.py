@@ -260,8 +260,51 @@ def run_reference(args):
                                        "OpenMP %d threads; the reference runs this path only on a GPU"
                                        % (done, cores)},
             "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    gpu = reference_gpu_runner(args.scene, args.warmup, min(args.steps, 20))
+    if gpu is not None:
+        line["gpu_runner"] = gpu
     print(json.dumps(line))
     return 0
+
+
+def reference_gpu_runner(scene_name, warmup, frames):
+    """The reference's own CUDA substep (cuda_simulation.cu compiled unmodified with the
+    project's fast math, oracle/_ref/libsnowref.so) on this GPU over the same scene, for
+    comparison with the other arm: frames of 4 substeps timed with CUDA events on the
+    default stream, which the reference uses (each of its calls synchronises)."""
+    try:
+        import torch
+        from oracle import ref_runner
+    except ImportError:
+        return None
+    if not torch.cuda.is_available():
+        return None
+    if not ref_runner.available("fast"):
+        return {"unavailable": "oracle/_ref/libsnowref.so not built (needs the reference sources)"}
+    from snowsimulation_b200 import scene
+    w = getattr(scene, scene_name)()
+    n = w.n_sph + w.n_dem
+    r = ref_runner.RefWorld(w, "fast").setup()
+    try:
+        for _ in range(max(3, warmup) * SUBSTEPS):
+            r.step()
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(frames):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(SUBSTEPS):
+                r.step()
+            b.record()
+            b.synchronize()
+            ms.append(a.elapsed_time(b))
+    finally:
+        r.close()
+    per = sum(ms) / len(ms)
+    return {"value": n * SUBSTEPS / (per / 1000.0), "unit": UNIT, "ms_per_step": per, "frames": len(ms),
+            "warmup_frames": max(3, warmup),
+            "workload": "%s, 1 step = 1 frame = %d substeps, the same frames as the other arm" % (scene_name, SUBSTEPS),
+            "build": "the reference's cuda_simulation.cu + cuda_tool.cu, unmodified, fast math, sm_100a"}
 
 
 # ----------------------------------------------------------------- batched vs plain
