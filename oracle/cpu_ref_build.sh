@@ -3,8 +3,8 @@
 # ConstraintSolver.cpp, Constraints.cpp and the Particle/Collider files they link against,
 # unmodified, compiled where they lie under /root/reference) with this directory's
 # cpu_ref_harness.cpp into oracle/_ref/libsnowcpuref.so.  Measurement infrastructure: the
-# library times the reference's own CPU code for the reported CPU baselines.  Only this
-# container has /root/reference; the GPU box uses the built library.
+# library times the reference's own CPU code for the reported CPU baselines.  Where the
+# reference sources are absent the script skips, and the library built earlier is used.
 # Shims, as the reference's Visual Studio project has on its include path: the GL scalar
 # typedefs (type names only) for the OpenGL headers, `std::floorf` (NeighborSearch.cpp
 # calls it; libstdc++ only declares ::floorf) and MSVC's __forceinline.

@@ -2,8 +2,8 @@
 # Builds the reference's own CUDA solver (cuda_simulation.cu + cuda_tool.cu, unmodified,
 # compiled where they lie under /root/reference) together with this directory's harness
 # into oracle/_ref/libsnowref.so, for sm_100a.  Test infrastructure: the reference run is
-# the pin of the CPU oracle.  Only this container has /root/reference; the GPU box uses
-# the built library.  The reference project is a Visual Studio build with OpenGL headers
+# the pin of the CPU oracle.  Where the reference sources are absent the script skips,
+# and the library built earlier is used.  The reference project is a Visual Studio build with OpenGL headers
 # on its include path; two type-only stand-ins written here (GL/gl.h with the GL scalar
 # typedefs, and nothing else) let nvcc parse those headers.  The build mirrors the
 # reference's project settings: fast math and relocatable device code.

@@ -2,10 +2,11 @@
 
 oracle/_ref/libsnowref.so is the reference's cuda_simulation.cu compiled unchanged for
 sm_100a with ref_harness.cu, with the project's fast math; libsnowref_ieee.so is the same
-build with IEEE arithmetic and no contraction (built by ref_build.sh where
-/root/reference exists; the built libraries travel to the GPU box).  RefWorld runs a HostWorld through it so tests can
-pin the CPU oracle to the reference's actual results.  Only one RefWorld can exist at a
-time (the reference keeps its parameters in a __constant__ symbol and static counters).
+build with IEEE arithmetic and no contraction (both built by ref_build.sh from the
+reference's sources).  RefWorld runs a HostWorld through it so tests can pin the CPU
+oracle to the reference's actual results, and the reference arm of the benchmark times
+it.  Only one RefWorld can exist at a time (the reference keeps its parameters in a
+__constant__ symbol and static counters).
 """
 import ctypes as C
 import os
