@@ -485,18 +485,25 @@ __device__ void link_particle_list(const DevParams& P, const SetView& vd, const 
             // changes in this pass), so the walk below needs no load for a duplicate
             og = vd.gi[j];
         }
-        uint32_t mask = __ballot_sync(0xffffffffu, k < n_list);
+        // Candidates of a cell are contiguous and in order.  Once a cell is skipped (a
+        // duplicate ends it, as the reference returns from its cell helper), its remaining
+        // candidates leave the mask in one step; once the count reaches the cap, no later
+        // candidate can do anything (counts only grow), so the walk ends.
+        if (!(count < tol)) break;
+        uint32_t mask = __ballot_sync(0xffffffffu, k < n_list && cell != skip_cell);
         while (mask) {
             const int kk = __ffs(mask) - 1;
             mask &= mask - 1u;
             const uint32_t ck = __shfl_sync(0xffffffffu, cell, kk);
-            const float dk2 = __shfl_sync(0xffffffffu, d2, kk);
-            if (ck == skip_cell) continue;
-            if (!(count < tol)) continue;
+            if (!(count < tol)) break;
             const uint32_t o1 = __shfl_sync(0xffffffffu, og, kk);
-            const float dist = sqrtf(dk2);
             const bool dup = __any_sync(0xffffffffu, lane < M && rk == o1);
-            if (dup) { skip_cell = ck; continue; }   // the reference returns from the cell helper
+            if (dup) {
+                skip_cell = ck;
+                mask &= ~__ballot_sync(0xffffffffu, cell == ck);
+                continue;
+            }
+            const float dist = sqrtf(__shfl_sync(0xffffffffu, d2, kk));
             const uint32_t freem = __ballot_sync(0xffffffffu, lane < M && rk == SNOWB_UMAX);
             if (!freem) continue;
             const int free_k = __ffs(freem) - 1;
@@ -556,24 +563,53 @@ __global__ void k_link_colour_warp(DevParams P, DevState* S, SetView vd, snowb_p
         const uint32_t sx = 2u * (t % qx) + (colour & 1u);
         const uint32_t sy = 2u * ((t / qx) % qy) + ((colour >> 1) & 1u);
         const uint32_t sz = 2u * (t / (qx * qy)) + ((colour >> 2) & 1u);
-        for (uint32_t dz = 0; dz < 2; ++dz)
-            for (uint32_t dy = 0; dy < 2; ++dy)
-                for (uint32_t dx = 0; dx < 2; ++dx) {
-                    const uint32_t h = ((2u * sz + dz) * P.gsy + (2u * sy + dy)) * P.gsx + (2u * sx + dx);
-                    const uint32_t b = fs[h], e = fe[h];
-                    for (uint32_t i0 = b; i0 < e; i0 += 32u) {
-                        const uint32_t i = i0 + lane;
-                        uint32_t am = __ballot_sync(0xffffffffu, i < e && active[i]);
-                        while (am) {
-                            const int k = __ffs(am) - 1;
-                            am &= am - 1u;
-                            const uint32_t ii = i0 + (uint32_t)k;
-                            const uint32_t lc = lists ? L.cnt[L.cap + ii] : NL_OVF;
-                            if (lc & NL_OVF) link_particle_warp(P, vd, dem, ii, dynamic, S);
-                            else link_particle_list(P, vd, dem, ii, dynamic, S, L, lc & 1023u);
-                        }
-                    }
-                }
+        // The 8 cells (dz, dy, dx) in hash order -- ascending sorted index -- with lane c
+        // loading cell c's range; the super-cell's particles are then taken 32 at a time in
+        // that order (cell by cell, ascending index), as the cell-by-cell loops would.
+        uint32_t cb = 0, cn = 0;
+        if (lane < 8u) {
+            const uint32_t dz = lane >> 2, dy = (lane >> 1) & 1u, dx = lane & 1u;
+            const uint32_t h = ((2u * sz + dz) * P.gsy + (2u * sy + dy)) * P.gsx + (2u * sx + dx);
+            cb = fs[h];
+            cn = fe[h] - cb;
+        }
+        uint32_t incl = cn;
+#pragma unroll
+        for (uint32_t o = 1; o < 8u; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        uint32_t st[8], bs[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            st[q] = __shfl_sync(0xffffffffu, incl - cn, q);   // first flattened position of cell q
+            bs[q] = __shfl_sync(0xffffffffu, cb, q);
+        }
+        const uint32_t total_p = __shfl_sync(0xffffffffu, incl, 7);
+        for (uint32_t f0 = 0; f0 < total_p; f0 += 32u) {
+            const uint32_t f = f0 + lane;
+            uint32_t i = 0;
+            bool act = false;
+            if (f < total_p) {
+                // the last cell starting at or before f holds it (empty cells start where the
+                // next one does)
+                uint32_t s0 = st[0], b0 = bs[0];
+#pragma unroll
+                for (int r = 1; r < 8; ++r)
+                    if (st[r] <= f) { s0 = st[r]; b0 = bs[r]; }
+                i = b0 + (f - s0);
+                act = active[i] != 0;
+            }
+            uint32_t am = __ballot_sync(0xffffffffu, act);
+            while (am) {
+                const int k = __ffs(am) - 1;
+                am &= am - 1u;
+                const uint32_t ii = __shfl_sync(0xffffffffu, i, k);
+                const uint32_t lc = lists ? L.cnt[L.cap + ii] : NL_OVF;
+                if (lc & NL_OVF) link_particle_warp(P, vd, dem, ii, dynamic, S);
+                else link_particle_list(P, vd, dem, ii, dynamic, S, L, lc & 1023u);
+            }
+        }
     }
 }
 // general maximum_connection: the plain restatement with every access in memory
