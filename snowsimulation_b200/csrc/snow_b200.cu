@@ -646,6 +646,7 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
         STOP(base + 2);
         // the reference's snow PBF pass adds into repeated targets with float atomics (Q3):
         // its order follows the launch shape, so that pass keeps the built-in shape
+        TLAUNCH(k_pbf_water_warp, 256, (uint64_t)full * 32, 128, P, S, vs, vd, vb, X, ss, sd, sb, a.dt, F);
         TLAUNCH_IF(!ref, k_pbf, 256, 2 * full, 128, P, S, vs, vd, vb, X, ss, sd, sb, a.dt, F, NL);
         STOP(base + 3);
         TLAUNCH(k_dem_corr, 256, full, 128, P, S, vs, vd, vb, X, ss, sd, sb, F, NL);

@@ -54,114 +54,122 @@ struct NLWriter {
 
 // ------------------------------------------------------------ per-cell neighbour sums
 // pbf_correction (:883-929)
+__device__ __forceinline__ float3 pbf_own_cell(const DevParams& P, const SetView& v, float3 p, GCell g, int ox, int oy,
+                                               int oz, uint32_t skip, float li, const float* lam_s, const float* lam_o,
+                                               const float* con_s, const float* con_o, float dt)
+{
+    float3 cs = f3(0.f, 0.f, 0.f);
+    uint32_t s, e;
+    if (v.range(P, g, ox, oy, oz, s, e))
+        for (uint32_t j = s; j < e; ++j) {
+            if (j == skip) continue;
+            float3 dv = sub3(p, v.pos(j));
+            float d2 = dot3(dv, dv);
+            if (d2 < P.h2_lt) {
+                float d = sqrtf(d2);
+                float3 gr = G_spiky(P, dv, d);
+                float sc = scorr_of(P, d, dt);
+                float lj = v.attr(lam_s, lam_o, j), cj = v.attr(con_s, con_o, j);
+                cs = add3(cs, sc3(cj * ((li + lj) + sc), gr));
+            }
+        }
+    return cs;
+}
 __device__ __forceinline__ float3 acc_pbf_own(const DevParams& P, float3 acc, const SetView& v, float3 p, GCell g,
                                               uint32_t skip, float li, const float* lam_s, const float* lam_o,
                                               const float* con_s, const float* con_o, float dt)
 {
-    FOR27 {
-        float3 cs = f3(0.f, 0.f, 0.f);
-        uint32_t s, e;
-        if (v.range(P, g, ox, oy, oz, s, e))
-            for (uint32_t j = s; j < e; ++j) {
-                if (j == skip) continue;
-                float3 dv = sub3(p, v.pos(j));
-                float d2 = dot3(dv, dv);
-                if (d2 < P.h2_lt) {
-                    float d = sqrtf(d2);
-                    float3 gr = G_spiky(P, dv, d);
-                    float sc = scorr_of(P, d, dt);
-                    float lj = v.attr(lam_s, lam_o, j), cj = v.attr(con_s, con_o, j);
-                    cs = add3(cs, sc3(cj * ((li + lj) + sc), gr));
-                }
-            }
-        acc = add3(acc, cs);
-    }
+    FOR27 acc = add3(acc, pbf_own_cell(P, v, p, g, ox, oy, oz, skip, li, lam_s, lam_o, con_s, con_o, dt));
     return acc;
 }
 // pbf_correction_boundary (:932-979)
+__device__ __forceinline__ float3 pbf_bnd_cell(const DevParams& P, const SetView& v, float3 p, GCell g, int ox, int oy,
+                                               int oz, float li, const float* lam_s, const float* lam_o, float dt)
+{
+    float3 cs = f3(0.f, 0.f, 0.f);
+    uint32_t s, e;
+    if (v.range(P, g, ox, oy, oz, s, e))
+        for (uint32_t j = s; j < e; ++j) {
+            float3 dv = sub3(p, v.pos(j));
+            float d2 = dot3(dv, dv);
+            if (d2 < P.h2_lt) {
+                float d = sqrtf(d2);
+                float3 gr = G_spiky(P, dv, d);
+                float sc = scorr_of(P, d, dt);
+                cs = add3(cs, sc3((li + v.attr(lam_s, lam_o, j)) + sc, gr));
+            }
+        }
+    return cs;
+}
 __device__ __forceinline__ float3 acc_pbf_bnd(const DevParams& P, float3 acc, const SetView& v, float3 p, GCell g,
                                               float li, const float* lam_s, const float* lam_o, float dt)
 {
-    FOR27 {
-        float3 cs = f3(0.f, 0.f, 0.f);
-        uint32_t s, e;
-        if (v.range(P, g, ox, oy, oz, s, e))
-            for (uint32_t j = s; j < e; ++j) {
-                float3 dv = sub3(p, v.pos(j));
-                float d2 = dot3(dv, dv);
-                if (d2 < P.h2_lt) {
-                    float d = sqrtf(d2);
-                    float3 gr = G_spiky(P, dv, d);
-                    float sc = scorr_of(P, d, dt);
-                    cs = add3(cs, sc3((li + v.attr(lam_s, lam_o, j)) + sc, gr));
-                }
-            }
-        acc = add3(acc, cs);
-    }
+    FOR27 acc = add3(acc, pbf_bnd_cell(P, v, p, g, ox, oy, oz, li, lam_s, lam_o, dt));
     return acc;
 }
 // pbf_correction_coupling (:982-1034); reference quirks: the self-skip compares indices of
 // two different sets, and s_corr is taken as 0 (it reads an uninitialised value times 0)
+__device__ __forceinline__ float3 pbf_cpl_cell(const DevParams& P, const SetView& v, float3 p, GCell g, int ox, int oy,
+                                               int oz, uint32_t skip, float li, const float* lam_s, const float* lam_o,
+                                               float dt)
+{
+    const bool ref = P.quirks == SNOWB_QUIRKS_REFERENCE;
+    float3 cs = f3(0.f, 0.f, 0.f);
+    uint32_t s, e;
+    if (v.range(P, g, ox, oy, oz, s, e))
+        for (uint32_t j = s; j < e; ++j) {
+            if (ref && j == skip) continue;
+            float3 dv = sub3(p, v.pos(j));
+            float d2 = dot3(dv, dv);
+            if (d2 < P.r2_le) {
+                float d = sqrtf(d2);
+                float3 gr = G_poly6(P, dv, d);
+                float x = W_poly6(P, d) / P.scorr_div;
+                float x4 = (x * x) * (x * x);
+                float sc = ref ? ((((-P.scorr_coeff) * 0.f) * x4) * dt) * dt
+                               : ((-P.scorr_coeff * x4) * dt) * dt;
+                cs = add3(cs, sc3((li + v.attr(lam_s, lam_o, j)) + sc, gr));
+            }
+        }
+    return cs;
+}
 __device__ __forceinline__ float3 acc_pbf_cpl(const DevParams& P, float3 acc, const SetView& v, float3 p, GCell g,
                                               uint32_t skip, float li, const float* lam_s, const float* lam_o,
                                               float dt)
 {
-    const bool ref = P.quirks == SNOWB_QUIRKS_REFERENCE;
-    FOR27 {
-        float3 cs = f3(0.f, 0.f, 0.f);
-        uint32_t s, e;
-        if (v.range(P, g, ox, oy, oz, s, e))
-            for (uint32_t j = s; j < e; ++j) {
-                if (ref && j == skip) continue;
-                float3 dv = sub3(p, v.pos(j));
-                float d2 = dot3(dv, dv);
-                if (d2 < P.r2_le) {
-                    float d = sqrtf(d2);
-                    float3 gr = G_poly6(P, dv, d);
-                    float x = W_poly6(P, d) / P.scorr_div;
-                    float x4 = (x * x) * (x * x);
-                    float sc = ref ? ((((-P.scorr_coeff) * 0.f) * x4) * dt) * dt
-                                   : ((-P.scorr_coeff * x4) * dt) * dt;
-                    cs = add3(cs, sc3((li + v.attr(lam_s, lam_o, j)) + sc, gr));
-                }
-            }
-        acc = add3(acc, cs);
-    }
+    FOR27 acc = add3(acc, pbf_cpl_cell(P, v, p, g, ox, oy, oz, skip, li, lam_s, lam_o, dt));
     return acc;
 }
 // non-penetration: pbd_distance_correction_contrib (:1470-1527, skip) and
 // pbd_distance_correction_coupling_contrib (:1648-1705, no skip)
+// per-cell partial of acc_contact (cell at offset ox, oy, oz)
+__device__ __forceinline__ float3 contact_cell(const DevParams& P, const SetView& v, float3 p, GCell g, int ox, int oy,
+                                               int oz, uint32_t skip, float w0, const float* invm_s,
+                                               const float* invm_o)
+{
+    float3 cs = f3(0.f, 0.f, 0.f);
+    uint32_t s, e;
+    if (v.range_culled(P, g, ox, oy, oz, p, P.r2_cull, s, e))
+        for (uint32_t j = s; j < e; ++j) {
+            if (j == skip) continue;
+            float3 dv = sub3(p, v.pos(j));
+            float d2 = dot3(dv, dv);
+            if (d2 < P.r2_lt) {
+                float d = sqrtf(d2);
+                float w1 = v.attr(invm_s, invm_o, j);
+                float ws = w0 + w1;
+                float C = d - P.two_r;
+                float3 n = div3(dv, d + P.pbd_eps);
+                cs = add3(cs, sc3(((-w0) * (1.f / ws)) * C, n));
+            }
+        }
+    return cs;
+}
 __device__ __forceinline__ float3 acc_contact(const DevParams& P, float3 acc, const SetView& v, float3 p, GCell g,
                                               uint32_t skip, float w0, const float* invm_s, const float* invm_o)
 {
-    FOR27 {
-        float3 cs = f3(0.f, 0.f, 0.f);
-        uint32_t s, e;
-        if (v.range_culled(P, g, ox, oy, oz, p, P.r2_cull, s, e))
-            for (uint32_t j = s; j < e; ++j) {
-                if (j == skip) continue;
-                float3 dv = sub3(p, v.pos(j));
-                float d2 = dot3(dv, dv);
-                if (d2 < P.r2_lt) {
-                    float d = sqrtf(d2);
-                    float w1 = v.attr(invm_s, invm_o, j);
-                    float ws = w0 + w1;
-                    float C = d - P.two_r;
-                    float3 n = div3(dv, d + P.pbd_eps);
-                    cs = add3(cs, sc3(((-w0) * (1.f / ws)) * C, n));
-                }
-            }
-        acc = add3(acc, cs);
-    }
+    FOR27 acc = add3(acc, contact_cell(P, v, p, g, ox, oy, oz, skip, w0, invm_s, invm_o));
     return acc;
-}
-// pbd_sph_sph_distance_correction (:1586-1646)
-__device__ __forceinline__ float3 acc_contact_sph(const DevParams& P, float3 acc, const SetView& v, float3 p,
-                                                  GCell g, uint32_t skip, float w0, float contrib_i,
-                                                  const float* invm_s, const float* invm_o)
-{
-    if (!(contrib_i <= 0.99f)) return add3(acc, f3(0.f, 0.f, 0.f));
-    return acc_contact(P, acc, v, p, g, skip, w0, invm_s, invm_o);
 }
 
 // Replays of a recorded neighbour segment [k0, k1) of slot `slot`, per-cell partial sums
@@ -443,46 +451,11 @@ __global__ void __launch_bounds__(256) k_pbf(DevParams P, const DevState* __rest
     const uint32_t ns = S->n_sph, nd = S->n_dem, nb = S->n_b;
     vs.n = ns; vd.n = nd; vb.n = nb;
     const bool ref = P.quirks == SNOWB_QUIRKS_REFERENCE;
+    // the water particles' terms come from k_pbf_water_warp; the snow particles keep the
+    // thread mapping t = ns + i of the reference's launch (its float atomics, Q3, follow it)
     GRID_LOOP(t, ns + nd) {
         if (t < ns) {
-            const uint32_t i = t, o = vs.gi[i];
-            float3 p = xyz(vs.p4[i]); GCell g = grid_pos(P, p, vs.scene(i));
-            const float li = ss.lambda[i];
-            float3 c = f3(0.f, 0.f, 0.f);
-            Seg so, sx, sbn;
-            const bool lst = segments(L, i, so, sx, sbn);
-            if (lst) {
-                c = seg_pbf_own(P, c, so, vs, p, li, ss.lambda, X.sph.lambda, ss.contrib, X.sph.contrib, dt);
-                c = seg_pbf_cpl(P, c, sx, vd, p, i, li, sd.lambda, X.dem.lambda, dt);
-                c = seg_pbf_bnd(P, c, sbn, vb, p, li, sb.lambda, X.bnd.lambda, dt);
-            } else {
-                c = acc_pbf_own(P, c, vs, p, g, i, li, ss.lambda, X.sph.lambda, ss.contrib, X.sph.contrib, dt);
-                c = acc_pbf_cpl(P, c, vd, p, g, i, li, sd.lambda, X.dem.lambda, dt);
-                c = acc_pbf_bnd(P, c, vb, p, g, li, sb.lambda, X.bnd.lambda, dt);
-            }
-            c = sc3(P.inv_rho0, c);
-            const float ci = X.sph.contrib[o];
-            c = sc3(ci, c);
-            if (nan3(c)) c = f3(0.f, 0.f, 0.f);
-            float3 acc = add3(ldv3(X.sph.correction, o), c);
-            const float3 z = f3(0.f, 0.f, 0.f);
-            const float w0 = X.sph.massInv[o];
-            // the contact terms are scaled by (1 - contrib): with contrib == 1 they add a
-            // zero to a correction that is never -0 here, which leaves it unchanged
-            if (F.correct_dem && ci != 1.f) {     // compute_sph_dem_distance_correction
-                float3 d = lst ? seg_contact(P, z, sx, vd, p, w0, sd.invm, X.dem.massInv)
-                               : acc_contact(P, z, vd, p, g, SNOWB_UMAX, w0, sd.invm, X.dem.massInv);
-                d = sc3(1.f - ci, d);
-                if (nan3(d)) d = z;
-                acc = add3(acc, sc3(P.k_stretch, d));
-            }
-            if (F.sph_sph && ci != 1.f) {         // compute_sph_sph_distance_correction
-                float3 d = acc_contact_sph(P, z, vs, p, g, i, w0, ci, ss.invm, X.sph.massInv);
-                d = sc3(1.f - ci, d);
-                if (nan3(d)) d = z;
-                acc = add3(acc, d);
-            }
-            st3(X.sph.correction, o, acc);
+            continue;
         } else {
             const uint32_t i = t - ns;
             const uint32_t o = ref ? vs.gi[i] : vd.gi[i];   // Q3: SPH grid_index in the reference
@@ -925,6 +898,62 @@ __device__ __forceinline__ float3 warp_ordered_sum(float3 acc, float3 part)
         acc = add3(acc, v);
     }
     return acc;
+}
+
+// =============================================== PBF + contact corrections of the water set
+// compute_pbf_sph_correction (:3070-3184), compute_sph_dem_distance_correction (:2061-2110)
+// and compute_sph_sph_distance_correction (:1586-1646, :2164-2217) for the water particles,
+// one warp per particle: lane k < 27 computes the per-cell partial of cell k for each sum
+// (own water, coupling to snow, boundary, contacts) and the partials are added in cell
+// order with shuffles -- the sums the one-thread loops form, with 27 cells in flight.  The
+// water set is small (a few thousand particles at a time), so one thread per particle
+// left the GPU nearly idle while each thread walked its neighbours.
+__global__ void __launch_bounds__(256) k_pbf_water_warp(DevParams P, const DevState* __restrict__ S, SetView vs,
+                                                        SetView vd, SetView vb, Sets X, Sorted ss, Sorted sd,
+                                                        Sorted sb, float dt, StageFlags F)
+{
+    const uint32_t ns = S->n_sph;
+    vs.n = ns; vd.n = S->n_dem; vb.n = S->n_b;
+    const uint32_t lane = threadIdx.x & 31u;
+    const bool cl = lane < 27u;
+    const int ox = (int)(lane % 3u) - 1, oy = (int)((lane / 3u) % 3u) - 1, oz = (int)(lane / 9u) - 1;
+    const float3 z = f3(0.f, 0.f, 0.f);
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < ns; i += nwarps) {
+        const uint32_t o = vs.gi[i];
+        const float3 p = xyz(vs.p4[i]);
+        const GCell g = grid_pos(P, p, vs.scene(i));
+        const float li = ss.lambda[i];
+        float3 c = z;
+        c = warp_ordered_sum(c, cl ? pbf_own_cell(P, vs, p, g, ox, oy, oz, i, li, ss.lambda, X.sph.lambda, ss.contrib,
+                                                  X.sph.contrib, dt) : z);
+        c = warp_ordered_sum(c, cl ? pbf_cpl_cell(P, vd, p, g, ox, oy, oz, i, li, sd.lambda, X.dem.lambda, dt) : z);
+        c = warp_ordered_sum(c, cl ? pbf_bnd_cell(P, vb, p, g, ox, oy, oz, li, sb.lambda, X.bnd.lambda, dt) : z);
+        c = sc3(P.inv_rho0, c);
+        const float ci = X.sph.contrib[o];
+        c = sc3(ci, c);
+        if (nan3(c)) c = z;
+        float3 acc = add3(ldv3(X.sph.correction, o), c);
+        const float w0 = X.sph.massInv[o];
+        // the contact terms are scaled by (1 - contrib): with contrib == 1 they add a zero to
+        // a correction that is never -0 here, which leaves it unchanged
+        if (F.correct_dem && ci != 1.f) {     // compute_sph_dem_distance_correction
+            float3 d = warp_ordered_sum(z, cl ? contact_cell(P, vd, p, g, ox, oy, oz, SNOWB_UMAX, w0, sd.invm,
+                                                             X.dem.massInv) : z);
+            d = sc3(1.f - ci, d);
+            if (nan3(d)) d = z;
+            acc = add3(acc, sc3(P.k_stretch, d));
+        }
+        if (F.sph_sph && ci != 1.f) {         // compute_sph_sph_distance_correction (contrib <= 0.99 only)
+            float3 d = ci <= 0.99f
+                ? warp_ordered_sum(z, cl ? contact_cell(P, vs, p, g, ox, oy, oz, i, w0, ss.invm, X.sph.massInv) : z)
+                : add3(z, z);
+            d = sc3(1.f - ci, d);
+            if (nan3(d)) d = z;
+            acc = add3(acc, d);
+        }
+        if (lane == 0) st3(X.sph.correction, o, acc);
+    }
 }
 __device__ __forceinline__ float3 xsph_cell(const DevParams& P, const SetView& v, const snowb_particle_data& O,
                                             const snowb_float3* vel, float3 p, GCell g, int ox, int oy, int oz,
