@@ -518,7 +518,9 @@ __device__ __forceinline__ float3 link_corr(const DevParams& P, const snowb_part
     float ws = w0 + w1, C = dist - L;
     float3 n3 = div3(v, dist + P.pbd_eps);
     float3 r = sc3(((P.k_ref * -w0) * (1.f / ws)) * C, n3);
-    if (len3(r) > 1.f) return z;
+    // len3(r) > 1 without the square root: sqrtf is monotone and correctly rounded, and the
+    // smallest float whose root rounds above 1 is 1 + 2^-22, so the test is d2 > 1 + 2^-23
+    if (dot3(r, r) > 0x1.000002p+0f) return z;
     if (nan3(r)) return z;
     if (inf3(r)) return z;
     return r;
