@@ -444,6 +444,10 @@ __global__ void __launch_bounds__(256) k_density(DevParams P, DevState* __restri
 struct StageFlags {
     int correct_dem, sph_sph, interlink, step_sph, step_dem;
 };
+// Water sets up to this size run the water terms one warp per particle (k_pbf_water_warp):
+// with few particles one thread each leaves the GPU idle while each thread walks its
+// neighbours; above it, threads fill the GPU and the warp form's extra work would cost more.
+constexpr uint32_t PBF_WARP_MAX_WATER = 65536;
 __global__ void __launch_bounds__(256) k_pbf(DevParams P, const DevState* __restrict__ S, SetView vs, SetView vd,
                                              SetView vb, Sets X, Sorted ss, Sorted sd, Sorted sb, float dt,
                                              StageFlags F, NList L)
@@ -451,11 +455,51 @@ __global__ void __launch_bounds__(256) k_pbf(DevParams P, const DevState* __rest
     const uint32_t ns = S->n_sph, nd = S->n_dem, nb = S->n_b;
     vs.n = ns; vd.n = nd; vb.n = nb;
     const bool ref = P.quirks == SNOWB_QUIRKS_REFERENCE;
-    // the water particles' terms come from k_pbf_water_warp; the snow particles keep the
-    // thread mapping t = ns + i of the reference's launch (its float atomics, Q3, follow it)
+    // up to PBF_WARP_MAX_WATER water particles the water terms come from k_pbf_water_warp;
+    // the snow particles keep the thread mapping t = ns + i of the reference's launch (its
+    // float atomics, Q3, follow it)
     GRID_LOOP(t, ns + nd) {
         if (t < ns) {
-            continue;
+            if (ns <= PBF_WARP_MAX_WATER) continue;   // k_pbf_water_warp has them
+            const uint32_t i = t, o = vs.gi[i];
+            float3 p = xyz(vs.p4[i]); GCell g = grid_pos(P, p, vs.scene(i));
+            const float li = ss.lambda[i];
+            float3 c = f3(0.f, 0.f, 0.f);
+            Seg so, sx, sbn;
+            const bool lst = segments(L, i, so, sx, sbn);
+            if (lst) {
+                c = seg_pbf_own(P, c, so, vs, p, li, ss.lambda, X.sph.lambda, ss.contrib, X.sph.contrib, dt);
+                c = seg_pbf_cpl(P, c, sx, vd, p, i, li, sd.lambda, X.dem.lambda, dt);
+                c = seg_pbf_bnd(P, c, sbn, vb, p, li, sb.lambda, X.bnd.lambda, dt);
+            } else {
+                c = acc_pbf_own(P, c, vs, p, g, i, li, ss.lambda, X.sph.lambda, ss.contrib, X.sph.contrib, dt);
+                c = acc_pbf_cpl(P, c, vd, p, g, i, li, sd.lambda, X.dem.lambda, dt);
+                c = acc_pbf_bnd(P, c, vb, p, g, li, sb.lambda, X.bnd.lambda, dt);
+            }
+            c = sc3(P.inv_rho0, c);
+            const float ci = X.sph.contrib[o];
+            c = sc3(ci, c);
+            if (nan3(c)) c = f3(0.f, 0.f, 0.f);
+            float3 acc = add3(ldv3(X.sph.correction, o), c);
+            const float3 z = f3(0.f, 0.f, 0.f);
+            const float w0 = X.sph.massInv[o];
+            // the contact terms are scaled by (1 - contrib): with contrib == 1 they add a
+            // zero to a correction that is never -0 here, which leaves it unchanged
+            if (F.correct_dem && ci != 1.f) {     // compute_sph_dem_distance_correction
+                float3 d = lst ? seg_contact(P, z, sx, vd, p, w0, sd.invm, X.dem.massInv)
+                               : acc_contact(P, z, vd, p, g, SNOWB_UMAX, w0, sd.invm, X.dem.massInv);
+                d = sc3(1.f - ci, d);
+                if (nan3(d)) d = z;
+                acc = add3(acc, sc3(P.k_stretch, d));
+            }
+            if (F.sph_sph && ci != 1.f) {         // compute_sph_sph_distance_correction
+                // pbd_sph_sph_distance_correction (:1586-1646) acts only for contrib <= 0.99
+                float3 d = ci <= 0.99f ? acc_contact(P, z, vs, p, g, i, w0, ss.invm, X.sph.massInv) : add3(z, z);
+                d = sc3(1.f - ci, d);
+                if (nan3(d)) d = z;
+                acc = add3(acc, d);
+            }
+            st3(X.sph.correction, o, acc);
         } else {
             const uint32_t i = t - ns;
             const uint32_t o = ref ? vs.gi[i] : vd.gi[i];   // Q3: SPH grid_index in the reference
@@ -915,6 +959,7 @@ __global__ void __launch_bounds__(256) k_pbf_water_warp(DevParams P, const DevSt
                                                         Sorted sb, float dt, StageFlags F)
 {
     const uint32_t ns = S->n_sph;
+    if (ns > PBF_WARP_MAX_WATER) return;   // k_pbf runs the water terms one thread each
     vs.n = ns; vd.n = S->n_dem; vb.n = S->n_b;
     const uint32_t lane = threadIdx.x & 31u;
     const bool cl = lane < 27u;

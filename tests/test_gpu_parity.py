@@ -128,3 +128,16 @@ def test_moved_walls_bit_exact(cuda, quirks):
     _assert_same(o, g, "moved walls")
     x = g.to_host().dem["positions"][: g.n_dem]
     assert (x[:, 1] >= 0.01).all()
+
+
+@pytest.mark.parametrize("quirks", [QUIRKS_REFERENCE, QUIRKS_FIXED])
+def test_large_water_set_bit_exact(cuda, quirks):
+    """More than 65,536 water particles: the water PBF and contact terms take the one-thread
+    path instead of the warp-per-particle one (both must match the oracle)."""
+    w = scene.scene_drop((42, 42, 42), (10, 4, 10), seed=5, water_jitter=0.002, snow_jitter=0.002,
+                         drop_height=0.05, name="large water")
+    assert w.n_sph > 65536
+    o, g = _pair(w, quirks)
+    for k in range(2):
+        o.step(); g.step()
+        _assert_same(o, g, "substep %d" % k)
