@@ -693,19 +693,45 @@ __global__ void __launch_bounds__(256) k_friction(DevParams P, const DevState* _
         GCell g = grid_pos(P, p, vd.scene(i));
         const Nbhd nb = make_nbhd(P, g, p, P.r2_cull);
         float3 c = f3(0.f, 0.f, 0.f);
-        // snow-snow contacts
+        // snow-snow contacts (current entries screened two at a time with packed arithmetic
+        // against the slightly larger r2_cull, then the exact scalar test, as in the density
+        // pass)
+        const P2 pp = bcast2(p);
         uint32_t n = 0;
+        auto record = [&](uint32_t j, uint32_t cell) {
+            if (n < FR_K) rec[n * bd] = j | (cell << 25);
+            ++n;
+        };
         FOR27 {
             uint32_t s, e;
-            if (vd.range_nb(nb, ox, oy, oz, s, e))
-                for (uint32_t j = s; j < e; ++j) {
-                    if (j == i) continue;
-                    const float3 v = sub3(p, vd.pos(j));
-                    if (dot3(v, v) < P.r2_le) {
-                        if (n < FR_K) rec[n * bd] = j | ((uint32_t)CELL27 << 25);
-                        ++n;
+            if (vd.range_nb(nb, ox, oy, oz, s, e)) {
+                const uint32_t cell = (uint32_t)CELL27;
+                if (e <= vd.n) {
+                    uint32_t j = s;
+                    for (; j + 1 < e; j += 2) {
+                        const float4 q0 = __ldg(vd.p4 + j), q1 = __ldg(vd.p4 + j + 1);
+                        const float2 dd = d2_pair(pp, q0, q1);
+                        if (dd.x < P.r2_cull && j != i) {
+                            const float3 v = sub3(p, xyz(q0));
+                            if (dot3(v, v) < P.r2_le) record(j, cell);
+                        }
+                        if (dd.y < P.r2_cull && j + 1 != i) {
+                            const float3 v = sub3(p, xyz(q1));
+                            if (dot3(v, v) < P.r2_le) record(j + 1, cell);
+                        }
+                    }
+                    if (j < e && j != i) {
+                        const float3 v = sub3(p, vd.pos(j));
+                        if (dot3(v, v) < P.r2_le) record(j, cell);
+                    }
+                } else {
+                    for (uint32_t j = s; j < e; ++j) {
+                        if (j == i) continue;
+                        const float3 v = sub3(p, vd.pos(j));
+                        if (dot3(v, v) < P.r2_le) record(j, cell);
                     }
                 }
+            }
         }
         if (n <= FR_K) {
             float3 cs = f3(0.f, 0.f, 0.f);
@@ -745,14 +771,33 @@ __global__ void __launch_bounds__(256) k_friction(DevParams P, const DevState* _
         n = 0;
         FOR27 {
             uint32_t s, e;
-            if (vb.range_nb(nb, ox, oy, oz, s, e))
-                for (uint32_t j = s; j < e; ++j) {
-                    const float3 v = sub3(p, vb.pos(j));
-                    if (dot3(v, v) < P.r2_le) {
-                        if (n < FR_K) rec[n * bd] = j | ((uint32_t)CELL27 << 25);
-                        ++n;
+            if (vb.range_nb(nb, ox, oy, oz, s, e)) {
+                const uint32_t cell = (uint32_t)CELL27;
+                if (e <= vb.n) {
+                    uint32_t j = s;
+                    for (; j + 1 < e; j += 2) {
+                        const float4 q0 = __ldg(vb.p4 + j), q1 = __ldg(vb.p4 + j + 1);
+                        const float2 dd = d2_pair(pp, q0, q1);
+                        if (dd.x < P.r2_cull) {
+                            const float3 v = sub3(p, xyz(q0));
+                            if (dot3(v, v) < P.r2_le) record(j, cell);
+                        }
+                        if (dd.y < P.r2_cull) {
+                            const float3 v = sub3(p, xyz(q1));
+                            if (dot3(v, v) < P.r2_le) record(j + 1, cell);
+                        }
+                    }
+                    if (j < e) {
+                        const float3 v = sub3(p, vb.pos(j));
+                        if (dot3(v, v) < P.r2_le) record(j, cell);
+                    }
+                } else {
+                    for (uint32_t j = s; j < e; ++j) {
+                        const float3 v = sub3(p, vb.pos(j));
+                        if (dot3(v, v) < P.r2_le) record(j, cell);
                     }
                 }
+            }
         }
         const float3 dx0 = sub3(p, op0);
         if (n <= FR_K) {
