@@ -243,12 +243,16 @@ __device__ __forceinline__ float3 seg_pbf_cpl(const DevParams& P, float3 acc, co
 __device__ __forceinline__ float3 seg_contact(const DevParams& P, float3 acc, const Seg& S, const SetView& v,
                                               float3 p, float w0, const float* invm_s, const float* invm_o)
 {
+    // entries taken two at a time: their squared distances screened with packed arithmetic
+    // against the slightly larger r2_cull, the exact test and the term for those that pass;
+    // per-cell partials closed where the cell changes, entry by entry in order
+    const P2 pp = bcast2(p);
     float3 cs = f3(0.f, 0.f, 0.f);
     uint32_t cur = 0xFFu;
-    for (uint32_t k = S.k0; k < S.k1; ++k) {
-        const uint32_t en = S.at(k), j = en & NL_J_MASK, cell = (en >> 25) & 31u;
+    auto one = [&](uint32_t j, uint32_t cell, float3 q, bool pass) {
         if (cell != cur) { if (cur != 0xFFu) acc = add3(acc, cs); cs = f3(0.f, 0.f, 0.f); cur = cell; }
-        float3 dv = sub3(p, v.pos(j));
+        if (!pass) return;
+        float3 dv = sub3(p, q);
         float d2 = dot3(dv, dv);
         if (d2 < P.r2_lt) {
             float d = sqrtf(d2);
@@ -258,6 +262,19 @@ __device__ __forceinline__ float3 seg_contact(const DevParams& P, float3 acc, co
             float3 n = div3(dv, d + P.pbd_eps);
             cs = add3(cs, sc3(((-w0) * (1.f / ws)) * C, n));
         }
+    };
+    uint32_t k = S.k0;
+    for (; k + 1 < S.k1; k += 2) {
+        const uint32_t e0 = S.at(k), e1 = S.at(k + 1);
+        const uint32_t j0 = e0 & NL_J_MASK, j1 = e1 & NL_J_MASK;
+        const float3 q0 = v.pos(j0), q1 = v.pos(j1);
+        const float2 dd = d2_pair(pp, make_float4(q0.x, q0.y, q0.z, 0.f), make_float4(q1.x, q1.y, q1.z, 0.f));
+        one(j0, (e0 >> 25) & 31u, q0, dd.x < P.r2_cull);
+        one(j1, (e1 >> 25) & 31u, q1, dd.y < P.r2_cull);
+    }
+    if (k < S.k1) {
+        const uint32_t e0 = S.at(k), j0 = e0 & NL_J_MASK;
+        one(j0, (e0 >> 25) & 31u, v.pos(j0), true);
     }
     if (cur != 0xFFu) acc = add3(acc, cs);
     return acc;
