@@ -223,6 +223,7 @@ __device__ __forceinline__ bool has_free_slot(const uint32_t* rec, uint32_t o, u
 }
 // L: the snow-snow candidate lists of the substep's first density pass (L.cnt null: none),
 // replayed instead of the traversal while no phase change re-sorted the sets.
+constexpr uint32_t LF_G = 4;
 __global__ void __launch_bounds__(256) k_link_filter(DevParams P, DevState* S, SetView vd,
                                                      snowb_particle_data dem, int dynamic,
                                                      uint8_t* __restrict__ active, NList L)
@@ -244,28 +245,51 @@ __global__ void __launch_bounds__(256) k_link_filter(DevParams P, DevState* S, S
         for (int k = 0; k < SNOWB_MAXC_FAST; ++k)
             r[k] = below && fast && (uint32_t)k < M ? dem.connect_record[M * o + k] : 0u;
         const uint32_t lc = lists ? L.cnt[L.cap + i] : NL_OVF;
-        if (!(lc & NL_OVF) && below && has_free_slot(dem.connect_record, o, M)) {
-            // the same scan over the listed candidates (cells in order, d < h, j != i)
+        // a free slot of o: from the registers (slots k >= M hold 0, never empty)
+        bool own_free = false;
+        if (below) {
+            if (fast) {
+#pragma unroll
+                for (int k = 0; k < SNOWB_MAXC_FAST; ++k) own_free |= r[k] == SNOWB_UMAX;
+            } else {
+                own_free = has_free_slot(dem.connect_record, o, M);
+            }
+        }
+        if (!(lc & NL_OVF) && own_free) {
+            // the same scan over the listed candidates (cells in order, d < h, j != i), taken
+            // LF_G at a time: entries, partners' original indices and counts are loaded for
+            // the group (all in range: listed entries are current sorted indices), then the
+            // candidates are examined in order
             uint32_t skip_cell = 0xFFu;
             const uint32_t nl = lc & 1023u;
-            for (uint32_t k = 0; k < nl && !act; ++k) {
-                const uint32_t en = L.e[(size_t)k * L.stride + L.cap + i];
-                const uint32_t cell = (en >> 25) & 31u;
-                if (cell == skip_cell) continue;
-                const uint32_t o1 = vd.gi[en & NL_J_MASK];
-                if (o1 == o) { act = 1; break; }
-                bool found = false;
-                if (fast) {
+            for (uint32_t k0 = 0; k0 < nl && !act; k0 += LF_G) {
+                uint32_t en[LF_G], o1[LF_G], ie[LF_G];
 #pragma unroll
-                    for (int q = 0; q < SNOWB_MAXC_FAST; ++q) found |= (uint32_t)q < M && r[q] == o1;
-                } else {
-                    for (uint32_t q = M * o; q < M * (o + 1); ++q)
-                        if (dem.connect_record[q] == o1) { found = true; break; }
+                for (uint32_t u = 0; u < LF_G; ++u)
+                    en[u] = k0 + u < nl ? L.e[(size_t)(k0 + u) * L.stride + L.cap + i] : 0u;
+#pragma unroll
+                for (uint32_t u = 0; u < LF_G; ++u) o1[u] = k0 + u < nl ? vd.gi[en[u] & NL_J_MASK] : 0u;
+#pragma unroll
+                for (uint32_t u = 0; u < LF_G; ++u) ie[u] = k0 + u < nl ? dem.iter_end[o1[u]] : 0u;
+#pragma unroll
+                for (uint32_t u = 0; u < LF_G; ++u) {
+                    if (k0 + u >= nl || act) break;
+                    const uint32_t cell = (en[u] >> 25) & 31u;
+                    if (cell == skip_cell) continue;
+                    if (o1[u] == o) { act = 1; break; }
+                    bool found = false;
+                    if (fast) {
+#pragma unroll
+                        for (int q = 0; q < SNOWB_MAXC_FAST; ++q) found |= (uint32_t)q < M && r[q] == o1[u];
+                    } else {
+                        for (uint32_t q = M * o; q < M * (o + 1); ++q)
+                            if (dem.connect_record[q] == o1[u]) { found = true; break; }
+                    }
+                    if (found) { skip_cell = cell; continue; }
+                    if (ie[u] < (o1[u] + 1) * M && has_free_slot(dem.connect_record, o1[u], M)) act = 1;
                 }
-                if (found) { skip_cell = cell; continue; }
-                if (dem.iter_end[o1] < (o1 + 1) * M && has_free_slot(dem.connect_record, o1, M)) act = 1;
             }
-        } else if ((lc & NL_OVF) && below && has_free_slot(dem.connect_record, o, M)) {
+        } else if ((lc & NL_OVF) && own_free) {
             const GCell g = grid_pos(P, p, vd.scene(i));
             FOR27 {
                 uint32_t s, e;
