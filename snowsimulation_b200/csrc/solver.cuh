@@ -243,9 +243,9 @@ __device__ __forceinline__ float3 seg_pbf_cpl(const DevParams& P, float3 acc, co
 __device__ __forceinline__ float3 seg_contact(const DevParams& P, float3 acc, const Seg& S, const SetView& v,
                                               float3 p, float w0, const float* invm_s, const float* invm_o)
 {
-    // entries taken two at a time: their squared distances screened with packed arithmetic
-    // against the slightly larger r2_cull, the exact test and the term for those that pass;
-    // per-cell partials closed where the cell changes, entry by entry in order
+    // entries taken four (then two) at a time: their squared distances screened with packed
+    // arithmetic against the slightly larger r2_cull, the exact test and the term for those
+    // that pass; per-cell partials closed where the cell changes, entry by entry in order
     const P2 pp = bcast2(p);
     float3 cs = f3(0.f, 0.f, 0.f);
     uint32_t cur = 0xFFu;
@@ -264,6 +264,17 @@ __device__ __forceinline__ float3 seg_contact(const DevParams& P, float3 acc, co
         }
     };
     uint32_t k = S.k0;
+    for (; k + 3 < S.k1; k += 4) {
+        const uint32_t e0 = S.at(k), e1 = S.at(k + 1), e2 = S.at(k + 2), e3 = S.at(k + 3);
+        const uint32_t j0 = e0 & NL_J_MASK, j1 = e1 & NL_J_MASK, j2 = e2 & NL_J_MASK, j3 = e3 & NL_J_MASK;
+        const float3 q0 = v.pos(j0), q1 = v.pos(j1), q2 = v.pos(j2), q3 = v.pos(j3);
+        const float2 da = d2_pair(pp, make_float4(q0.x, q0.y, q0.z, 0.f), make_float4(q1.x, q1.y, q1.z, 0.f));
+        const float2 db = d2_pair(pp, make_float4(q2.x, q2.y, q2.z, 0.f), make_float4(q3.x, q3.y, q3.z, 0.f));
+        one(j0, (e0 >> 25) & 31u, q0, da.x < P.r2_cull);
+        one(j1, (e1 >> 25) & 31u, q1, da.y < P.r2_cull);
+        one(j2, (e2 >> 25) & 31u, q2, db.x < P.r2_cull);
+        one(j3, (e3 >> 25) & 31u, q3, db.y < P.r2_cull);
+    }
     for (; k + 1 < S.k1; k += 2) {
         const uint32_t e0 = S.at(k), e1 = S.at(k + 1);
         const uint32_t j0 = e0 & NL_J_MASK, j1 = e1 & NL_J_MASK;
