@@ -597,9 +597,9 @@ __device__ __forceinline__ float3 link_corr(const DevParams& P, const snowb_part
     if (inf3(r)) return z;
     return r;
 }
-// compute_dem_sph_distance_correction (:2112-2162), compute_dem_distance_correction
-// (:1765-1834) and solve_snow_interlink_constraint_d (:4742-4765) for snow particle o,
-// added to its correction in the reference's kernel order (after the PBF pass).
+// compute_dem_sph_distance_correction (:2112-2162) and compute_dem_distance_correction
+// (:1765-1834) for snow particle o, added to its correction in the reference's kernel
+// order (after the PBF pass; the interlink terms of k_interlink follow).
 __global__ void __launch_bounds__(256) k_dem_corr(DevParams P, const DevState* __restrict__ S, SetView vs, SetView vd,
                                                   SetView vb, Sets X, Sorted ss, Sorted sd, Sorted sb, StageFlags F,
                                                   NList L)
