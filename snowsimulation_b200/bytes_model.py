@@ -46,7 +46,8 @@ def kernel_bytes(name, n_water, n_snow, n_boundary):
         "k_density": p["D"] * (n_water + n_snow + n_boundary),
         "k_lambda": p["L"] * (n_water + n_snow + n_boundary),
         "k_pbf": (p["P"] + p["X"]) * n_water + p["P"] * n_snow,
-        "k_dem_corr": (p["X"] + p["I"]) * n_snow,
+        "k_dem_corr": p["X"] * n_snow,
+        "k_interlink": p["I"] * n_snow,
         "k_friction": p["F"] * n_snow,
         "k_heat": p["H"] * (n_water + n_snow),
         "k_integrate": p["G"] * (n_water + n_snow),
