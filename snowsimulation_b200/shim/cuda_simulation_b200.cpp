@@ -1,12 +1,15 @@
 // cuda_simulation_b200.cpp -- the reference's cuda_simulation.cuh entry points
-// (cuda_simulation.cuh:13-75, C++ linkage, void returns) on top of libsnowb200's C ABI.
-// Compiled with the reference's headers in place of cuda_simulation.cu and cuda_tool.cu;
-// errors print the library's message and exit, as the reference's checkCudaErrors does.
+// (cuda_simulation.cuh:13-75, C++ linkage, void returns) and cuda_tool.cuh's fills on top
+// of libsnowb200's C ABI.  Compiled with the reference's headers in place of
+// cuda_simulation.cu and cuda_tool.cu; errors print the library's message and exit, as the
+// reference's checkCudaErrors does.
 #include "cuda_simulation.cuh"      // reference header: ParticleSet, CellData, SimParams, SceneParams
+#include "cuda_tool.cuh"            // reference header: cuda_tool_fill_uint / _float
 #include "snow_b200.h"              // this library
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <vector>
 
 static_assert(sizeof(ParticleDeviceData) == sizeof(snowb_particle_data), "layout");
 static_assert(sizeof(CellData) == sizeof(snowb_cell_data), "layout");
@@ -42,3 +45,16 @@ void snow_simulation(ParticleSet* sph, ParticleSet* dem, ParticleSet* b, Particl
     sph->setSize(ns);          // the reference's compact_and_clean does this (cuda_simulation.cu:4545-4546)
     dem->setSize(nd);
 }
+
+// cuda_tool.cu:3-13: d_arr[start, end) = value.  Called by ParticleSystem's set-up only, so
+// one synchronous copy of a host buffer, after the library's stream has drained.
+template <class T>
+static void fill_range(T* d, size_t start, size_t end, T value) {
+    if (end <= start) return;
+    check(snowb_synchronize());
+    std::vector<T> h(end - start, value);
+    const cudaError_t e = cudaMemcpy(d + start, h.data(), (end - start) * sizeof(T), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) { std::fprintf(stderr, "cuda_tool fill: %s\n", cudaGetErrorString(e)); std::exit(1); }
+}
+void cuda_tool_fill_uint(uint* d_arr, size_t start, size_t end, uint value)    { fill_range(d_arr, start, end, value); }
+void cuda_tool_fill_float(float* d_arr, size_t start, size_t end, float value) { fill_range(d_arr, start, end, value); }
