@@ -1,6 +1,6 @@
 // Link check of the C++ shim (test infrastructure, built by shim_check.sh): a caller
 // compiled against the reference's own declarations (cuda_simulation.cuh:13-75,
-// cuda_tool.cuh:11-12) refers to every entry point and is linked with no undefined symbol
+// cuda_tool.cuh:12-13) refers to every entry point and is linked with no undefined symbol
 // against the shim.  A shim definition whose signature drifted from the declaration would
 // be a separate overload and leave this caller's reference unresolved.  Nothing here is
 // ever run.
