@@ -173,3 +173,19 @@ def test_domain_default_is_reference_and_floor_moves():
     for _ in range(3):
         o2.step()
     assert o2.w.dem["positions"][: o2.w.n_dem, 1].min() < 0.03
+
+
+@pytest.mark.parametrize("empty", ["water", "snow"])
+def test_empty_set_substeps(empty):
+    """A scene whose water or snow set is empty from the start steps through whole
+    substeps (its sorts see zero particles); the other set stays finite and keeps its size."""
+    snow = [[0.3 + 0.02 * i, 0.5, 0.3] for i in range(8)]
+    water = [[0.02 * i, 0.3, 0.0] for i in range(8)]
+    w = _world([] if empty == "water" else water, [] if empty == "snow" else snow)
+    o = OracleWorld(w, 64).setup()
+    for _ in range(3):
+        o.step()
+    ns, nd = o.w.n_sph, o.w.n_dem
+    assert (ns, nd) == ((0, 8) if empty == "water" else (8, 0))
+    live = o.w.dem["positions"][:nd] if empty == "water" else o.w.sph["positions"][:ns]
+    assert np.all(np.isfinite(live))
