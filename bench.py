@@ -19,9 +19,9 @@ config 3 (40 substeps, forward with checkpoints + backward) against the same sub
 plain (--no-adjoint skips it), and "large": 3 frames of the 1.18M-particle config 4 in a
 widened domain (--no-large skips it).
 
---impl reference times the CPU restatement of the same substep (FP32, all host threads,
-one substep per step), the only CPU implementation of this path: the reference itself
-runs it only on a GPU.
+--impl reference times the CPU restatement of the same substep (FP32, all host threads) on
+the same frames of the same scene (W warm-up frames, K timed frames of 4 substeps), the
+only CPU implementation of this path: the reference itself runs it only on a GPU.
 """
 import argparse
 import ctypes as C
@@ -53,6 +53,7 @@ def parse():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-large", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--fp64-frames", type=int, default=24)
     ap.add_argument("--profile-out", default="")
     return ap.parse_args()
 
@@ -189,9 +190,12 @@ def reference_cpu_baselines(water_pos, snow_pos, links, snow_mass, h, dt, iters=
 
 
 # ----------------------------------------------------------------- error vs FP64
-def fp64_error(scene_name, dev, frames=2):
+def fp64_error(scene_name, dev, frames=24):
     """The GPU run of the timed scene against the FP64 oracle from the same start, frame by
-    frame (particles matched by track id): maximum position and temperature differences."""
+    frame (particles matched by track id, whichever set holds them): maximum position,
+    velocity and temperature differences, and the total heat energy sum(m C T) and momentum
+    sum(m v) of both runs (FP64 reductions: snowb_energy_momentum on the GPU state, the
+    oracle's own sums on its state), with their drift from the start."""
     import numpy as np
     from snowsimulation_b200 import scene
     from snowsimulation_b200.world import Simulation
@@ -202,32 +206,59 @@ def fp64_error(scene_name, dev, frames=2):
     out = []
 
     def by_id(world_sets):
-        ids, xs, ts = [], [], []
+        ids, xs, vs, ts = [], [], [], []
         for d, n in world_sets:
-            ids.append(d["trackId"][:n]); xs.append(d["positions"][:n]); ts.append(d["T"][:n])
+            ids.append(d["trackId"][:n]); xs.append(d["positions"][:n]); vs.append(d["velocity"][:n])
+            ts.append(d["T"][:n])
         ids = np.concatenate(ids)
         order = np.argsort(ids)
-        return ids[order], np.concatenate(xs)[order].astype(np.float64), np.concatenate(ts)[order].astype(np.float64)
+        f64 = lambda a: np.concatenate(a)[order].astype(np.float64)
+        return ids[order], f64(xs), f64(vs), f64(ts)
 
+    e0g, e0o = sim.energy_momentum(), o.energy_momentum()
+    t0 = time.perf_counter()
     for f in range(frames):
         sim.step(substeps=SUBSTEPS)
         for _ in range(SUBSTEPS):
             o.step()
         H = sim.to_host()
-        ig, xg, tg = by_id(((H.sph, H.n_sph), (H.dem, H.n_dem)))
-        io, xo, to = by_id(((o.w.sph, o.w.n_sph), (o.w.dem, o.w.n_dem)))
+        ig, xg, vg, tg = by_id(((H.sph, H.n_sph), (H.dem, H.n_dem)))
+        io, xo, vo, to = by_id(((o.w.sph, o.w.n_sph), (o.w.dem, o.w.n_dem)))
         same = np.array_equal(ig, io)
-        rec = {"frame": f, "same_particles": bool(same), "sizes": [H.n_sph, H.n_dem]}
+        eg, eo = sim.energy_momentum(), o.energy_momentum()
+        rec = {"frame": f, "same_particles": bool(same), "sizes": [H.n_sph, H.n_dem],
+               "sizes_fp64": [o.w.n_sph, o.w.n_dem]}
         if same:
             rec["pos_max_m"] = float(np.abs(xg - xo).max())
+            rec["vel_max_mps"] = float(np.abs(vg - vo).max())
             rec["T_max_C"] = float(np.abs(tg - to).max())
+        rec["energy_J"] = eg[0]
+        rec["energy_fp64_J"] = eo[0]
+        rec["energy_drift_rel"] = (eg[0] - e0g[0]) / abs(e0g[0])
+        rec["energy_drift_fp64_rel"] = (eo[0] - e0o[0]) / abs(e0o[0])
+        rec["momentum"] = eg[1:]
+        rec["momentum_fp64"] = eo[1:]
         out.append(rec)
+    el = time.perf_counter() - t0
+    fin = [r for r in out if r.get("same_particles")]
+    summary = {}
+    if fin:
+        summary = {"pos_max_m": max(r["pos_max_m"] for r in fin), "vel_max_mps": max(r["vel_max_mps"] for r in fin),
+                   "T_max_C": max(r["T_max_C"] for r in fin),
+                   "energy_rel_diff_max": max(abs(r["energy_J"] - r["energy_fp64_J"]) / abs(r["energy_fp64_J"])
+                                              for r in out),
+                   "first_contact_frame": next((r["frame"] for r in fin if r["T_max_C"] > 0.0), None)}
     return {"workload": "%s from rest, %d frames of %d substeps" % (scene_name, frames, SUBSTEPS),
-            "oracle": "FP64 C restatement of the substep (oracle/), reference quirks", "per_frame": out}
+            "oracle": "FP64 C restatement of the substep (oracle/), reference quirks, OpenMP %d threads, %.0f s"
+                      % (os.cpu_count() or 1, el),
+            "summary": summary, "per_frame": out}
 
 
 # ----------------------------------------------------------------- reference arm
 def run_reference(args):
+    """The CPU restatement of the substep on the same workload as the other arm: the same
+    scene from rest, W untimed frames, then K timed frames of SUBSTEPS substeps (wall
+    clock), all host threads; rank 0 only."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return 0
@@ -237,34 +268,41 @@ def run_reference(args):
     cores = os.cpu_count() or 1
     o = OracleWorld(w, 32, threads=cores).setup()
     n = w.n_sph + w.n_dem
-    warm = max(1, min(args.warmup, 1))
-    for _ in range(warm):
+    warm = max(3, args.warmup)
+    for _ in range(warm * SUBSTEPS):
         o.step()
-    budget = 150.0
+    budget = 240.0   # bound on the timed region (a slow host times fewer frames and says so)
     t0 = time.perf_counter()
     done = 0
     while done < args.steps:
-        o.step()
+        for _ in range(SUBSTEPS):
+            o.step()
         done += 1
         if time.perf_counter() - t0 > budget:
             break
     el = time.perf_counter() - t0
-    val = n * done / el
+    val = n * SUBSTEPS * done / el
+    workload = workload_name(args.scene, w)
     line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
             "steps": done, "warmup": warm, "ms_per_step": 1000.0 * el / done, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": args.scene + " (5888 water + 147928 snow + 52016 boundary), one substep per step",
-                       "substeps_per_step": 1, "iterations": 3, "l2": "n/a (CPU)"},
+            "config": {"workload": workload, "substeps_per_step": SUBSTEPS, "iterations": w.iterations,
+                       "quirks": "reference", "parallelism": "single", "l2": "n/a (CPU)"},
             "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": "%d substep(s), FP32 C restatement of the substep (oracle/), "
-                                       "OpenMP %d threads; the reference runs this path only on a GPU"
-                                       % (done, cores)},
+                             "sample": "frames %d-%d (%d substeps each) of %s from rest, FP32 C restatement of the "
+                                       "substep (oracle/), OpenMP %d threads; the reference runs this path only on "
+                                       "a GPU" % (warm, warm + done - 1, SUBSTEPS, args.scene, cores)},
             "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     gpu = reference_gpu_runner(args.scene, args.warmup, min(args.steps, 20))
     if gpu is not None:
         line["gpu_runner"] = gpu
     print(json.dumps(line))
     return 0
+
+
+def workload_name(scene_name, w):
+    return ("%s: %d water + %d snow + %d boundary particles, 1 step = 1 frame = %d substeps (dt 1/240 s, "
+            "%d iterations), seeded lattice" % (scene_name, w.n_sph, w.n_dem, w.n_b, SUBSTEPS, w.iterations))
 
 
 def reference_gpu_runner(scene_name, warmup, frames):
@@ -667,9 +705,7 @@ def main():
         "warmup": max(3, args.warmup), "ms_per_step": ms_per_step, "frame_ms_percentiles": pct,
         "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "%s: %d water + %d snow + %d boundary particles, 1 step = 1 frame = %d substeps "
-                               "(dt 1/240 s, 3 iterations), seeded lattice" % (args.scene, w.n_sph, w.n_dem,
-                                                                               w.n_b, SUBSTEPS),
+        "config": {"workload": workload_name(args.scene, w),
                    "substeps_per_step": SUBSTEPS, "iterations": w.iterations,
                    "quirks": "reference", "parallelism": "replicas" if ws > 1 else "single",
                    "l2": "flushed between timed steps (256 MB write)"},
@@ -698,7 +734,7 @@ def main():
             rest_state[0], rest_state[1], rest_state[2], rest_state[3], h=float(w.params.effective_radius),
             dt=1.0 / (60.0 * SUBSTEPS))
     if ws == 1 and not args.no_fp64:
-        line["fp64_error"] = fp64_error(args.scene, dev)
+        line["fp64_error"] = fp64_error(args.scene, dev, args.fp64_frames)
     print(json.dumps(line))
     if ws > 1:
         dist.destroy_process_group()

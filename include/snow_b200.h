@@ -8,14 +8,19 @@
  * CellData, SceneParams&); this ABI takes the same data as plain C structs of
  * device pointers whose layout is identical to the reference's structs
  * (ParticleDeviceData, CellData, SimParams, SceneParams), so a caller can pass
- * &particle_set->m_device_data unchanged.  INTEGRATION.md shows the C++ shim that
- * restores the reference's exact signatures on top of this ABI.
+ * &particle_set->m_device_data unchanged.  The C++ shim in
+ * snowsimulation_b200/shim/cuda_simulation_b200.cpp restores the reference's exact
+ * signatures on top of this ABI.
  *
  * Conventions (all entry points):
  *   - buffers are owned by the caller and live in device memory of the current device;
  *   - every function returns SNOWB_OK (0) or a negative SNOWB_ERR_* code and never
  *     calls exit(); snowb_last_error_string() describes the last failure;
- *   - work is issued on the stream set by snowb_set_stream (default: legacy stream 0).
+ *   - work is issued on the stream set by snowb_set_stream (default: legacy stream 0);
+ *   - the library is single-threaded, as the reference's host interface is: its scratch
+ *     buffers, graph cache, tape and profiling state are process-wide, so one host thread
+ *     calls it at a time (calls from several threads must be serialised by the caller);
+ *   - its device state does not survive a cudaDeviceReset; call snowb_release first.
  */
 #ifndef SNOW_B200_H
 #define SNOW_B200_H
@@ -127,13 +132,18 @@ int snowb_calculate_hash(snowb_cell_data cell_data, const snowb_float3* pos, uin
 int snowb_sort_particles(snowb_cell_data cell_data, uint32_t num_particles);
 
 /* No counterpart in the reference.  The stable sort of snowb_sort_particles for callers
- * that cannot allocate device memory (a host capturing its frame into a CUDA graph, a loop
- * that forbids allocation after start-up, a process under a fixed memory budget).  It
- * allocates nothing: its scratch is a static device array of about 6 MB that every GPU
- * loading the library holds until exit.  Limits: at most 262144 particles and 262144 cells
- * (larger requests fail with SNOWB_ERR_INVALID).  The first call on a device looks up the
- * array's address and should come before any stream capture.  Calls share the array, so
- * calls that overlap on the GPU race; the caller serialises them.  Blocks until done. */
+ * that cannot allocate device memory: a render or game loop that forbids allocation after
+ * start-up (cudaMalloc may synchronise the device mid-frame), a plugin whose host owns
+ * every device allocation, a process under a fixed device-memory budget.  It allocates
+ * nothing: its scratch is a static device array of about 6 MB that every GPU loading the
+ * library holds until exit.  Limits: at most SNOWB_STATIC_SORT_MAX_PARTICLES particles and
+ * SNOWB_STATIC_SORT_MAX_CELLS cells (larger requests fail with SNOWB_ERR_INVALID).  The
+ * first call on a device looks up the array's address and should come before any stream
+ * capture.  Calls share the array, so calls that overlap on the GPU race; the caller
+ * serialises them.  Not usable after a cudaDeviceReset in the same process.  Blocks until
+ * done. */
+#define SNOWB_STATIC_SORT_MAX_PARTICLES (1u << 18)
+#define SNOWB_STATIC_SORT_MAX_CELLS (1u << 18)
 int snowb_sort_particles_static(snowb_cell_data cell_data, uint32_t num_particles);
 
 /* reorder_data (cuda_simulation.cu:377-396 / reorderDataAndFindCellStartD :242-301):

@@ -87,3 +87,20 @@ def flag_bits(flags):
 
 QUIRKS_REFERENCE = 0
 QUIRKS_FIXED = 1
+
+
+def _header_limit(name):
+    """Value of a `#define NAME (1u << k)` limit in include/snow_b200.h."""
+    import os
+    import re
+    here = os.path.dirname(os.path.abspath(__file__))
+    txt = open(os.path.join(here, "..", "include", "snow_b200.h")).read()
+    m = re.search(r"#define\s+%s\s+\(1u\s*<<\s*(\d+)\)" % name, txt)
+    if not m:
+        raise RuntimeError("%s not found in include/snow_b200.h" % name)
+    return 1 << int(m.group(1))
+
+
+# Limits of snowb_sort_particles_static (its static device scratch), from the header.
+STATIC_SORT_MAX_PARTICLES = _header_limit("SNOWB_STATIC_SORT_MAX_PARTICLES")
+STATIC_SORT_MAX_CELLS = _header_limit("SNOWB_STATIC_SORT_MAX_CELLS")

@@ -1318,19 +1318,19 @@ int snowb_sort_particles(snowb_cell_data cd, uint32_t n)
 }
 
 // ---------------------------------------------------------------------------
-// Sort without allocation.  Some callers cannot call cudaMalloc: a host that captures
-// its whole frame into a CUDA graph (allocation is not capturable), a renderer or game
-// loop that forbids allocation after start-up, or a process running under a fixed
-// device-memory budget.  snowb_sort_particles_static does the same stable sort as
+// Sort without allocation.  Some callers cannot call cudaMalloc: a renderer or game loop
+// that forbids allocation after start-up (cudaMalloc may synchronise the device and stall
+// the frame), a plugin whose host owns every device allocation, or a process running under
+// a fixed device-memory budget.  snowb_sort_particles_static does the same stable sort as
 // snowb_sort_particles, but all its scratch lives in the fixed array below, which the
 // module reserves once on every device that loads this library and keeps until exit.
 // In host code the array's name is only a host-side stand-in, so its device address is
 // taken with cudaGetSymbolAddress once per device (on the first call made with that
 // device current; that first call should come before any stream capture).  All calls
 // share the array: calls that overlap on the GPU (other streams, other host threads)
-// race and must be serialised by the caller.
-#define SNOWB_STATIC_SORT_MAX_PARTICLES (1u << 18)
-#define SNOWB_STATIC_SORT_MAX_CELLS (1u << 18)
+// race and must be serialised by the caller.  The address is kept for the life of the
+// process; a cudaDeviceReset in between is not supported (the library's other device
+// state does not survive one either).  The limits are in include/snow_b200.h.
 static constexpr size_t kStaticBsum = SNOWB_STATIC_SORT_MAX_CELLS / SCAN_CHUNK + 2;
 static constexpr size_t kStaticWords = 4ull * SNOWB_STATIC_SORT_MAX_PARTICLES + SNOWB_STATIC_SORT_MAX_CELLS +
                                        (SNOWB_STATIC_SORT_MAX_CELLS + 1) + kStaticBsum + 1;

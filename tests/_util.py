@@ -57,3 +57,22 @@ def live(world, set_name):
 def track_ids(world):
     ids = np.concatenate([world.sph["trackId"][:world.n_sph], world.dem["trackId"][:world.n_dem]])
     return np.sort(ids)
+
+
+def max_abs_diff(a, b, fields=("positions", "velocity", "T")):
+    """Largest |a - b| per field over the live particles of both sets, matched by track id
+    (the sets' slot orders agree when the runs are bit-exact, but need not otherwise)."""
+    out = {}
+    for f in fields:
+        xs = []
+        for w in (a, b):
+            ids = np.concatenate([w.sph["trackId"][:w.n_sph], w.dem["trackId"][:w.n_dem]])
+            val = np.concatenate([w.sph[f][:w.n_sph], w.dem[f][:w.n_dem]]).astype(np.float64)
+            xs.append((ids, val))
+        (ia, va), (ib, vb) = xs
+        if not np.array_equal(np.sort(ia), np.sort(ib)):
+            out[f] = None
+            continue
+        va, vb = va[np.argsort(ia)], vb[np.argsort(ib)]
+        out[f] = float(np.abs(va - vb).max()) if len(va) else 0.0
+    return out

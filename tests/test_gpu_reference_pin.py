@@ -109,25 +109,65 @@ def test_link_topology_against_reference(cuda):
     assert deg_o.max() <= 25 and deg_r.max() <= 25
 
 
+def _by_id(w, field):
+    ids = np.concatenate([w.sph["trackId"][:w.n_sph], w.dem["trackId"][:w.n_dem]])
+    v = np.concatenate([w.sph[field][:w.n_sph], w.dem[field][:w.n_dem]]).astype(np.float64)
+    o = np.argsort(ids)
+    return ids[o], v[o]
+
+
+def _frame_errors(R, O):
+    """Max |reference - oracle| of positions and temperatures, particles matched by track id."""
+    ir, xr = _by_id(R, "positions")
+    io, xo = _by_id(O, "positions")
+    assert np.array_equal(ir, io)
+    _, tr = _by_id(R, "T")
+    _, to = _by_id(O, "T")
+    return float(np.abs(xr - xo).max()), float(np.abs(tr - to).max())
+
+
 @need_ref
-def test_fast_math_reference_within_tolerance(cuda):
-    """Eight substeps of the README-shaped small scene through the unmodified
-    snow_simulation (fast math).  Water, whose arithmetic differs only by fast math,
-    agrees to 1e-5 m; snow positions differ by the link topology (bound 2e-3 m, the same
-    order as the FP32-vs-FP64 gap of the oracle itself); temperatures to 1e-3 C."""
-    r, o = _pair(scene.config0(), "fast")
+def test_fast_math_reference_within_1e4_m_without_links(cuda):
+    """Eight frames (32 substeps) of config 0 through the unmodified snow_simulation as its
+    project builds it (fast math), against the FP32 oracle, with interlinks off: the link
+    topology (racy in the reference, Q10) then plays no part, and what is left is the
+    arithmetic.  Positions agree to 1e-4 m and temperatures to 1e-3 C every frame."""
+    w = scene.config0()
+    w.flags["use_interlink"] = False
+    r, o = _pair(w, "fast")
+    errs = []
     try:
-        for _ in range(8):
-            r.step()
-            o.step()
-        R = r.to_host()
+        for f in range(8):
+            for _ in range(4):
+                r.step()
+                o.step()
+            errs.append(_frame_errors(r.to_host(), o.w))
     finally:
         r.close()
-    assert (R.n_sph, R.n_dem) == (o.w.n_sph, o.w.n_dem)
-    ns, nd = R.n_sph, R.n_dem
-    dw = np.abs(R.sph["positions"][:ns] - o.w.sph["positions"][:ns]).max()
-    ds = np.abs(R.dem["positions"][:nd] - o.w.dem["positions"][:nd]).max()
-    dT = max(np.abs(R.sph["T"][:ns] - o.w.sph["T"][:ns]).max(), np.abs(R.dem["T"][:nd] - o.w.dem["T"][:nd]).max())
-    assert dw < 1e-5, dw
-    assert ds < 2e-3, ds
-    assert dT < 1e-3, dT
+    assert max(e[0] for e in errs) <= 1e-4, errs
+    assert max(e[1] for e in errs) <= 1e-3, errs
+
+
+@need_ref
+def test_fast_math_reference_link_topology_per_frame(cuda):
+    """With interlinks on, the reference forms links with racing slot claims (Q10) and the
+    oracle (bit-exact with the CUDA path) in one deterministic order, so the topologies
+    differ; per frame over eight frames of config 0 the pair sets overlap with Jaccard
+    >= 0.7, and the positions stay within 2e-3 m (the snow moves with its links)."""
+    r, o = _pair(scene.config0(), "fast")
+    rows = []
+    try:
+        for f in range(8):
+            for _ in range(4):
+                r.step()
+                o.step()
+            R = r.to_host()
+            a, _ = link_pairs(o.w)
+            b, _ = link_pairs(R)
+            jac = len(a & b) / max(1, len(a | b))
+            rows.append((f, round(jac, 4), len(a), len(b)) + _frame_errors(R, o.w))
+    finally:
+        r.close()
+    print("frame, Jaccard, oracle pairs, reference pairs, pos err m, T err C:", rows)
+    assert all(x[1] >= 0.7 for x in rows), rows
+    assert max(x[4] for x in rows) <= 2e-3, rows
