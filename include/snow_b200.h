@@ -412,8 +412,11 @@ int snowb_read_sizes(uint32_t* sph_size, uint32_t* dem_size);
 /* Device counters of the last substep, in this order: n_sph, n_dem, n_boundary, sizes at
  * substep start (2), particles freezing, melting, phase-change flag, sizes after compaction
  * (2), device error bits, tail-dirty flag, particles kept by the link prefilter, links added,
- * neighbour lists that overflowed in the substep's density+lambda passes.
- * Copies min(n, 16) values into out (blocks). */
+ * neighbour lists that overflowed in the substep's density+lambda passes, (index 15 unused),
+ * then for the water and the snow set: the pending full-sort flags (2), the last sort
+ * decisions (2), and since the call started the sort points that sorted in full (2) and
+ * those that kept the previous sort because no particle had left its cell (2).
+ * Copies min(n, 24) values into out (blocks). */
 int snowb_device_counters(uint32_t* out, int n);
 
 /* Default quirk mode of snowb_snow_simulation (SNOWB_QUIRKS_REFERENCE initially). */

@@ -6,7 +6,8 @@
 # and linked, with no undefined symbol left, against libsnowb200.so and the reference's
 # Particle/Collider sources (ParticleSet::setSize and its constructors); then
 # shim_caller.cpp, which calls every entry point through the reference's declarations, is
-# linked against it with no undefined symbol left.  Outputs go to
+# linked against it with no undefined symbol left; last, the C++ host driver
+# snowsimulation_b200/shim/snow_host.cpp is built on the same objects.  Outputs go to
 # oracle/_ref/shim/ only.  Where the reference sources are absent the script skips.
 # Shims, as in cpu_ref_build.sh: GL scalar typedefs, std::floorf, MSVC's __forceinline.
 set -e
@@ -44,4 +45,10 @@ g++ -shared -Wl,--no-undefined -o "$OUT/libshimcheck.so" "$OUT/shim.o" "${OBJS[@
 g++ "${FLAGS[@]}" -c "$HERE/shim_caller.cpp" -o "$OUT/caller.o"
 g++ -shared -Wl,--no-undefined -o "$OUT/libshimcaller.so" "$OUT/caller.o" -L"$OUT" -lshimcheck \
     -L"$ROOT/snowsimulation_b200" -lsnowb200 -L"$CUDA/lib64" -lcudart
-echo "shim ok: $OUT/libshimcheck.so"
+# the C++ host driver (snowsimulation_b200/shim/snow_host.cpp): the reference's host call
+# sequence on the reference's types, linked with the shim in place of cuda_simulation.cu
+g++ "${FLAGS[@]}" -c "$ROOT/snowsimulation_b200/shim/snow_host.cpp" -o "$OUT/snow_host.o"
+g++ -o "$OUT/snow_host" "$OUT/snow_host.o" "$OUT/shim.o" "${OBJS[@]}" \
+    -L"$ROOT/snowsimulation_b200" -lsnowb200 -L"$CUDA/lib64" -lcudart \
+    -Wl,-rpath,'$ORIGIN/../../../snowsimulation_b200' -Wl,-rpath,"$CUDA/lib64"
+echo "shim ok: $OUT/libshimcheck.so $OUT/snow_host"

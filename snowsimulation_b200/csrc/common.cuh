@@ -53,6 +53,12 @@ struct DevState {
     uint32_t n_links;               // links added by the last link pass
     uint32_t n_nl_ovf;              // neighbour lists that overflowed in the last density+lambda pass
     uint32_t pad;
+    // Sort skipping.  moved[k]: set k must be sorted in full at its next sort point (a
+    // particle's cell differs from its key at the set's last sort, the set was compacted, or
+    // a call started).  resort[k]: the decision of the current sort point, taken from moved
+    // by k_sort_gate.  sorts_full/sorts_kept count the decisions since the call started.
+    uint32_t moved[2], resort[2];
+    uint32_t sorts_full[2], sorts_kept[2];
 };
 #define SNOWB_DEVERR_SCATTER 1u
 #define SNOWB_DEVERR_SCENE 2u      // a batched scene id >= the scene count

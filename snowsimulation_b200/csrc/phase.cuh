@@ -184,7 +184,10 @@ __global__ void k_compact_finish(DevParams P, DevState* S, snowb_particle_data s
 }
 __global__ void k_commit_sizes(DevState* S)
 {
-    if (blockIdx.x == 0 && threadIdx.x == 0 && S->changed) { S->n_sph = S->new_sph; S->n_dem = S->new_dem; }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && S->changed) {
+        S->n_sph = S->new_sph; S->n_dem = S->new_dem;
+        S->moved[0] = 1u; S->moved[1] = 1u;   // compacted sets: sort both in full
+    }
 }
 __global__ void k_clear_tail_flag(DevState* S)
 {

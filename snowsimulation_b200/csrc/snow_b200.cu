@@ -126,6 +126,7 @@ struct SetBufs {
     float4* p4 = nullptr;
     float *invm = nullptr, *contrib = nullptr, *lambda = nullptr, *mass = nullptr;
     uint32_t* sid = nullptr;   // scene id per sorted particle (batched runs)
+    uint32_t* inv = nullptr;   // sorted index per original index (last sort)
 };
 
 struct Ctx {
@@ -154,7 +155,7 @@ static uint64_t g_ctx_gen = 0;   // bumped whenever the scratch buffers are (re)
 static void free_set(SetBufs& s)
 {
     void* ptrs[] = {s.key, s.slot, s.tmp, s.cnt, s.off, s.bsum, s.val, s.p4, s.invm, s.contrib, s.lambda, s.mass,
-                    s.sid};
+                    s.sid, s.inv};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     s = SetBufs();
@@ -183,7 +184,7 @@ static int alloc_sort(SetBufs& s, uint32_t cap, uint32_t ncells, bool attrs)
     CUDA_TRY(cudaMemset(s.bsum, 0, sizeof(uint32_t) * (ncells / SCAN_CHUNK + 2)));
     if (attrs) {
         TRY(dalloc(&s.p4, cap)); TRY(dalloc(&s.invm, cap)); TRY(dalloc(&s.contrib, cap)); TRY(dalloc(&s.lambda, cap));
-        TRY(dalloc(&s.sid, cap));
+        TRY(dalloc(&s.sid, cap)); TRY(dalloc(&s.inv, cap));
     }
     return SNOWB_OK;
 }
@@ -387,7 +388,7 @@ static int sort_set(const DevParams& P, SetBufs& B, const snowb_particle_data& D
     KL(k_cell_scan, nb, SCAN_TPB, B.cnt, B.bsum, nc, B.off, cd.cell_start, n_ptr, 0u, clear_all ? 1 : 0, cond);
     LAUNCH(k_scatter, cap, 256, B.key, B.slot, B.off, B.tmp, n_ptr, 0u, cond, B.bsum, nb);
     LAUNCH(k_rank_reorder, cap, 256, B.key, B.off, B.tmp, D.predict_positions, D.mass, D.massInv, D.contrib, cd, B.p4,
-           B.invm, B.contrib, n_ptr, 0u, cond, sid_o, sid_o ? B.sid : nullptr);
+           B.invm, B.contrib, n_ptr, 0u, cond, sid_o, sid_o ? B.sid : nullptr, B.inv);
     return SNOWB_OK;
 }
 
@@ -551,36 +552,53 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
     const uint32_t* n_s = &S->n_sph;
     const uint32_t* n_d = &S->n_dem;
     const uint32_t work3 = 2 * full + a.nb;
+    // dirty_*: the host knows the set may have moved since its last sort (no launch at all
+    // otherwise).  On the device, k_sort_gate turns the writers' moved flags into the sort
+    // point's decision: a set whose particles all kept their cells keeps its sort outputs
+    // (the writers updated its sorted copies) and its sort launches return at once.
     bool dirty_s = true, dirty_d = true;
-    auto sort_if = [&](int set, const uint32_t* cond) -> int {
-        bool& dirty = set ? dirty_d : dirty_s;
-        if (!dirty && !cond) return SNOWB_OK;
-        TRY(sort_set(P, c.s[set], set ? *a.dem : *a.sph, set ? a.dcd : a.scd, set ? n_d : n_s, cap, cond,
+    auto track = [&](int set) {
+        SetBufs& B = c.s[set];
+        return SortTrack{B.key, B.inv, B.p4, B.contrib, (set ? a.dcd : a.scd).sorted_pos,
+                         set ? a.sid_dem : a.sid_sph, &S->moved[set]};
+    };
+    const SortTrack track_s = track(0), track_d = track(1);
+    auto sort_if = [&](int set) -> int {
+        TRY(sort_set(P, c.s[set], set ? *a.dem : *a.sph, set ? a.dcd : a.scd, set ? n_d : n_s, cap, &S->resort[set],
                      !ref, set ? a.sid_dem : a.sid_sph));
-        if (!cond) dirty = false;
         return SNOWB_OK;
     };
     // The two sets' sorts share no buffer: the water sort runs on a side stream beside the
     // snow sort (a fork and a join of the captured graph), so the small set's chain of
-    // latency-bound launches overlaps the large one's.
-    auto sort_pair = [&](const uint32_t* cond) -> int {
+    // latency-bound launches overlaps the large one's.  after_phase: the sort point after
+    // the phase change, where only a compaction (which marks both sets moved) alters the
+    // result.
+    auto sort_pair = [&](bool after_phase) -> int {
+        const bool need_s = dirty_s || after_phase, need_d = dirty_d || after_phase;
+        if (!need_s && !need_d) return SNOWB_OK;
+        LAUNCH1(k_sort_gate, S, (need_s ? 1u : 0u) | (need_d ? 2u : 0u));
         const cudaStream_t main_stream = g_stream;
-        CUDA_TRY(cudaEventRecord(c.fork, main_stream));
-        CUDA_TRY(cudaStreamWaitEvent(c.side, c.fork, 0));
-        g_stream = c.side;
-        const int rc = sort_if(0, cond);
-        g_stream = main_stream;
-        TRY(rc);
-        TRY(sort_if(1, cond));
-        CUDA_TRY(cudaEventRecord(c.join, c.side));
-        CUDA_TRY(cudaStreamWaitEvent(main_stream, c.join, 0));
+        if (need_s) {
+            CUDA_TRY(cudaEventRecord(c.fork, main_stream));
+            CUDA_TRY(cudaStreamWaitEvent(c.side, c.fork, 0));
+            g_stream = c.side;
+            const int rc = sort_if(0);
+            g_stream = main_stream;
+            TRY(rc);
+        }
+        if (need_d) TRY(sort_if(1));
+        if (need_s) {
+            CUDA_TRY(cudaEventRecord(c.join, c.side));
+            CUDA_TRY(cudaStreamWaitEvent(main_stream, c.join, 0));
+        }
+        dirty_s = dirty_d = false;
         return SNOWB_OK;
     };
 #define STOP(k) do { if (a.stop_after == (k)) return SNOWB_OK; } while (0)
 
     TAPE_HOOK(0, 0);
     LAUNCH1(k_begin_substep, S);
-    TRY(sort_pair(nullptr));
+    TRY(sort_pair(false));
     STOP(1);
     TLAUNCH(k_density<false>, 256, work3, 128, P, S, vs, vd, vb, X, ss, sd, sb, NL);
     STOP(2);
@@ -612,7 +630,7 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
     }
     STOP(4);
     if (a.change_phase) {   // the reference sorts again; only a phase change alters the result
-        TRY(sort_pair(&S->changed));
+        TRY(sort_pair(true));
     }
     STOP(5);
     if (a.interlink) {
@@ -630,7 +648,8 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
     }
     STOP(6);
     if (step_sph || step_dem) {
-        LAUNCH(k_integrate, 2 * full, 256, P, S, X, full, a.dt, a.cd_on, step_sph ? 1 : 0, step_dem ? 1 : 0);
+        LAUNCH(k_integrate, 2 * full, 256, P, S, X, full, a.dt, a.cd_on, step_sph ? 1 : 0, step_dem ? 1 : 0, track_s,
+               track_d);
         if (step_sph) dirty_s = true;
         if (step_dem) dirty_d = true;
     }
@@ -638,7 +657,7 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
     STOP(7);
     for (int it = 0; it < a.iterations; ++it) {
         const int base = 10 + 10 * it;
-        TRY(sort_pair(nullptr));
+        TRY(sort_pair(false));
         TAPE_HOOK(2, it);
         STOP(base + 0);
         // density + lambda in one pass (stage boundaries base+1 and base+2 coincide)
@@ -653,16 +672,17 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
         if (a.interlink) TLAUNCH(k_interlink, 1024, full, 128, P, S, *a.dem);
         STOP(base + 5);
         if (step_sph || step_dem) {
-            TLAUNCH(k_apply, 1024, 2 * full, 256, P, S, vs, vd, X, step_sph ? 1 : 0, step_dem ? 1 : 0);
+            TLAUNCH(k_apply, 1024, 2 * full, 256, P, S, vs, vd, X, step_sph ? 1 : 0, step_dem ? 1 : 0, track_s,
+                    track_d);
             if (step_sph) dirty_s = true;
             if (step_dem) dirty_d = true;
         }
         TAPE_HOOK(3, it);
         STOP(base + 6);
         if (a.friction && step_dem) {
-            TRY(sort_pair(nullptr));
+            TRY(sort_pair(false));
             TLAUNCH(k_friction, 256, full, 128, P, S, vd, vb, X, sd, sb);
-            TLAUNCH(k_apply, 1024, full, 256, P, S, vs, vd, X, 0, 1);
+            TLAUNCH(k_apply, 1024, full, 256, P, S, vs, vd, X, 0, 1, track_s, track_d);
             dirty_d = true;
         }
         STOP(base + 7);
@@ -1421,7 +1441,7 @@ int snowb_integrate_pbd(snowb_particle_data* particles, float dt, uint32_t n, in
     P.quirks = SNOWB_QUIRKS_FIXED;   // exactly n particles (the caller owns the launch size)
     LAUNCH1(k_set_state, g_ctx.S, n, 0u, 0u);
     Sets X{*particles, *particles, *particles};
-    LAUNCH(k_integrate, n, 256, P, g_ctx.S, X, n, dt, cd_on, 1, 0);
+    LAUNCH(k_integrate, n, 256, P, g_ctx.S, X, n, dt, cd_on, 1, 0, SortTrack{}, SortTrack{});
     return SNOWB_OK;
 }
 

@@ -9,6 +9,7 @@
 // d < 2r, d <= 2r) because sqrt is correctly rounded and monotone.
 #pragma once
 #include "common.cuh"
+#include "sort.cuh"
 
 namespace snowb {
 
@@ -575,28 +576,6 @@ __device__ __forceinline__ void delete_record(const snowb_particle_data& D, uint
     for (uint32_t s = i1 * M; s < (i1 + 1) * M; ++s)
         if (atomicCAS(D.connect_record + s, i0, SNOWB_UMAX) == i0) { atomicExch(D.connect_length + s, 0.f); break; }
 }
-// compute_interlink_correction (:4661-4739).  Both ends of a link hold the same length
-// and see the same distance, so whichever end breaks it first, neither adds a correction.
-__device__ __forceinline__ float3 link_corr(const DevParams& P, const snowb_particle_data& D, uint32_t i0,
-                                            uint32_t i1, float L, uint32_t n)
-{
-    const float3 z = f3(0.f, 0.f, 0.f);
-    if (i0 == i1 || i0 >= n || i1 >= n || L == 0.f) return z;
-    float3 v = sub3(ldv3(D.predict_positions, i0), ldv3(D.predict_positions, i1));
-    float dist = len3(v);
-    if (dist > P.brk * L) { delete_record(D, P.maxc, i0, i1); return z; }
-    if (dist > P.h) { delete_record(D, P.maxc, i0, i1); return z; }
-    float w0 = D.massInv[i0], w1 = D.massInv[i1];
-    float ws = w0 + w1, C = dist - L;
-    float3 n3 = div3(v, dist + P.pbd_eps);
-    float3 r = sc3(((P.k_ref * -w0) * (1.f / ws)) * C, n3);
-    // len3(r) > 1 without the square root: sqrtf is monotone and correctly rounded, and the
-    // smallest float whose root rounds above 1 is 1 + 2^-22, so the test is d2 > 1 + 2^-23
-    if (dot3(r, r) > 0x1.000002p+0f) return z;
-    if (nan3(r)) return z;
-    if (inf3(r)) return z;
-    return r;
-}
 // compute_dem_sph_distance_correction (:2112-2162) and compute_dem_distance_correction
 // (:1765-1834) for snow particle o, added to its correction in the reference's kernel
 // order (after the PBF pass; the interlink terms of k_interlink follow).
@@ -634,10 +613,16 @@ __global__ void __launch_bounds__(256) k_dem_corr(DevParams P, const DevState* _
     }
     (void)ns; (void)nb;
 }
-// solve_snow_interlink_constraint_d (:4742-4765), one thread per snow particle in original
-// order (consecutive threads read consecutive slot blocks; linked partners are near in
-// index), added to the correction after the contact terms as in the reference.
-__global__ void k_interlink(DevParams P, const DevState* __restrict__ S, snowb_particle_data dem)
+// solve_snow_interlink_constraint_d (:4742-4765) with compute_interlink_correction
+// (:4661-4739) per filled slot, one thread per snow particle in original order (consecutive
+// threads read consecutive slot blocks; linked partners are near in index), added to the
+// correction after the contact terms as in the reference, over the filled slots in slot
+// order.  Both ends of a link hold the same length and see the same distance, so whichever end breaks it first (delete_record),
+// neither adds a correction.  The particle's own position, inverse mass and k_ref * -w0 are
+// loaded once, and 1 / (w0 + w1) is kept while the partner's inverse mass repeats (the same
+// operands give the same quotient); every other operation is the reference's, in its order.
+__global__ void __launch_bounds__(256) k_interlink(DevParams P, const DevState* __restrict__ S,
+                                                   snowb_particle_data dem)
 {
     const uint32_t nd = S->n_dem, M = P.maxc;
     const float3 z = f3(0.f, 0.f, 0.f);
@@ -647,10 +632,47 @@ __global__ void k_interlink(DevParams P, const DevState* __restrict__ S, snowb_p
     const uint32_t* rec = dem.connect_record;
     const float* len = dem.connect_length;
     GRID_LOOP(o, nd) {
+        const float3 p0 = ldv3(dem.predict_positions, o);
+        const float w0 = dem.massInv[o];
+        const float kw0 = P.k_ref * -w0;
+        uint32_t w1_last = 0u;     // bits of the partner inverse mass inv_ws was taken for
+        float inv_ws = 0.f;
+        bool have_ws = false;
         float3 d = z;
-        for (uint32_t s = M * o; s < M * (o + 1); ++s) {
-            const uint32_t j = rec[s];
-            if (j != SNOWB_UMAX) d = add3(d, link_corr(P, dem, o, j, len[s], nd));
+        const uint32_t end = M * (o + 1);
+        // each lane steps to its own next filled slot, so one pass of the loop body serves
+        // every lane that still has a link (an empty slot adds nothing)
+        for (uint32_t s = M * o;; ++s) {
+            uint32_t j = SNOWB_UMAX;
+            for (; s < end; ++s) {
+                j = rec[s];
+                if (j != SNOWB_UMAX) break;
+            }
+            if (s >= end) break;
+            const float L = len[s];
+            float3 r = z;
+            if (!(o == j || j >= nd || L == 0.f)) {
+                const float3 v = sub3(p0, ldv3(dem.predict_positions, j));
+                const float dist = len3(v);
+                if (dist > P.brk * L || dist > P.h) {
+                    delete_record(dem, M, o, j);
+                } else {
+                    const float w1 = dem.massInv[j];
+                    if (!have_ws || __float_as_uint(w1) != w1_last) {
+                        inv_ws = 1.f / (w0 + w1);
+                        w1_last = __float_as_uint(w1);
+                        have_ws = true;
+                    }
+                    const float C = dist - L;
+                    const float3 n3 = div3(v, dist + P.pbd_eps);
+                    const float3 t = sc3((kw0 * inv_ws) * C, n3);
+                    // len3(t) > 1 without the square root: sqrtf is monotone and correctly
+                    // rounded, and the smallest float whose root rounds above 1 is 1 + 2^-22,
+                    // so the test is d2 > 1 + 2^-23
+                    if (!(dot3(t, t) > 0x1.000002p+0f) && !nan3(t) && !inf3(t)) r = t;
+                }
+            }
+            d = add3(d, r);
         }
         if (nan3(d)) d = z;
         st3(dem.correction, o, add3(ldv3(dem.correction, o), d));
@@ -663,8 +685,10 @@ __device__ __forceinline__ uint32_t launch_limit(const DevParams& P, uint32_t n0
 {
     return P.quirks == SNOWB_QUIRKS_REFERENCE ? umin32(coverage(n0), n) : n;
 }
+// The sorted copies of the moved set (ts, td: key null when not tracked) follow the new
+// positions, so a later sort of a set whose particles kept their cells has nothing to do.
 __global__ void k_apply(DevParams P, const DevState* __restrict__ S, SetView vs, SetView vd, Sets X, int do_sph,
-                        int do_dem)
+                        int do_dem, SortTrack ts, SortTrack td)
 {
     const uint32_t ls = do_sph ? launch_limit(P, S->n0_sph, S->n_sph) : 0u;
     const uint32_t ld = do_dem ? launch_limit(P, S->n0_dem, S->n_dem) : 0u;
@@ -674,10 +698,13 @@ __global__ void k_apply(DevParams P, const DevState* __restrict__ S, SetView vs,
         const SetView& v = w ? vs : vd;
         const snowb_particle_data& D = w ? X.sph : X.dem;
         const uint32_t o = v.gi[i];
-        float3 np = add3(xyz(v.p4[i]), sc3(P.sor, ldv3(D.correction, o)));
+        const float4 q = v.p4[i];
+        float3 np = add3(xyz(q), sc3(P.sor, ldv3(D.correction, o)));
         st3(D.new_positions, o, np);
         st3(D.predict_positions, o, np);
         st3(D.correction, o, f3(0.f, 0.f, 0.f));
+        const SortTrack& T = w ? ts : td;
+        if (T.key) track_move(P, T, o, i, np, v.scene(i), q.w);
     }
 }
 
@@ -895,15 +922,26 @@ __device__ __forceinline__ void integrate_one(const DevParams& P, const snowb_pa
     if (c >= 0.99f) c = 1.f;
     D.contrib[i] = c;
 }
+// ts, td: the sets' sorted copies, kept current for the particles of the last sort (i < n;
+// key null when not tracked)
 __global__ void k_integrate(DevParams P, const DevState* __restrict__ S, Sets X, uint32_t full, float dt, int cd_on,
-                            int do_sph, int do_dem)
+                            int do_sph, int do_dem, SortTrack ts, SortTrack td)
 {
     const bool ref = P.quirks == SNOWB_QUIRKS_REFERENCE;
-    const uint32_t ls = do_sph ? (ref ? umin32(coverage(S->n_sph), full) : S->n_sph) : 0u;
-    const uint32_t ld = do_dem ? (ref ? umin32(coverage(S->n_dem), full) : S->n_dem) : 0u;
+    const uint32_t ns = S->n_sph, nd = S->n_dem;
+    const uint32_t ls = do_sph ? (ref ? umin32(coverage(ns), full) : ns) : 0u;
+    const uint32_t ld = do_dem ? (ref ? umin32(coverage(nd), full) : nd) : 0u;
     GRID_LOOP(t, ls + ld) {
-        if (t < ls) integrate_one(P, X.sph, t, dt, cd_on);
-        else integrate_one(P, X.dem, t - ls, dt, cd_on);
+        const bool w = t < ls;
+        const uint32_t i = w ? t : t - ls;
+        const snowb_particle_data& D = w ? X.sph : X.dem;
+        integrate_one(P, D, i, dt, cd_on);
+        const SortTrack& T = w ? ts : td;
+        if (T.key && i < (w ? ns : nd)) {
+            const uint32_t p = __ldg(T.inv + i);
+            track_move(P, T, i, p, ldv3(D.predict_positions, i), T.sid ? __ldg(T.sid + i) : 0u, D.mass[i]);
+            T.contrib_s[p] = D.contrib[i];
+        }
     }
 }
 
@@ -1189,6 +1227,8 @@ __global__ void k_set_state(DevState* S, uint32_t ns, uint32_t nd, uint32_t nb)
         // the caller may have changed the tail slots between calls: the first compaction
         // of a call cleans the tail as the reference's does every substep
         S->tail_dirty = 1u;
+        // ... and the particles: the first sort point of a call sorts both sets in full
+        for (int k = 0; k < 2; ++k) { S->moved[k] = 1u; S->sorts_full[k] = 0u; S->sorts_kept[k] = 0u; }
     }
 }
 // batched runs: every live slot's scene id must name a scene of the batch

@@ -198,7 +198,8 @@ __global__ void k_rank_reorder(const uint32_t* __restrict__ key_o, const uint32_
                                const float* __restrict__ contrib, snowb_cell_data cd, float4* __restrict__ p4,
                                float* __restrict__ invm_s, float* __restrict__ contrib_s,
                                const uint32_t* n_ptr, uint32_t n_fixed, const uint32_t* cond,
-                               const uint32_t* __restrict__ sid_o, uint32_t* __restrict__ sid_s)
+                               const uint32_t* __restrict__ sid_o, uint32_t* __restrict__ sid_s,
+                               uint32_t* __restrict__ inv_o = nullptr)
 {
     if (cond && *cond == 0) return;
     const uint32_t n = n_ptr ? *n_ptr : n_fixed;
@@ -206,6 +207,7 @@ __global__ void k_rank_reorder(const uint32_t* __restrict__ key_o, const uint32_
         const uint32_t h = key_o[o], b = off[h], e = off[h + 1];
         const uint32_t r = stable_rank(tmp, b, e, o);
         const uint32_t p = b + r;
+        if (inv_o) inv_o[o] = p;
         cd.grid_index[p] = o;
         cd.grid_hash[p] = h;
         if (r == 0) { cd.cell_start[h] = b; cd.cell_end[h] = e; }
@@ -217,6 +219,45 @@ __global__ void k_rank_reorder(const uint32_t* __restrict__ key_o, const uint32_
         if (sid_s) sid_s[p] = sid_o[o];
     }
 }
+// Decision of one sort point for the sets in `sets` (bit k: set k is sorted here): a set
+// whose particles all kept their cells since its last sort (moved[k] clear) keeps its sort
+// outputs, which the position writers have kept current (SortTrack), so its sort launches
+// return at once.  moved[k] is consumed; the writers set it again.
+__global__ void k_sort_gate(DevState* S, uint32_t sets)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        for (int k = 0; k < 2; ++k)
+            if ((sets >> k) & 1u) {
+                const uint32_t m = S->moved[k];
+                S->resort[k] = m;
+                S->moved[k] = 0u;
+                if (m) ++S->sorts_full[k];
+                else ++S->sorts_kept[k];
+            }
+}
+
+// The sorted copies of a set, kept current by the kernels that move its particles while
+// no particle leaves its cell; a particle whose cell changed marks the set for a full sort.
+struct SortTrack {
+    const uint32_t* key;        // cell key per original index at the set's last sort (null: no tracking)
+    const uint32_t* inv;        // sorted index per original index at the set's last sort
+    float4* p4;                 // sorted (x, y, z, mass)
+    float* contrib_s;           // sorted contrib
+    snowb_float3* sorted_pos;   // the caller's CellData::sorted_pos
+    const uint32_t* sid;        // scene id per original index (batched runs) or null
+    uint32_t* moved;            // &DevState::moved[set]
+};
+// a particle moved to predicted position q: keep the sorted copies (sorted index p) or mark
+// the set when its cell changed
+__device__ __forceinline__ void track_move(const DevParams& P, const SortTrack& T, uint32_t o, uint32_t p, float3 q,
+                                           uint32_t scene, float w)
+{
+    const uint32_t h = grid_hash(P, grid_pos(P, q, scene), 0, 0, 0);
+    if (h != __ldg(T.key + o)) *T.moved = 1u;
+    T.p4[p] = make_float4(q.x, q.y, q.z, w);
+    st3(T.sorted_pos, p, q);
+}
+
 // sort_particles path: write the sorted keys and values only.
 __global__ void k_rank_pairs(const uint32_t* __restrict__ key_o, const uint32_t* __restrict__ val_o,
                              const uint32_t* __restrict__ off, const uint32_t* __restrict__ tmp,

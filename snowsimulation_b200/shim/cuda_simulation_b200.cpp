@@ -46,6 +46,12 @@ void snow_simulation(ParticleSet* sph, ParticleSet* dem, ParticleSet* b, Particl
     dem->setSize(nd);
 }
 
+// connect_and_record (cuda_simulation.cu:4286-4292; defined there with C++ linkage, not
+// declared in cuda_simulation.cuh): interlink formation over the sorted snow set.
+void connect_and_record(ParticleSet* dem, CellData dcd, bool dynamic) {
+    check(snowb_connect_and_record(pd(dem), (uint32_t)dem->m_size, cd(dcd), dynamic));
+}
+
 // cuda_tool.cu:3-13: d_arr[start, end) = value.  Called by ParticleSystem's set-up only, so
 // one synchronous copy of a host buffer, after the library's stream has drained.
 template <class T>

@@ -30,3 +30,17 @@ def test_bgeo_plain_int_label_and_empty(tmp_path):
     export.write_host(path, np.zeros((0, 3), np.float32), export.WATER_RGB, 0.01, 0)
     b = export.read_bgeo(path)
     assert b["n_points"] == 0 and b["trailer"] == b"\x00\xff"
+
+
+def test_host_driver_scene_file_round_trip(tmp_path):
+    """The C++ host driver's scene file holds a HostWorld exactly (no GPU involved)."""
+    from snowsimulation_b200 import scene
+    from snowsimulation_b200.host_io import read_world, write_world
+    from tests._util import diff_worlds
+    w = scene.tiny(seed=2, init_links=True)
+    w.scene = [0.0, 0.5, 0.125]
+    p = str(tmp_path / "w.bin")
+    write_world(p, w)
+    r = read_world(p, w)
+    assert not diff_worlds(w, r)
+    assert r.scene == w.scene and bytes(r.params) == bytes(w.params)
