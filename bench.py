@@ -14,10 +14,15 @@ the slowest rank's time.
 
 The line also carries "batched": 64 scenes of uneven size (log-uniform 2k-40k particles)
 stepped as one batch, against the same scenes stepped one after another through the
-plain entry point (--no-batched skips it), and "adjoint": a differentiable rollout of
-config 3 (40 substeps, forward with checkpoints + backward) against the same substeps run
-plain (--no-adjoint skips it), and "large": 3 frames of the 1.18M-particle config 4 in a
-widened domain (--no-large skips it).
+plain entry point (--no-batched skips it); "adjoint": a differentiable rollout of config 3
+to frame 60 (240 substeps, forward with checkpoints every 10 + backward) against the same
+substeps run plain (--no-adjoint skips it); "large": 3 frames of the 1.18M-particle
+config 4 in a widened domain (--no-large skips it); "long_window": every frame 0-99 of the
+scene from rest (--long-frames); "fp64_error": the first 24 frames against the FP64 oracle
+with the heat-energy drift of both runs (--fp64-frames, --no-fp64).
+
+--precision-study runs the config-4 precision study instead (FP64 oracle comparison of the
+first frames, GPU heat-energy drift over 600 frames, per-kernel HBM fractions).
 
 --impl reference times the CPU restatement of the same substep (FP32, all host threads) on
 the same frames of the same scene (W warm-up frames, K timed frames of 4 substeps), the
@@ -54,6 +59,10 @@ def parse():
     ap.add_argument("--no-large", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--fp64-frames", type=int, default=24)
+    ap.add_argument("--long-frames", type=int, default=100)
+    ap.add_argument("--precision-study", action="store_true")
+    ap.add_argument("--precision-fp64-frames", type=int, default=10)
+    ap.add_argument("--precision-energy-frames", type=int, default=600)
     ap.add_argument("--profile-out", default="")
     return ap.parse_args()
 
@@ -441,6 +450,122 @@ def large_scene(frames, dev, seed, flush, warmup=2):
     return res
 
 
+# ----------------------------------------------------------------- long window
+def long_window(frames, dev, seed, flush, scene_name="config1"):
+    """Device time of every frame 0..frames-1 of the scene from rest (graph replay, L2
+    flushed before each frame outside the events): the mean over the whole window and per
+    20-frame span, where the cost changes as the water melts into the snow."""
+    import torch
+    from snowsimulation_b200 import scene
+    from snowsimulation_b200.world import Simulation
+    w = getattr(scene, scene_name)(seed=seed)
+    sim = Simulation(w, device=dev).setup()
+    stream = torch.cuda.current_stream(dev)
+    ms = []
+    for _ in range(frames):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        sim.step(substeps=SUBSTEPS, sync=False, use_graph=True)
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        ms.append(a.elapsed_time(b))
+    sim.read_sizes()
+    n = w.n_sph + w.n_dem
+    spans = {"%d-%d" % (k, min(k + 19, frames - 1)): sum(ms[k:k + 20]) / len(ms[k:k + 20]) for k in range(0, frames, 20)}
+    res = {"workload": "%s from rest, frames 0-%d, 1 frame = %d substeps" % (scene_name, frames - 1, SUBSTEPS),
+           "ms_per_frame_mean": sum(ms) / frames, "value": n * SUBSTEPS * frames / (sum(ms) / 1000.0),
+           "unit": UNIT, "ms_per_frame_by_span": spans, "sizes_after": [sim.n_sph, sim.n_dem],
+           "note": "the frame-0 graph capture happens before the first timed event"}
+    del sim
+    torch.cuda.empty_cache()
+    return res
+
+
+# ----------------------------------------------------------------- precision study (config 4)
+def precision_study(dev, fp64_frames=10, energy_frames=600, profile_frames=2):
+    """The large scene (1,048,576 snow + 131,072 water, 128^3 grid, walls at +-1.5 m) from
+    rest: (1) the FP32 GPU run against the FP64 oracle run of the same scene, frame by frame
+    for `fp64_frames` frames (particles matched by track id): position, velocity and
+    temperature errors and both runs' heat energy; (2) the GPU run continued to
+    `energy_frames` frames with its FP64 heat-energy and momentum reductions every 10
+    frames (drift from the start); (3) the per-kernel device time over `profile_frames`
+    frames (CUDA-event nodes in the substep graph) against the algorithmic bytes of each
+    kernel: achieved GB/s and fraction of the measured HBM peak."""
+    import numpy as np
+    import torch
+    from snowsimulation_b200 import scene, bytes_model, _native
+    from snowsimulation_b200.world import Simulation
+    from oracle.oracle import OracleWorld
+    w = scene.config4(seed=0)
+    sim = Simulation(w, device=dev).setup()
+    t0 = time.perf_counter()
+    o = OracleWorld(w, 64, threads=os.cpu_count() or 1).setup()
+
+    def by_id(sets):
+        ids = np.concatenate([d["trackId"][:n] for d, n in sets])
+        order = np.argsort(ids)
+        cat = lambda f: np.concatenate([d[f][:n] for d, n in sets])[order].astype(np.float64)
+        return ids[order], cat("positions"), cat("velocity"), cat("T")
+
+    e0g, e0o = sim.energy_momentum(), o.energy_momentum()
+    rows = []
+    for f in range(fp64_frames):
+        sim.step(substeps=SUBSTEPS)
+        for _ in range(SUBSTEPS):
+            o.step()
+        H = sim.to_host()
+        ig, xg, vg, tg = by_id(((H.sph, H.n_sph), (H.dem, H.n_dem)))
+        io, xo, vo, to = by_id(((o.w.sph, o.w.n_sph), (o.w.dem, o.w.n_dem)))
+        eg, eo = sim.energy_momentum(), o.energy_momentum()
+        r = {"frame": f, "sizes": [H.n_sph, H.n_dem], "sizes_fp64": [o.w.n_sph, o.w.n_dem],
+             "energy_drift_rel": (eg[0] - e0g[0]) / abs(e0g[0]), "energy_drift_fp64_rel": (eo[0] - e0o[0]) / abs(e0o[0])}
+        if np.array_equal(ig, io):
+            r.update(pos_max_m=float(np.abs(xg - xo).max()), vel_max_mps=float(np.abs(vg - vo).max()),
+                     T_max_C=float(np.abs(tg - to).max()))
+        rows.append(r)
+        print("precision frame %d: %s" % (f, json.dumps(r)), file=sys.stderr, flush=True)
+    t_fp64 = time.perf_counter() - t0
+    del o
+    drift = []
+    for f in range(fp64_frames, energy_frames):
+        sim.step(substeps=SUBSTEPS, sync=False, use_graph=True)
+        if (f + 1) % 10 == 0 or f == energy_frames - 1:
+            sim.read_sizes()
+            e = sim.energy_momentum()
+            drift.append({"frame": f, "energy_drift_rel": (e[0] - e0g[0]) / abs(e0g[0]), "momentum": e[1:],
+                          "sizes": [sim.n_sph, sim.n_dem]})
+    # per-kernel table over the next frames
+    lib = sim.lib
+    lib.snowb_profile_begin()
+    for _ in range(profile_frames):
+        sim.step(substeps=SUBSTEPS, sync=False, use_graph=True)
+    buf = C.create_string_buffer(1 << 16)
+    _native.check(lib.snowb_profile_end(buf, len(buf)))
+    sim.read_sizes()
+    peak, peak_kind = peaks()
+    table = []
+    for line in buf.value.decode().splitlines():
+        nm, c, t = line.split()
+        c, t = int(c), float(t)
+        base = nm.split("<")[0]
+        kb = bytes_model.kernel_bytes(base, sim.n_sph, sim.n_dem, sim.n_b)
+        if kb is not None and base == "k_density" and "true" in nm:
+            kb += bytes_model.PASS["L"] * (sim.n_sph + sim.n_dem + sim.n_b)
+        row = {"kernel": nm, "launches_per_frame": c / profile_frames, "ms_per_frame": t / profile_frames}
+        if kb is not None:
+            gbs = kb * c / (t / 1000.0) / 1e9
+            row.update(algorithmic_bytes_per_launch=kb, achieved_GBs=gbs, hbm_frac=gbs / peak)
+        table.append(row)
+    table.sort(key=lambda r: -r["ms_per_frame"])
+    return {"workload": "config4: %d water + %d snow + %d boundary, 128^3 grid, walls +-1.5 m, from rest"
+                        % (w.n_sph, w.n_dem, w.n_b),
+            "fp64": {"frames": fp64_frames, "oracle": "FP64 C restatement, OpenMP %d threads, %.0f s"
+                                                      % (os.cpu_count() or 1, t_fp64), "per_frame": rows},
+            "energy": {"frames": energy_frames, "start_J": e0g[0], "every_10_frames": drift},
+            "kernels": {"frames": profile_frames, "peak_GBs": peak, "peak_kind": peak_kind, "table": table}}
+
+
 # ----------------------------------------------------------------- adjoint vs plain
 def adjoint_compare(substeps, dev, seed, checkpoint_every=10):
     """Config 3 (1,024 water on 8,192 snow with interlinks, phase change off): device time of
@@ -505,6 +630,12 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.precision_study:
+        import torch
+        dev = torch.device("cuda", 0)
+        torch.cuda.set_device(dev)
+        print(json.dumps(precision_study(dev, args.precision_fp64_frames, args.precision_energy_frames)))
+        return 0
     import torch
     import torch.distributed as dist
     from snowsimulation_b200 import scene, bytes_model, _native
@@ -692,9 +823,14 @@ def main():
             n = large_res["value"] * large_res["ms_per_step"] / 1000.0
             large_res["value"] = job_rate(n, ws, ms_max)
             large_res["ms_per_step"] = ms_max
+    long_res = long_window(args.long_frames, dev, rank, flush, args.scene) if args.long_frames > 0 else None
+    if long_res is not None and ws > 1:
+        ms_max = slowest([long_res["ms_per_frame_mean"]], ws, dev)[0]
+        long_res["value"] = job_rate(long_res["value"] * long_res["ms_per_frame_mean"] / 1000.0, ws, ms_max)
+        long_res["ms_per_frame_mean"] = ms_max
     adjoint_res = None
     if not args.no_adjoint:
-        adjoint_res = adjoint_compare(40, dev, rank)
+        adjoint_res = adjoint_compare(240, dev, rank)
 
     if rank != 0:
         if ws > 1:
@@ -728,6 +864,8 @@ def main():
         line["adjoint"] = adjoint_res
     if large_res is not None:
         line["large"] = large_res
+    if long_res is not None:
+        line["long_window"] = long_res
     if ws == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.scene)
         line["cpu_baseline"]["reference_cpu"] = reference_cpu_baselines(

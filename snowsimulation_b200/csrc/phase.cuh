@@ -60,23 +60,43 @@ __device__ __forceinline__ void reset_records(const snowb_particle_data& d, uint
     d.iter_end[t] = M * t;
 }
 
-// freeze / melt predicates (:4425, :4396)
-__global__ void k_phase_flags(DevParams P, const DevState* __restrict__ S, snowb_particle_data sph,
+// freeze / melt predicates (:4425, :4396); the particles changing phase are also counted
+// here (one atomic per warp and kind), so the decision below needs no scan
+__global__ void k_phase_flags(DevParams P, DevState* __restrict__ S, snowb_particle_data sph,
                               snowb_particle_data dem, int freeze, int melt, uint32_t* __restrict__ fl_s,
                               uint32_t* __restrict__ fl_d)
 {
     const uint32_t ns = S->n_sph, nd = S->n_dem;
+    const uint32_t lane = threadIdx.x & 31u;
     GRID_LOOP(t, ns + nd) {
-        if (t < ns) fl_s[t] = (freeze && sph.T[t] <= P.Tf && sph.contrib[t] >= 0.99f) ? 1u : 0u;
-        else {
+        bool f = false, m = false;
+        if (t < ns) {
+            f = freeze && sph.T[t] <= P.Tf && sph.contrib[t] >= 0.99f;
+            fl_s[t] = f ? 1u : 0u;
+        } else {
             const uint32_t i = t - ns;
-            fl_d[i] = (melt && dem.T[i] > P.Tf && dem.contrib[i] >= 0.99f) ? 1u : 0u;
+            m = melt && dem.T[i] > P.Tf && dem.contrib[i] >= 0.99f;
+            fl_d[i] = m ? 1u : 0u;
+        }
+        const uint32_t am = __activemask();
+        const uint32_t bf = __ballot_sync(am, f), bm = __ballot_sync(am, m);
+        if (lane == (uint32_t)(__ffs(am) - 1)) {
+            if (bf) atomicAdd(&S->n_freeze, (uint32_t)__popc(bf));
+            if (bm) atomicAdd(&S->n_melt, (uint32_t)__popc(bm));
         }
     }
 }
-__global__ void k_phase_count(DevState* S)
+// changed = some particle changes phase.  Without a change, and with a clean tail, the rest
+// of the phase-change chain (ranks, moves, compaction, record remap) leaves the state as it
+// is (the previous substep's compaction already wrote the same scan_index and predicates),
+// so a captured substep skips it: `use_h` writes that decision into the graph's IF node.
+__global__ void k_phase_count(DevState* S, cudaGraphConditionalHandle h, int use_h)
 {
-    if (blockIdx.x == 0 && threadIdx.x == 0) S->changed = (S->n_freeze + S->n_melt) != 0u;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        const uint32_t ch = (S->n_freeze + S->n_melt) != 0u;
+        S->changed = ch;
+        if (use_h) cudaGraphSetConditional(h, (ch || S->tail_dirty) ? 1u : 0u);
+    }
 }
 // freezing (:4416-4449) and melting (:4387-4414) with ranked targets
 // scene ids of batched runs travel with the particles (null pointers: one scene)

@@ -616,8 +616,7 @@ __global__ void __launch_bounds__(256) k_dem_corr(DevParams P, const DevState* _
 // solve_snow_interlink_constraint_d (:4742-4765) with compute_interlink_correction
 // (:4661-4739) per filled slot, one thread per snow particle in original order (consecutive
 // threads read consecutive slot blocks; linked partners are near in index), added to the
-// correction after the contact terms as in the reference, over the filled slots in slot
-// order.  Both ends of a link hold the same length and see the same distance, so whichever end breaks it first (delete_record),
+// correction after the contact terms as in the reference.  Both ends of a link hold the same length and see the same distance, so whichever end breaks it first (delete_record),
 // neither adds a correction.  The particle's own position, inverse mass and k_ref * -w0 are
 // loaded once, and 1 / (w0 + w1) is kept while the partner's inverse mass repeats (the same
 // operands give the same quotient); every other operation is the reference's, in its order.
@@ -639,16 +638,9 @@ __global__ void __launch_bounds__(256) k_interlink(DevParams P, const DevState* 
         float inv_ws = 0.f;
         bool have_ws = false;
         float3 d = z;
-        const uint32_t end = M * (o + 1);
-        // each lane steps to its own next filled slot, so one pass of the loop body serves
-        // every lane that still has a link (an empty slot adds nothing)
-        for (uint32_t s = M * o;; ++s) {
-            uint32_t j = SNOWB_UMAX;
-            for (; s < end; ++s) {
-                j = rec[s];
-                if (j != SNOWB_UMAX) break;
-            }
-            if (s >= end) break;
+        for (uint32_t s = M * o; s < M * (o + 1); ++s) {
+            const uint32_t j = rec[s];
+            if (j == SNOWB_UMAX) continue;   // an empty slot adds nothing
             const float L = len[s];
             float3 r = z;
             if (!(o == j || j >= nd || L == 0.f)) {
@@ -685,8 +677,8 @@ __device__ __forceinline__ uint32_t launch_limit(const DevParams& P, uint32_t n0
 {
     return P.quirks == SNOWB_QUIRKS_REFERENCE ? umin32(coverage(n0), n) : n;
 }
-// The sorted copies of the moved set (ts, td: key null when not tracked) follow the new
-// positions, so a later sort of a set whose particles kept their cells has nothing to do.
+// ts, td: a particle that leaves its cell marks its set for a full sort at the next sort
+// point (key null: not tracked).
 __global__ void k_apply(DevParams P, const DevState* __restrict__ S, SetView vs, SetView vd, Sets X, int do_sph,
                         int do_dem, SortTrack ts, SortTrack td)
 {
@@ -698,13 +690,12 @@ __global__ void k_apply(DevParams P, const DevState* __restrict__ S, SetView vs,
         const SetView& v = w ? vs : vd;
         const snowb_particle_data& D = w ? X.sph : X.dem;
         const uint32_t o = v.gi[i];
-        const float4 q = v.p4[i];
-        float3 np = add3(xyz(q), sc3(P.sor, ldv3(D.correction, o)));
+        float3 np = add3(xyz(v.p4[i]), sc3(P.sor, ldv3(D.correction, o)));
         st3(D.new_positions, o, np);
         st3(D.predict_positions, o, np);
         st3(D.correction, o, f3(0.f, 0.f, 0.f));
         const SortTrack& T = w ? ts : td;
-        if (T.key) track_move(P, T, o, i, np, v.scene(i), q.w);
+        if (T.key) track_move(P, T, o, np, v.scene(i));
     }
 }
 
@@ -922,8 +913,8 @@ __device__ __forceinline__ void integrate_one(const DevParams& P, const snowb_pa
     if (c >= 0.99f) c = 1.f;
     D.contrib[i] = c;
 }
-// ts, td: the sets' sorted copies, kept current for the particles of the last sort (i < n;
-// key null when not tracked)
+// ts, td: a particle of the last sort (i < n) that leaves its cell marks its set for a
+// full sort at the next sort point (key null: not tracked)
 __global__ void k_integrate(DevParams P, const DevState* __restrict__ S, Sets X, uint32_t full, float dt, int cd_on,
                             int do_sph, int do_dem, SortTrack ts, SortTrack td)
 {
@@ -937,11 +928,8 @@ __global__ void k_integrate(DevParams P, const DevState* __restrict__ S, Sets X,
         const snowb_particle_data& D = w ? X.sph : X.dem;
         integrate_one(P, D, i, dt, cd_on);
         const SortTrack& T = w ? ts : td;
-        if (T.key && i < (w ? ns : nd)) {
-            const uint32_t p = __ldg(T.inv + i);
-            track_move(P, T, i, p, ldv3(D.predict_positions, i), T.sid ? __ldg(T.sid + i) : 0u, D.mass[i]);
-            T.contrib_s[p] = D.contrib[i];
-        }
+        if (T.key && i < (w ? ns : nd))
+            track_move(P, T, i, ldv3(D.predict_positions, i), T.sid ? __ldg(T.sid + i) : 0u);
     }
 }
 

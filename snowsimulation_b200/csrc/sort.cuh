@@ -198,8 +198,7 @@ __global__ void k_rank_reorder(const uint32_t* __restrict__ key_o, const uint32_
                                const float* __restrict__ contrib, snowb_cell_data cd, float4* __restrict__ p4,
                                float* __restrict__ invm_s, float* __restrict__ contrib_s,
                                const uint32_t* n_ptr, uint32_t n_fixed, const uint32_t* cond,
-                               const uint32_t* __restrict__ sid_o, uint32_t* __restrict__ sid_s,
-                               uint32_t* __restrict__ inv_o = nullptr)
+                               const uint32_t* __restrict__ sid_o, uint32_t* __restrict__ sid_s)
 {
     if (cond && *cond == 0) return;
     const uint32_t n = n_ptr ? *n_ptr : n_fixed;
@@ -207,7 +206,6 @@ __global__ void k_rank_reorder(const uint32_t* __restrict__ key_o, const uint32_
         const uint32_t h = key_o[o], b = off[h], e = off[h + 1];
         const uint32_t r = stable_rank(tmp, b, e, o);
         const uint32_t p = b + r;
-        if (inv_o) inv_o[o] = p;
         cd.grid_index[p] = o;
         cd.grid_hash[p] = h;
         if (r == 0) { cd.cell_start[h] = b; cd.cell_end[h] = e; }
@@ -220,10 +218,13 @@ __global__ void k_rank_reorder(const uint32_t* __restrict__ key_o, const uint32_
     }
 }
 // Decision of one sort point for the sets in `sets` (bit k: set k is sorted here): a set
-// whose particles all kept their cells since its last sort (moved[k] clear) keeps its sort
-// outputs, which the position writers have kept current (SortTrack), so its sort launches
-// return at once.  moved[k] is consumed; the writers set it again.
-__global__ void k_sort_gate(DevState* S, uint32_t sets)
+// whose particles all kept their cells since its last sort (moved[k] clear) keeps its
+// permutation and cell table, so its sort launches return at once and k_sort_gather
+// refreshes the gathered outputs.  moved[k] is consumed; the writers set it again.
+// In a captured substep the decision also goes into the IF node of each set's sort (bit k
+// of use_h: h[k] is that node's handle), which then skips the launches altogether.
+__global__ void k_sort_gate(DevState* S, uint32_t sets, cudaGraphConditionalHandle h0,
+                            cudaGraphConditionalHandle h1, uint32_t use_h)
 {
     if (blockIdx.x == 0 && threadIdx.x == 0)
         for (int k = 0; k < 2; ++k)
@@ -233,29 +234,44 @@ __global__ void k_sort_gate(DevState* S, uint32_t sets)
                 S->moved[k] = 0u;
                 if (m) ++S->sorts_full[k];
                 else ++S->sorts_kept[k];
+                if ((use_h >> k) & 1u) cudaGraphSetConditional(k ? h1 : h0, m ? 1u : 0u);
             }
 }
 
-// The sorted copies of a set, kept current by the kernels that move its particles while
-// no particle leaves its cell; a particle whose cell changed marks the set for a full sort.
+// A set whose particles all kept their cells since its last sort sorts to the same
+// permutation and cell table, so only the gathered outputs change: the kernels that move
+// particles compare each new cell with the particle's key at the last sort and mark the
+// set when one differs.
 struct SortTrack {
     const uint32_t* key;        // cell key per original index at the set's last sort (null: no tracking)
-    const uint32_t* inv;        // sorted index per original index at the set's last sort
-    float4* p4;                 // sorted (x, y, z, mass)
-    float* contrib_s;           // sorted contrib
-    snowb_float3* sorted_pos;   // the caller's CellData::sorted_pos
     const uint32_t* sid;        // scene id per original index (batched runs) or null
     uint32_t* moved;            // &DevState::moved[set]
 };
-// a particle moved to predicted position q: keep the sorted copies (sorted index p) or mark
-// the set when its cell changed
-__device__ __forceinline__ void track_move(const DevParams& P, const SortTrack& T, uint32_t o, uint32_t p, float3 q,
-                                           uint32_t scene, float w)
+__device__ __forceinline__ void track_move(const DevParams& P, const SortTrack& T, uint32_t o, float3 q,
+                                           uint32_t scene)
 {
-    const uint32_t h = grid_hash(P, grid_pos(P, q, scene), 0, 0, 0);
-    if (h != __ldg(T.key + o)) *T.moved = 1u;
-    T.p4[p] = make_float4(q.x, q.y, q.z, w);
-    st3(T.sorted_pos, p, q);
+    if (grid_hash(P, grid_pos(P, q, scene), 0, 0, 0) != __ldg(T.key + o)) *T.moved = 1u;
+}
+// The outputs of k_rank_reorder for a kept sort (grid_hash, grid_index and the cell table
+// stay as the last sort wrote them): sorted_pos, the compact copies and the sorted scene
+// ids gathered from the current values.  Runs when *skip == 0 (the sort point's decision).
+__global__ void k_sort_gather(const snowb_float3* __restrict__ pos, const float* __restrict__ w,
+                              const float* __restrict__ invm, const float* __restrict__ contrib, snowb_cell_data cd,
+                              float4* __restrict__ p4, float* __restrict__ invm_s, float* __restrict__ contrib_s,
+                              const uint32_t* n_ptr, const uint32_t* skip, const uint32_t* __restrict__ sid_o,
+                              uint32_t* __restrict__ sid_s)
+{
+    if (*skip != 0) return;
+    const uint32_t n = *n_ptr;
+    GRID_LOOP(p, n) {
+        const uint32_t o = cd.grid_index[p];
+        const float3 q = ldv3(pos, o);
+        st3(cd.sorted_pos, p, q);
+        p4[p] = make_float4(q.x, q.y, q.z, w[o]);
+        invm_s[p] = invm[o];
+        contrib_s[p] = contrib[o];
+        if (sid_s) sid_s[p] = sid_o[o];
+    }
 }
 
 // sort_particles path: write the sorted keys and values only.
