@@ -60,43 +60,23 @@ __device__ __forceinline__ void reset_records(const snowb_particle_data& d, uint
     d.iter_end[t] = M * t;
 }
 
-// freeze / melt predicates (:4425, :4396); the particles changing phase are also counted
-// here (one atomic per warp and kind), so the decision below needs no scan
-__global__ void k_phase_flags(DevParams P, DevState* __restrict__ S, snowb_particle_data sph,
+// freeze / melt predicates (:4425, :4396)
+__global__ void k_phase_flags(DevParams P, const DevState* __restrict__ S, snowb_particle_data sph,
                               snowb_particle_data dem, int freeze, int melt, uint32_t* __restrict__ fl_s,
                               uint32_t* __restrict__ fl_d)
 {
     const uint32_t ns = S->n_sph, nd = S->n_dem;
-    const uint32_t lane = threadIdx.x & 31u;
     GRID_LOOP(t, ns + nd) {
-        bool f = false, m = false;
-        if (t < ns) {
-            f = freeze && sph.T[t] <= P.Tf && sph.contrib[t] >= 0.99f;
-            fl_s[t] = f ? 1u : 0u;
-        } else {
+        if (t < ns) fl_s[t] = (freeze && sph.T[t] <= P.Tf && sph.contrib[t] >= 0.99f) ? 1u : 0u;
+        else {
             const uint32_t i = t - ns;
-            m = melt && dem.T[i] > P.Tf && dem.contrib[i] >= 0.99f;
-            fl_d[i] = m ? 1u : 0u;
-        }
-        const uint32_t am = __activemask();
-        const uint32_t bf = __ballot_sync(am, f), bm = __ballot_sync(am, m);
-        if (lane == (uint32_t)(__ffs(am) - 1)) {
-            if (bf) atomicAdd(&S->n_freeze, (uint32_t)__popc(bf));
-            if (bm) atomicAdd(&S->n_melt, (uint32_t)__popc(bm));
+            fl_d[i] = (melt && dem.T[i] > P.Tf && dem.contrib[i] >= 0.99f) ? 1u : 0u;
         }
     }
 }
-// changed = some particle changes phase.  Without a change, and with a clean tail, the rest
-// of the phase-change chain (ranks, moves, compaction, record remap) leaves the state as it
-// is (the previous substep's compaction already wrote the same scan_index and predicates),
-// so a captured substep skips it: `use_h` writes that decision into the graph's IF node.
-__global__ void k_phase_count(DevState* S, cudaGraphConditionalHandle h, int use_h)
+__global__ void k_phase_count(DevState* S)
 {
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        const uint32_t ch = (S->n_freeze + S->n_melt) != 0u;
-        S->changed = ch;
-        if (use_h) cudaGraphSetConditional(h, (ch || S->tail_dirty) ? 1u : 0u);
-    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) S->changed = (S->n_freeze + S->n_melt) != 0u;
 }
 // freezing (:4416-4449) and melting (:4387-4414) with ranked targets
 // scene ids of batched runs travel with the particles (null pointers: one scene)
@@ -259,6 +239,15 @@ __global__ void __launch_bounds__(256) k_link_filter(DevParams P, DevState* S, S
         const float3 p = vd.pos(i);
         const uint32_t count = dem.iter_end[o] - o * M;
         uint8_t act = 0;
+        // With dynamic caps, adjust_connections (:4768-4808) can leave iter_end below the
+        // particle's first slot (it decrements for every slot past the cap, empty ones
+        // included), so count wraps round; links that partners add during the pass then
+        // bring it back below the cap.  Such a particle is kept: the pass decides.
+        if (dem.iter_end[o] < o * M) {
+            active[i] = 1;
+            atomicAdd(&S->n_active, 1u);
+            continue;
+        }
         // a particle at its cap stays inactive: its slots are not even read
         const bool below = count < link_tolerance(P, dem.T[o], dynamic);
         // own slots in registers (M <= SNOWB_MAXC_FAST), else read from memory

@@ -146,7 +146,6 @@ struct Ctx {
     DevState* S_host = nullptr;
     uint32_t* err_dev = nullptr;
     cudaStream_t side = nullptr;          // second stream for the water sort (see sort_pair)
-    cudaStream_t body[2] = {};            // capture streams of conditional graph regions
     cudaEvent_t fork = nullptr, join = nullptr;
 };
 static Ctx g_ctx;
@@ -171,8 +170,6 @@ static void free_ctx(Ctx& c)
         if (p) cudaFree(p);
     if (c.S_host) cudaFreeHost(c.S_host);
     if (c.side) cudaStreamDestroy(c.side);
-    for (cudaStream_t b : c.body)
-        if (b) cudaStreamDestroy(b);
     if (c.fork) cudaEventDestroy(c.fork);
     if (c.join) cudaEventDestroy(c.join);
     c = Ctx();
@@ -220,7 +217,6 @@ static int ensure_ctx(uint32_t full, uint32_t nb, uint32_t ncells)
     CUDA_TRY(cudaMemset(c.err_dev, 0, sizeof(uint32_t)));
     CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&c.S_host), sizeof(DevState)));
     CUDA_TRY(cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking));
-    for (cudaStream_t& b : c.body) CUDA_TRY(cudaStreamCreateWithFlags(&b, cudaStreamNonBlocking));
     CUDA_TRY(cudaEventCreateWithFlags(&c.fork, cudaEventDisableTiming));
     CUDA_TRY(cudaEventCreateWithFlags(&c.join, cudaEventDisableTiming));
     int sms = 148;
@@ -250,13 +246,10 @@ static uint64_t g_launches = 0;
 static std::vector<ProfRec> g_prof_pool;
 static size_t g_prof_used = 0;
 static bool g_capturing = false;
-static int g_cond_depth = 0;   // > 0 while capturing into a conditional region's body
 
 static void prof_begin(const char* name)
 {
-    // kernels in a conditional region's body run only when its condition holds, so they
-    // are not counted as launched
-    if (g_cond_depth == 0) ++g_launches;
+    ++g_launches;
     if (!g_prof) return;
     if (g_prof_used == g_prof_pool.size()) {
         ProfRec r{name, nullptr, nullptr};
@@ -368,80 +361,6 @@ static void tune_pick(const char* name, uint64_t work, int tpb0, int max_tpb, in
         else LAUNCH(kernel, work, tpb0, __VA_ARGS__);                                        \
     } while (0)
 #define LAUNCH1(kernel, ...) KL(kernel, 1, 32, __VA_ARGS__)
-
-// ------------------------------------------------------------------ conditional regions
-// Inside a capture, a region whose work leaves the state unchanged when a device-side
-// decision is false becomes an IF node of the graph, so a replay skips its launches instead
-// of launching kernels that return at once.  The decision is taken by a kernel launched
-// before the region, which also writes it into the node's handle (cudaGraphSetConditional);
-// the region's kernels read the same device flags, so direct launches (outside a capture)
-// return early or do the same identity work and give the same results.  A conditional body
-// may hold only kernels (no event records), so regions are not used while profiling, and a
-// stream fork or join stays outside them.
-struct CondRegion {
-    bool on = false;
-    cudaGraphConditionalHandle h = 0;
-    cudaStream_t outer = nullptr, body = nullptr, saved = nullptr;
-    cudaGraph_t* bodies = nullptr;   // the node's body graphs (then, else)
-};
-// handle on the graph being captured on g_stream; the node will follow the last work on `outer`
-static int cond_open(CondRegion& R, cudaStream_t outer, cudaStream_t body)
-{
-    R = CondRegion();
-    if (!g_capturing || g_prof) return SNOWB_OK;
-    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
-    cudaGraph_t graph = nullptr;
-    CUDA_TRY(cudaStreamGetCaptureInfo(g_stream, &st, nullptr, &graph, nullptr, nullptr));
-    if (st != cudaStreamCaptureStatusActive) return fail(SNOWB_ERR_CUDA, "conditional region outside a capture");
-    CUDA_TRY(cudaGraphConditionalHandleCreate(&R.h, graph, 0, cudaGraphCondAssignDefault));
-    R.on = true;
-    R.outer = outer;
-    R.body = body;
-    return SNOWB_OK;
-}
-// adds the IF node (with an ELSE body when with_else) after the work captured so far on
-// R.outer; launches go into its first body
-static int cond_body(CondRegion& R, bool with_else = false)
-{
-    if (!R.on) return SNOWB_OK;
-    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
-    cudaGraph_t graph = nullptr;
-    const cudaGraphNode_t* deps = nullptr;
-    size_t ndeps = 0;
-    CUDA_TRY(cudaStreamGetCaptureInfo(R.outer, &st, nullptr, &graph, &deps, &ndeps));
-    if (st != cudaStreamCaptureStatusActive) return fail(SNOWB_ERR_CUDA, "conditional region on a stream not captured");
-    cudaGraphNodeParams prm = {cudaGraphNodeTypeConditional};
-    prm.conditional.handle = R.h;
-    prm.conditional.type = cudaGraphCondTypeIf;
-    prm.conditional.size = with_else ? 2 : 1;
-    cudaGraphNode_t node = nullptr;
-    CUDA_TRY(cudaGraphAddNode(&node, graph, deps, ndeps, &prm));
-    CUDA_TRY(cudaStreamUpdateCaptureDependencies(R.outer, &node, 1, cudaStreamSetCaptureDependencies));
-    R.bodies = prm.conditional.phGraph_out;
-    CUDA_TRY(cudaStreamBeginCaptureToGraph(R.body, R.bodies[0], nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    R.saved = g_stream;
-    g_stream = R.body;
-    ++g_cond_depth;
-    return SNOWB_OK;
-}
-// launches go into the ELSE body (run when the decision is false)
-static int cond_else(CondRegion& R)
-{
-    if (!R.on) return SNOWB_OK;
-    cudaGraph_t g = nullptr;
-    CUDA_TRY(cudaStreamEndCapture(R.body, &g));
-    CUDA_TRY(cudaStreamBeginCaptureToGraph(R.body, R.bodies[1], nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    return SNOWB_OK;
-}
-static int cond_end(CondRegion& R)
-{
-    if (!R.on) return SNOWB_OK;
-    g_stream = R.saved;
-    --g_cond_depth;
-    cudaGraph_t g = nullptr;
-    CUDA_TRY(cudaStreamEndCapture(R.body, &g));
-    return SNOWB_OK;
-}
 
 static inline unsigned scan_blocks(uint32_t n) { return (n + SCAN_CHUNK - 1) / SCAN_CHUNK + (n == 0); }
 
@@ -639,27 +558,11 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
     bool dirty_s = true, dirty_d = true;
     auto track = [&](int set) { return SortTrack{c.s[set].key, set ? a.sid_dem : a.sid_sph, &S->moved[set]}; };
     const SortTrack track_s = track(0), track_d = track(1);
-    // a sort point of one set: the full sort when the gate's decision is set, else the
-    // gather of the kept sort (each kernel returns at once on the other decision)
+    // a sort point of one set: the full sort when the gate's decision is set, else only the
+    // refresh of the gathered outputs (the hash, scan and scatter launches return at once)
     auto sort_if = [&](int set) -> int {
         TRY(sort_set(P, c.s[set], set ? *a.dem : *a.sph, set ? a.dcd : a.scd, set ? n_d : n_s, cap, &S->resort[set],
                      !ref, set ? a.sid_dem : a.sid_sph));
-        return SNOWB_OK;
-    };
-    auto gather_if = [&](int set) -> int {
-        SetBufs& B = c.s[set];
-        const snowb_particle_data& D = set ? *a.dem : *a.sph;
-        const uint32_t* sid = set ? a.sid_dem : a.sid_sph;
-        LAUNCH(k_sort_gather, cap, 256, D.predict_positions, D.mass, D.massInv, D.contrib, set ? a.dcd : a.scd, B.p4,
-               B.invm, B.contrib, set ? n_d : n_s, &S->resort[set], sid, sid ? B.sid : nullptr);
-        return SNOWB_OK;
-    };
-    auto sort_region = [&](int set, CondRegion& R) -> int {
-        TRY(cond_body(R, true));
-        TRY(sort_if(set));
-        TRY(cond_else(R));
-        TRY(gather_if(set));
-        TRY(cond_end(R));
         return SNOWB_OK;
     };
     // The two sets' sorts share no buffer: the water sort runs on a side stream beside the
@@ -670,21 +573,17 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
     auto sort_pair = [&](bool after_phase) -> int {
         const bool need_s = dirty_s || after_phase, need_d = dirty_d || after_phase;
         if (!need_s && !need_d) return SNOWB_OK;
+        LAUNCH1(k_sort_gate, S, (need_s ? 1u : 0u) | (need_d ? 2u : 0u));
         const cudaStream_t main_stream = g_stream;
-        CondRegion rs, rd;
-        if (need_s) TRY(cond_open(rs, c.side, c.body[0]));
-        if (need_d) TRY(cond_open(rd, main_stream, c.body[1]));
-        LAUNCH1(k_sort_gate, S, (need_s ? 1u : 0u) | (need_d ? 2u : 0u), rs.h, rd.h,
-                (rs.on ? 1u : 0u) | (rd.on ? 2u : 0u));
         if (need_s) {
             CUDA_TRY(cudaEventRecord(c.fork, main_stream));
             CUDA_TRY(cudaStreamWaitEvent(c.side, c.fork, 0));
             g_stream = c.side;
-            const int rc = sort_region(0, rs);
+            const int rc = sort_if(0);
             g_stream = main_stream;
             TRY(rc);
         }
-        if (need_d) TRY(sort_region(1, rd));
+        if (need_d) TRY(sort_if(1));
         if (need_s) {
             CUDA_TRY(cudaEventRecord(c.join, c.side));
             CUDA_TRY(cudaStreamWaitEvent(main_stream, c.join, 0));
@@ -707,13 +606,10 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
     STOP(3);
     if (a.change_phase) {
         LAUNCH(k_phase_flags, 2 * full, 256, P, S, *a.sph, *a.dem, a.freezing, a.melting, c.fl_s, c.fl_d);
-        CondRegion rp;
-        TRY(cond_open(rp, g_stream, c.body[0]));
-        LAUNCH1(k_phase_count, S, rp.h, rp.on ? 1 : 0);
-        TRY(cond_body(rp));
         const uint32_t sb_stride = cap / SCAN_CHUNK + 2;
         TRY(scan(c.fl_s, n_s, 0, cap, c.sbsum, c.rk_s, &S->n_freeze, nullptr));
         TRY(scan(c.fl_d, n_d, 0, cap, c.sbsum + sb_stride, c.rk_d, &S->n_melt, nullptr));
+        LAUNCH1(k_phase_count, S);
         LAUNCH(k_phase_move, 2 * full, 256, P, S, *a.sph, *a.dem, c.fl_s, c.rk_s, c.fl_d, c.rk_d, scn);
         // compact_and_clean (:4495-4589): predicate scans run every substep (they define
         // scan_index), the data movement only after a phase change.
@@ -727,7 +623,6 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
         LAUNCH(k_compact_finish, 2 * full, 256, P, S, *a.sph, *a.dem, full);
         LAUNCH1(k_commit_sizes, S);
         LAUNCH(k_update_records, (uint64_t)P.maxc * full, 256, P, S, *a.dem);
-        TRY(cond_end(rp));
         LAUNCH1(k_clear_tail_flag, S);
     }
     STOP(4);
@@ -1158,15 +1053,6 @@ static int graph_substeps(const DevParams& P, const StepArgs& a, bool step_sph, 
         g_capturing = true;
         int rc = e0 == cudaSuccess ? substep(P, a, step_sph, step_dem) : SNOWB_ERR_CUDA;
         g_capturing = false;
-        if (g_cond_depth != 0) {   // a failure inside a conditional region: close its capture
-            g_cond_depth = 0;
-            for (cudaStream_t b : g_ctx.body) {
-                cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
-                cudaGraph_t bg = nullptr;
-                if (b && cudaStreamIsCapturing(b, &st) == cudaSuccess && st != cudaStreamCaptureStatusNone)
-                    cudaStreamEndCapture(b, &bg);
-            }
-        }
         const uint64_t nodes = g_launches - before;
         g_launches = before;
         cudaGraph_t gr = nullptr;

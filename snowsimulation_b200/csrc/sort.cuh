@@ -191,7 +191,10 @@ __device__ __forceinline__ uint32_t stable_rank(const uint32_t* __restrict__ tmp
 
 // ------------------------------------------------------------------ 4. rank + outputs
 // Fused path (sort_and_reorder :398-420 with hash = cell of pos).  Also gathers the
-// compact sorted attributes: p4 = (pos, w[o]), invm_s, contrib_s.
+// compact sorted attributes: p4 = (pos, w[o]), invm_s, contrib_s.  With *cond == 0 the
+// sort point keeps the last sort (no particle left its cell, same set size): grid_hash,
+// grid_index and the cell table are already what this sort would write, so only the
+// gathered outputs are refreshed, sorted slot by sorted slot.
 __global__ void k_rank_reorder(const uint32_t* __restrict__ key_o, const uint32_t* __restrict__ off,
                                const uint32_t* __restrict__ tmp, const snowb_float3* __restrict__ pos,
                                const float* __restrict__ w, const float* __restrict__ invm,
@@ -200,8 +203,19 @@ __global__ void k_rank_reorder(const uint32_t* __restrict__ key_o, const uint32_
                                const uint32_t* n_ptr, uint32_t n_fixed, const uint32_t* cond,
                                const uint32_t* __restrict__ sid_o, uint32_t* __restrict__ sid_s)
 {
-    if (cond && *cond == 0) return;
     const uint32_t n = n_ptr ? *n_ptr : n_fixed;
+    if (cond && *cond == 0) {
+        GRID_LOOP(p, n) {
+            const uint32_t o = cd.grid_index[p];
+            const float3 q = ldv3(pos, o);
+            st3(cd.sorted_pos, p, q);
+            if (p4) p4[p] = make_float4(q.x, q.y, q.z, w ? w[o] : 0.f);
+            if (invm_s) invm_s[p] = invm[o];
+            if (contrib_s) contrib_s[p] = contrib[o];
+            if (sid_s) sid_s[p] = sid_o[o];
+        }
+        return;
+    }
     GRID_LOOP(o, n) {
         const uint32_t h = key_o[o], b = off[h], e = off[h + 1];
         const uint32_t r = stable_rank(tmp, b, e, o);
@@ -219,12 +233,10 @@ __global__ void k_rank_reorder(const uint32_t* __restrict__ key_o, const uint32_
 }
 // Decision of one sort point for the sets in `sets` (bit k: set k is sorted here): a set
 // whose particles all kept their cells since its last sort (moved[k] clear) keeps its
-// permutation and cell table, so its sort launches return at once and k_sort_gather
-// refreshes the gathered outputs.  moved[k] is consumed; the writers set it again.
-// In a captured substep the decision also goes into the IF node of each set's sort (bit k
-// of use_h: h[k] is that node's handle), which then skips the launches altogether.
-__global__ void k_sort_gate(DevState* S, uint32_t sets, cudaGraphConditionalHandle h0,
-                            cudaGraphConditionalHandle h1, uint32_t use_h)
+// permutation and cell table: the hash, scan and scatter launches return at once and
+// k_rank_reorder only refreshes the gathered outputs.  moved[k] is consumed; the writers
+// set it again.
+__global__ void k_sort_gate(DevState* S, uint32_t sets)
 {
     if (blockIdx.x == 0 && threadIdx.x == 0)
         for (int k = 0; k < 2; ++k)
@@ -234,7 +246,6 @@ __global__ void k_sort_gate(DevState* S, uint32_t sets, cudaGraphConditionalHand
                 S->moved[k] = 0u;
                 if (m) ++S->sorts_full[k];
                 else ++S->sorts_kept[k];
-                if ((use_h >> k) & 1u) cudaGraphSetConditional(k ? h1 : h0, m ? 1u : 0u);
             }
 }
 
@@ -252,28 +263,6 @@ __device__ __forceinline__ void track_move(const DevParams& P, const SortTrack& 
 {
     if (grid_hash(P, grid_pos(P, q, scene), 0, 0, 0) != __ldg(T.key + o)) *T.moved = 1u;
 }
-// The outputs of k_rank_reorder for a kept sort (grid_hash, grid_index and the cell table
-// stay as the last sort wrote them): sorted_pos, the compact copies and the sorted scene
-// ids gathered from the current values.  Runs when *skip == 0 (the sort point's decision).
-__global__ void k_sort_gather(const snowb_float3* __restrict__ pos, const float* __restrict__ w,
-                              const float* __restrict__ invm, const float* __restrict__ contrib, snowb_cell_data cd,
-                              float4* __restrict__ p4, float* __restrict__ invm_s, float* __restrict__ contrib_s,
-                              const uint32_t* n_ptr, const uint32_t* skip, const uint32_t* __restrict__ sid_o,
-                              uint32_t* __restrict__ sid_s)
-{
-    if (*skip != 0) return;
-    const uint32_t n = *n_ptr;
-    GRID_LOOP(p, n) {
-        const uint32_t o = cd.grid_index[p];
-        const float3 q = ldv3(pos, o);
-        st3(cd.sorted_pos, p, q);
-        p4[p] = make_float4(q.x, q.y, q.z, w[o]);
-        invm_s[p] = invm[o];
-        contrib_s[p] = contrib[o];
-        if (sid_s) sid_s[p] = sid_o[o];
-    }
-}
-
 // sort_particles path: write the sorted keys and values only.
 __global__ void k_rank_pairs(const uint32_t* __restrict__ key_o, const uint32_t* __restrict__ val_o,
                              const uint32_t* __restrict__ off, const uint32_t* __restrict__ tmp,
