@@ -657,10 +657,8 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
         TRY(sort_pair(false));
         TAPE_HOOK(2, it);
         STOP(base + 0);
-        // density + lambda: the candidate lists, then the sums over them (stage boundaries
-        // base+1 and base+2 coincide)
-        TLAUNCH(k_nlist_build, 256, 2 * full, 128, P, S, vs, vd, vb, NL);
-        TLAUNCH(k_density<true>, 256, work3, 128, P, S, vs, vd, vb, X, ss, sd, sb, NL, 1);
+        // density + lambda in one pass (stage boundaries base+1 and base+2 coincide)
+        TLAUNCH(k_density<true>, 256, work3, 128, P, S, vs, vd, vb, X, ss, sd, sb, NL);
         STOP(base + 2);
         // the reference's snow PBF pass adds into repeated targets with float atomics (Q3):
         // its order follows the launch shape, so that pass keeps the built-in shape

@@ -385,94 +385,9 @@ __device__ __forceinline__ void acc_WG(const DevParams& P, float& rho, float& gs
         if (LAMBDA) gs += cg;
     }
 }
-// ------------------------------------------- density + lambda in two phases (lists)
-// The one-pass form evaluates each accepted candidate's terms inside the candidate scan, so
-// the lanes of a warp wait on one another's accepted terms at almost every step (about one
-// candidate in eight is accepted, at different steps in different lanes).  In two phases:
-// k_nlist_build runs the scan alone and records every candidate with d < h (own set
-// without the particle itself, then the other set, then the boundary; cells z-y-x, index
-// ascending, each tagged with its cell), and k_density<true> evaluates the terms over each
-// particle's list, closing the per-cell partial sums where the cell changes -- the same
-// operations in the same order as the one-pass form.  Cells without accepted candidates
-// add +0 there, which leaves the (non-negative) sums unchanged, so they are not visited.
-__device__ __forceinline__ void push_if_near(const DevParams& P, float3 p, float3 q, uint32_t j, int cell, int set,
-                                             NLWriter& wr)
-{
-    const float3 dv = sub3(p, q);
-    if (dot3(dv, dv) < P.h2_lt) wr.push(j, cell, set);
-}
-__device__ __forceinline__ void acc_push(const DevParams& P, const SetView& v, float3 p, const Nbhd& nb,
-                                         uint32_t skip, NLWriter& wr, int set)
-{
-    const P2 pp = bcast2(p);
-    FOR27 {
-        uint32_t s, e;
-        if (!v.range_nb(nb, ox, oy, oz, s, e)) continue;
-        const int cell = CELL27;
-        if (e <= v.n) {
-            // current entries, screened two at a time as in acc_WG, then the exact test
-            uint32_t j = s;
-            for (; j + 1 < e; j += 2) {
-                const float4 q0 = __ldg(v.p4 + j), q1 = __ldg(v.p4 + j + 1);
-                const float2 dd = d2_pair(pp, q0, q1);
-                if (dd.x < P.h2_cull && j != skip) push_if_near(P, p, xyz(q0), j, cell, set, wr);
-                if (dd.y < P.h2_cull && j + 1 != skip) push_if_near(P, p, xyz(q1), j + 1, cell, set, wr);
-            }
-            if (j < e && j != skip) push_if_near(P, p, xyz(__ldg(v.p4 + j)), j, cell, set, wr);
-        } else {
-            for (uint32_t j = s; j < e; ++j)
-                if (j != skip) push_if_near(P, p, v.pos(j), j, cell, set, wr);
-        }
-    }
-}
-__global__ void __launch_bounds__(256) k_nlist_build(DevParams P, DevState* __restrict__ S, SetView vs, SetView vd,
-                                                     SetView vb, NList L)
-{
-    const uint32_t ns = S->n_sph, nd = S->n_dem, nb = S->n_b;
-    vs.n = ns; vd.n = nd; vb.n = nb;
-    GRID_LOOP(t, ns + nd) {
-        const bool w = t < ns;
-        const uint32_t i = w ? t : t - ns;
-        const SetView& own = w ? vs : vd;
-        const SetView& oth = w ? vd : vs;
-        const float3 p = xyz(own.p4[i]);
-        const GCell g = grid_pos(P, p, own.scene(i));
-        const Nbhd nbh = make_nbhd(P, g, p, P.h2_cull);
-        NLWriter wr{L.e, L.stride, (w ? 0u : L.cap) + i, 0u};
-        acc_push(P, own, p, nbh, i, wr, 0);
-        const uint32_t n_own = wr.n;
-        acc_push(P, oth, p, nbh, SNOWB_UMAX, wr, 1);
-        const uint32_t n_oth = wr.n - n_own;
-        acc_push(P, vb, p, nbh, SNOWB_UMAX, wr, 2);
-        const uint32_t n_bnd = wr.n - n_own - n_oth;
-        L.cnt[wr.slot] = wr.n > NLIST_K ? NL_OVF : (n_own | (n_oth << 10) | (n_bnd << 20));
-        if (wr.n > NLIST_K) atomicAdd(&S->n_nl_ovf, 1u);
-    }
-    (void)nb;
-}
-// density and lambda-gradient sums over a recorded segment (modes 0 and 1 of wg_term)
-__device__ __forceinline__ void seg_WG(const DevParams& P, float& rho, float& gs, const Seg& G, const SetView& v,
-                                       float3 p, bool vol, int mode, float m_self)
-{
-    float cs = 0.f, cg = 0.f;
-    uint32_t cur = 0xFFu;
-    for (uint32_t k = G.k0; k < G.k1; ++k) {
-        const uint32_t en = G.at(k), j = en & NL_J_MASK, cell = (en >> 25) & 31u;
-        if (cell != cur) {
-            if (cur != 0xFFu) { rho += cs; gs += cg; }
-            cs = 0.f; cg = 0.f; cur = cell;
-        }
-        wg_term<true>(P, cs, cg, v.pw(j), p, j, vol, mode, m_self, 0.f, nullptr, 0, 0);
-    }
-    if (cur != 0xFFu) { rho += cs; gs += cg; }
-}
-
-// lists (LAMBDA only): the candidates of the water and snow particles were recorded by
-// k_nlist_build; their terms come from the lists (traversal for an overflowed list).
 template <bool LAMBDA>
 __global__ void __launch_bounds__(256) k_density(DevParams P, DevState* __restrict__ S, SetView vs, SetView vd,
-                                                 SetView vb, Sets X, Sorted ss, Sorted sd, Sorted sb, NList L,
-                                                 int lists = 0)
+                                                 SetView vb, Sets X, Sorted ss, Sorted sd, Sorted sb, NList L)
 {
     const uint32_t ns = S->n_sph, nd = S->n_dem, nb = S->n_b;
     vs.n = ns; vd.n = nd; vb.n = nb;
@@ -490,37 +405,25 @@ __global__ void __launch_bounds__(256) k_density(DevParams P, DevState* __restri
             D = w ? &X.sph : &X.dem;
             lam_s = w ? ss.lambda : sd.lambda;
             o = own.gi[i];
-            const float3 p = xyz(own.p4[i]);
+            float3 p = xyz(own.p4[i]); GCell g = grid_pos(P, p, own.scene(i));
+            const Nbhd nb = make_nbhd(P, g, p, P.h2_cull);
             rho = D->mass[o] * P.W0;
-            Seg so, sx, sbn;
-            const bool replay = LAMBDA && lists && segments(L, (w ? 0u : L.cap) + i, so, sx, sbn);
-            const Nbhd nb = replay ? Nbhd{} : make_nbhd(P, grid_pos(P, p, own.scene(i)), p, P.h2_cull);
-            if (replay) {
-                seg_WG(P, rho, gs, so, own, p, false, 0, 0.f);
-                seg_WG(P, rho, gs, sx, oth, p, false, 0, 0.f);
-                seg_WG(P, rho, gs, sbn, vb, p, true, 1, D->mass[o]);
-            } else if (LAMBDA && lists) {   // overflowed list: the traversal, nothing recorded
-                acc_WG<true>(P, rho, gs, own, p, nb, i, false, 0, 0.f, nullptr, nullptr);
-                acc_WG<true>(P, rho, gs, oth, p, nb, SNOWB_UMAX, false, 0, 0.f, nullptr, nullptr);
-                acc_WG<true>(P, rho, gs, vb, p, nb, SNOWB_UMAX, true, 1, D->mass[o], nullptr, nullptr);
-            } else {
-                NLWriter wr{L.e, L.stride, (w ? 0u : L.cap) + i, 0u};
-                // the one-pass density+lambda form lists all three sets for the PBF and contact passes;
-                // the substep's first density pass lists the snow-snow candidates for link formation
-                NLWriter* pw = (LAMBDA || !w) ? &wr : nullptr;
-                acc_WG<LAMBDA>(P, rho, gs, own, p, nb, i, false, 0, 0.f, nullptr, nullptr, pw, 0);
-                const uint32_t n_own = wr.n;
-                if (!LAMBDA) pw = nullptr;
-                acc_WG<LAMBDA>(P, rho, gs, oth, p, nb, SNOWB_UMAX, false, 0, 0.f, nullptr, nullptr, pw, 1);
-                const uint32_t n_oth = wr.n - n_own;
-                acc_WG<LAMBDA>(P, rho, gs, vb, p, nb, SNOWB_UMAX, true, 1, D->mass[o], nullptr, nullptr, pw, 2);
-                if (LAMBDA) {
-                    const uint32_t n_bnd = wr.n - n_own - n_oth;
-                    L.cnt[wr.slot] = wr.n > NLIST_K ? NL_OVF : (n_own | (n_oth << 10) | (n_bnd << 20));
-                    if (wr.n > NLIST_K) atomicAdd(&S->n_nl_ovf, 1u);
-                } else if (!w) {
-                    L.cnt[wr.slot] = n_own > NLIST_K ? NL_OVF : n_own;
-                }
+            NLWriter wr{L.e, L.stride, (w ? 0u : L.cap) + i, 0u};
+            // the density+lambda pass lists all three sets for the PBF and contact passes; the
+            // substep's first density pass lists the snow-snow candidates for link formation
+            NLWriter* pw = (LAMBDA || !w) ? &wr : nullptr;
+            acc_WG<LAMBDA>(P, rho, gs, own, p, nb, i, false, 0, 0.f, nullptr, nullptr, pw, 0);
+            const uint32_t n_own = wr.n;
+            if (!LAMBDA) pw = nullptr;
+            acc_WG<LAMBDA>(P, rho, gs, oth, p, nb, SNOWB_UMAX, false, 0, 0.f, nullptr, nullptr, pw, 1);
+            const uint32_t n_oth = wr.n - n_own;
+            acc_WG<LAMBDA>(P, rho, gs, vb, p, nb, SNOWB_UMAX, true, 1, D->mass[o], nullptr, nullptr, pw, 2);
+            if (LAMBDA) {
+                const uint32_t n_bnd = wr.n - n_own - n_oth;
+                L.cnt[wr.slot] = wr.n > NLIST_K ? NL_OVF : (n_own | (n_oth << 10) | (n_bnd << 20));
+                if (wr.n > NLIST_K) atomicAdd(&S->n_nl_ovf, 1u);
+            } else if (!w) {
+                L.cnt[wr.slot] = n_own > NLIST_K ? NL_OVF : n_own;
             }
         } else {
             // boundary: density sums the sets in the order (b, snow, water), lambda (b, water, snow)
