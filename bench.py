@@ -63,6 +63,7 @@ def parse():
     ap.add_argument("--precision-study", action="store_true")
     ap.add_argument("--precision-fp64-frames", type=int, default=10)
     ap.add_argument("--precision-energy-frames", type=int, default=600)
+    ap.add_argument("--precision-quirks", default="fixed", choices=["fixed", "reference"])
     ap.add_argument("--profile-out", default="")
     return ap.parse_args()
 
@@ -483,7 +484,7 @@ def long_window(frames, dev, seed, flush, scene_name="config1"):
 
 
 # ----------------------------------------------------------------- precision study (config 4)
-def precision_study(dev, fp64_frames=10, energy_frames=600, profile_frames=2):
+def precision_study(dev, fp64_frames=10, energy_frames=600, profile_frames=2, quirks="fixed"):
     """The large scene (1,048,576 snow + 131,072 water, 128^3 grid, walls at +-1.5 m) from
     rest: (1) the FP32 GPU run against the FP64 oracle run of the same scene, frame by frame
     for `fp64_frames` frames (particles matched by track id): position, velocity and
@@ -491,16 +492,22 @@ def precision_study(dev, fp64_frames=10, energy_frames=600, profile_frames=2):
     `energy_frames` frames with its FP64 heat-energy and momentum reductions every 10
     frames (drift from the start); (3) the per-kernel device time over `profile_frames`
     frames (CUDA-event nodes in the substep graph) against the algorithmic bytes of each
-    kernel: achieved GB/s and fraction of the measured HBM peak."""
+    kernel: achieved GB/s and fraction of the measured HBM peak, taken right after (1).
+    quirks: "fixed" (the intended physics) or "reference".  With the reference's quirks the
+    heat pass sums each particle's own cell 27 times (Q7), which with conductivities of
+    600 and 2500 W/mK puts the explicit snow-snow conduction step above its stability limit
+    once the melt brings temperature gradients into the snow, so a long run blows up."""
     import numpy as np
     import torch
     from snowsimulation_b200 import scene, bytes_model, _native
     from snowsimulation_b200.world import Simulation
     from oracle.oracle import OracleWorld
+    from snowsimulation_b200.abi import QUIRKS_FIXED, QUIRKS_REFERENCE
+    qm = QUIRKS_FIXED if quirks == "fixed" else QUIRKS_REFERENCE
     w = scene.config4(seed=0)
-    sim = Simulation(w, device=dev).setup()
+    sim = Simulation(w, device=dev, quirks=qm).setup()
     t0 = time.perf_counter()
-    o = OracleWorld(w, 64, threads=os.cpu_count() or 1).setup()
+    o = OracleWorld(w, 64, qm, threads=os.cpu_count() or 1).setup()
 
     def by_id(sets):
         ids = np.concatenate([d["trackId"][:n] for d, n in sets])
@@ -527,16 +534,10 @@ def precision_study(dev, fp64_frames=10, energy_frames=600, profile_frames=2):
         print("precision frame %d: %s" % (f, json.dumps(r)), file=sys.stderr, flush=True)
     t_fp64 = time.perf_counter() - t0
     del o
-    drift = []
-    for f in range(fp64_frames, energy_frames):
-        sim.step(substeps=SUBSTEPS, sync=False, use_graph=True)
-        if (f + 1) % 10 == 0 or f == energy_frames - 1:
-            sim.read_sizes()
-            e = sim.energy_momentum()
-            drift.append({"frame": f, "energy_drift_rel": (e[0] - e0g[0]) / abs(e0g[0]), "momentum": e[1:],
-                          "sizes": [sim.n_sph, sim.n_dem]})
     # per-kernel table over the next frames
     lib = sim.lib
+    for _ in range(2):   # the graphs of these frames, captured before the profiled ones
+        sim.step(substeps=SUBSTEPS, sync=False, use_graph=True)
     lib.snowb_profile_begin()
     for _ in range(profile_frames):
         sim.step(substeps=SUBSTEPS, sync=False, use_graph=True)
@@ -558,12 +559,22 @@ def precision_study(dev, fp64_frames=10, energy_frames=600, profile_frames=2):
             row.update(algorithmic_bytes_per_launch=kb, achieved_GBs=gbs, hbm_frac=gbs / peak)
         table.append(row)
     table.sort(key=lambda r: -r["ms_per_frame"])
-    return {"workload": "config4: %d water + %d snow + %d boundary, 128^3 grid, walls +-1.5 m, from rest"
-                        % (w.n_sph, w.n_dem, w.n_b),
+    prof_at = fp64_frames + 2
+    drift = []
+    for f in range(fp64_frames + 2 + profile_frames, energy_frames):
+        sim.step(substeps=SUBSTEPS, sync=False, use_graph=True)
+        if (f + 1) % 10 == 0 or f == energy_frames - 1:
+            sim.read_sizes()
+            e = sim.energy_momentum()
+            drift.append({"frame": f, "energy_drift_rel": (e[0] - e0g[0]) / abs(e0g[0]), "momentum": e[1:],
+                          "sizes": [sim.n_sph, sim.n_dem]})
+    return {"workload": "config4: %d water + %d snow + %d boundary, 128^3 grid, walls +-1.5 m, from rest, %s quirks"
+                        % (w.n_sph, w.n_dem, w.n_b, quirks),
             "fp64": {"frames": fp64_frames, "oracle": "FP64 C restatement, OpenMP %d threads, %.0f s"
                                                       % (os.cpu_count() or 1, t_fp64), "per_frame": rows},
             "energy": {"frames": energy_frames, "start_J": e0g[0], "every_10_frames": drift},
-            "kernels": {"frames": profile_frames, "peak_GBs": peak, "peak_kind": peak_kind, "table": table}}
+            "kernels": {"frames": "%d-%d" % (prof_at, prof_at + profile_frames - 1), "peak_GBs": peak,
+                        "peak_kind": peak_kind, "table": table}}
 
 
 # ----------------------------------------------------------------- adjoint vs plain
@@ -634,7 +645,8 @@ def main():
         import torch
         dev = torch.device("cuda", 0)
         torch.cuda.set_device(dev)
-        print(json.dumps(precision_study(dev, args.precision_fp64_frames, args.precision_energy_frames)))
+        print(json.dumps(precision_study(dev, args.precision_fp64_frames, args.precision_energy_frames,
+                                         quirks=args.precision_quirks)))
         return 0
     import torch
     import torch.distributed as dist

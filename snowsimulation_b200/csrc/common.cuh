@@ -59,6 +59,10 @@ struct DevState {
     // by k_sort_gate.  sorts_full/sorts_kept count the decisions since the call started.
     uint32_t moved[2], resort[2];
     uint32_t sorts_full[2], sorts_kept[2];
+    // a snow particle moved more than FR_LIST_MOVE since the iteration's neighbour lists
+    // were built (set by k_apply, cleared by the density+lambda pass)
+    uint32_t far_move;
+    uint32_t sc_count[8];           // super-cells listed for each link colour (SCList)
 };
 #define SNOWB_DEVERR_SCATTER 1u
 #define SNOWB_DEVERR_SCENE 2u      // a batched scene id >= the scene count

@@ -224,12 +224,39 @@ __device__ __forceinline__ bool has_free_slot(const uint32_t* rec, uint32_t o, u
         if (rec[q] == SNOWB_UMAX) return true;
     return false;
 }
+// Super-cells holding an active particle, listed per colour by the prefilter so that a
+// colour pass visits only those (same-coloured super-cells are independent, so their order
+// does not matter; inside one the particles are still taken in ascending sorted index).
+// flag null: no list, the colour pass visits every super-cell of its colour.
+struct SCList {
+    uint32_t* flag;     // per super-cell (colour c, index t at c * per + t): listed
+    uint32_t* list;     // colour c's listed indices t at list[c * per + k], k < count[c]
+    uint32_t* count;    // DevState::sc_count
+    uint32_t per;       // super-cells per colour
+};
+// colour and index within the colour of the super-cell holding hash cell h (the layout of
+// k_link_colour_warp: super-cell (sx, sy, sz) = cell / 2, colour = parities of sx, sy, sz)
+__device__ __forceinline__ void supercell_of(const DevParams& P, uint32_t h, uint32_t& colour, uint32_t& t)
+{
+    const uint32_t x = h % P.gsx, y = (h / P.gsx) % P.gsy, z = h / (P.gsx * P.gsy);
+    const uint32_t sx = x >> 1, sy = y >> 1, sz = z >> 1;
+    colour = (sx & 1u) | ((sy & 1u) << 1) | ((sz & 1u) << 2);
+    t = (sx >> 1) + (P.gsx >> 2) * ((sy >> 1) + (P.gsy >> 2) * (sz >> 1));
+}
+__device__ __forceinline__ void list_supercell(const DevParams& P, const SCList& sc, uint32_t h)
+{
+    uint32_t colour, t;
+    supercell_of(P, h, colour, t);
+    if (atomicCAS(sc.flag + colour * sc.per + t, 0u, 1u) == 0u)
+        sc.list[colour * sc.per + atomicAdd(sc.count + colour, 1u)] = t;
+}
+
 // L: the snow-snow candidate lists of the substep's first density pass (L.cnt null: none),
 // replayed instead of the traversal while no phase change re-sorted the sets.
 constexpr uint32_t LF_G = 4;
 __global__ void __launch_bounds__(256) k_link_filter(DevParams P, DevState* S, SetView vd,
                                                      snowb_particle_data dem, int dynamic,
-                                                     uint8_t* __restrict__ active, NList L)
+                                                     uint8_t* __restrict__ active, NList L, SCList sc)
 {
     const uint32_t nd = S->n_dem, M = P.maxc;
     vd.n = nd;
@@ -246,6 +273,7 @@ __global__ void __launch_bounds__(256) k_link_filter(DevParams P, DevState* S, S
         if (dem.iter_end[o] < o * M) {
             active[i] = 1;
             atomicAdd(&S->n_active, 1u);
+            if (sc.flag) list_supercell(P, sc, vd.gh[i]);
             continue;
         }
         // a particle at its cap stays inactive: its slots are not even read
@@ -330,7 +358,10 @@ __global__ void __launch_bounds__(256) k_link_filter(DevParams P, DevState* S, S
             }
         }
         active[i] = act;
-        if (act) atomicAdd(&S->n_active, 1u);
+        if (act) {
+            atomicAdd(&S->n_active, 1u);
+            if (sc.flag) list_supercell(P, sc, vd.gh[i]);
+        }
     }
 }
 // connect_and_record_cell (:4127-4252) + connect_and_record_d (:4255-4284) for one particle.
@@ -587,15 +618,18 @@ __device__ void link_particle_list(const DevParams& P, const SetView& vd, const 
 // they are valid while no phase change re-sorted the sets.
 __global__ void k_link_colour_warp(DevParams P, DevState* S, SetView vd, snowb_particle_data dem,
                                    const uint32_t* __restrict__ fs, const uint32_t* __restrict__ fe,
-                                   const uint8_t* __restrict__ active, uint32_t colour, int dynamic, NList L)
+                                   const uint8_t* __restrict__ active, uint32_t colour, int dynamic, NList L,
+                                   SCList sc)
 {
     vd.n = S->n_dem;
     const bool lists = L.cnt != nullptr && S->changed == 0;
     const uint32_t qx = P.gsx >> 2, qy = P.gsy >> 2, qz = P.gsz >> 2;
-    const uint32_t total = qx * qy * qz;
+    // the listed super-cells of this colour, or all of them
+    const uint32_t total = sc.flag ? sc.count[colour] : qx * qy * qz;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < total; t += nwarps) {
+    for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < total; w += nwarps) {
+        const uint32_t t = sc.flag ? sc.list[colour * sc.per + w] : w;
         const uint32_t sx = 2u * (t % qx) + (colour & 1u);
         const uint32_t sy = 2u * ((t / qx) % qy) + ((colour >> 1) & 1u);
         const uint32_t sz = 2u * (t / (qx * qy)) + ((colour >> 2) & 1u);
@@ -646,6 +680,7 @@ __global__ void k_link_colour_warp(DevParams P, DevState* S, SetView vd, snowb_p
                 else link_particle_list(P, vd, dem, ii, dynamic, S, L, lc & 1023u);
             }
         }
+        if (sc.flag && lane == 0) sc.flag[colour * sc.per + t] = 0u;   // ready for the next pass
     }
 }
 // general maximum_connection: the plain restatement with every access in memory

@@ -137,6 +137,7 @@ struct Ctx {
     uint32_t gen_cap = 0;
     uint32_t *fl_s = nullptr, *fl_d = nullptr, *rk_s = nullptr, *rk_d = nullptr, *sbsum = nullptr;
     uint8_t* active = nullptr;
+    uint32_t *sc_flag = nullptr, *sc_list = nullptr;   // link super-cell lists (SCList)
     uint32_t *fs = nullptr, *fe = nullptr;
     snowb_float3* tmp_vel = nullptr;
     uint32_t *nl_e = nullptr, *nl_cnt = nullptr;
@@ -164,7 +165,8 @@ static void free_ctx(Ctx& c)
     for (auto& s : c.s) free_set(s);
     free_set(c.b);
     free_set(c.gen);
-    void* ptrs[] = {c.fl_s, c.fl_d, c.rk_s, c.rk_d, c.sbsum, c.active, c.fs, c.fe, c.tmp_vel, c.epart, c.eout,
+    void* ptrs[] = {c.fl_s, c.fl_d, c.rk_s, c.rk_d, c.sbsum, c.active, c.sc_flag, c.sc_list, c.fs, c.fe, c.tmp_vel,
+                    c.epart, c.eout,
                     c.S, c.err_dev, c.nl_e, c.nl_cnt};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -207,6 +209,8 @@ static int ensure_ctx(uint32_t full, uint32_t nb, uint32_t ncells)
     TRY(dalloc(&c.fl_s, c.cap)); TRY(dalloc(&c.fl_d, c.cap)); TRY(dalloc(&c.rk_s, c.cap)); TRY(dalloc(&c.rk_d, c.cap));
     TRY(dalloc(&c.sbsum, 4 * (c.cap / SCAN_CHUNK + 2)));
     TRY(dalloc(&c.active, c.cap));
+    TRY(dalloc(&c.sc_flag, ncells / 8 + 1)); TRY(dalloc(&c.sc_list, ncells / 8 + 1));
+    CUDA_TRY(cudaMemset(c.sc_flag, 0, sizeof(uint32_t) * (ncells / 8 + 1)));
     TRY(dalloc(&c.fs, ncells)); TRY(dalloc(&c.fe, ncells));
     TRY(dalloc(&c.tmp_vel, c.cap));
     TRY(dalloc(&c.nl_e, (size_t)NLIST_K * 2 * c.cap));
@@ -224,6 +228,12 @@ static int ensure_ctx(uint32_t full, uint32_t nb, uint32_t ncells)
     g_max_blocks = sms * 16;
     g_sms = sms;
     return SNOWB_OK;
+}
+// the link passes' super-cell lists (warp form only: maximum_connection <= SNOWB_MAXC_FAST)
+static SCList sc_lists(const DevParams& P)
+{
+    if (P.maxc > SNOWB_MAXC_FAST) return SCList{nullptr, nullptr, nullptr, 0u};
+    return SCList{g_ctx.sc_flag, g_ctx.sc_list, g_ctx.S->sc_count, P.ncells / 64u};
 }
 static int ensure_gen(uint32_t n, uint32_t ncells)
 {
@@ -548,6 +558,9 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
     Sorted sb{c.b.invm, nullptr, c.b.lambda, c.b.mass};
     StageFlags F{a.correct_dem, a.sph_sph, a.interlink, step_sph ? 1 : 0, step_dem ? 1 : 0};
     NList NL{c.nl_e, c.nl_cnt, 2 * cap, cap};
+    // the friction pass may replay the density+lambda lists when a contact (d <= 2r) after a
+    // move of at most FR_LIST_MOVE per particle was within h before it
+    const bool fr_lists = P.two_r + 2.f * FR_LIST_MOVE < 0.9f * P.h;
     const uint32_t* n_s = &S->n_sph;
     const uint32_t* n_d = &S->n_dem;
     const uint32_t work3 = 2 * full + a.nb;
@@ -631,12 +644,13 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
     }
     STOP(5);
     if (a.interlink) {
-        TLAUNCH(k_link_filter, 256, full, 128, P, S, vd, *a.dem, a.dynamic, c.active, NL);
+        const SCList scl = sc_lists(P);
+        TLAUNCH(k_link_filter, 256, full, 128, P, S, vd, *a.dem, a.dynamic, c.active, NL, scl);
         const uint32_t nsc = (P.gsx / 4) * (P.gsy / 4) * (P.gsz / 4);   // super-cells per colour
         for (uint32_t col = 0; col < 8; ++col) {
             if (P.maxc <= SNOWB_MAXC_FAST)
                 TLAUNCH(k_link_colour_warp, 256, (uint64_t)nsc * 32, 128, P, S, vd, *a.dem, c.s[1].off,
-                        c.s[1].off + 1, c.active, col, a.dynamic, NL);
+                        c.s[1].off + 1, c.active, col, a.dynamic, NL, scl);
             else
                 TLAUNCH(k_link_colour, 128, nsc, 64, P, S, vd, *a.dem, c.s[1].off, c.s[1].off + 1, c.active, col,
                         a.dynamic);
@@ -678,7 +692,7 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
         STOP(base + 6);
         if (a.friction && step_dem) {
             TRY(sort_pair(false));
-            TLAUNCH(k_friction, 256, full, 128, P, S, vd, vb, X, sd, sb);
+            TLAUNCH(k_friction, 256, full, 128, P, S, vd, vb, X, sd, sb, NL, fr_lists ? 1 : 0);
             TLAUNCH(k_apply, 1024, full, 256, P, S, vs, vd, X, 0, 1, track_s, track_d);
             dirty_d = true;
         }
@@ -1255,12 +1269,13 @@ static int connect_links(const DevParams& P, snowb_particle_data* dem, uint32_t 
     LAUNCH(k_boundary_prep, n, 256, dcd, dem->mass, dem->massInv, dem->mass, n, c.s[1].p4, c.s[1].invm, c.s[1].lambda,
            sid, sid ? c.s[1].sid : nullptr);
     SetView vd = make_view(dcd, c.s[1].p4, dem->mass, sid ? c.s[1].sid : nullptr);
-    LAUNCH(k_link_filter, n, 128, P, c.S, vd, *dem, dynamic, c.active, NList{nullptr, nullptr, 0u, 0u});
+    const SCList scl = sc_lists(P);
+    LAUNCH(k_link_filter, n, 128, P, c.S, vd, *dem, dynamic, c.active, NList{nullptr, nullptr, 0u, 0u}, scl);
     const uint32_t nsc = (P.gsx / 4) * (P.gsy / 4) * (P.gsz / 4);
     for (uint32_t col = 0; col < 8; ++col) {
         if (P.maxc <= SNOWB_MAXC_FAST)
             LAUNCH(k_link_colour_warp, (uint64_t)nsc * 32, 128, P, c.S, vd, *dem, c.fs, c.fe, c.active, col, dynamic,
-                   NList{nullptr, nullptr, 0u, 0u});
+                   NList{nullptr, nullptr, 0u, 0u}, scl);
         else
             LAUNCH(k_link_colour, nsc, 64, P, c.S, vd, *dem, c.fs, c.fe, c.active, col, dynamic);
     }

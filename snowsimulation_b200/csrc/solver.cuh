@@ -392,6 +392,7 @@ __global__ void __launch_bounds__(256) k_density(DevParams P, DevState* __restri
     const uint32_t ns = S->n_sph, nd = S->n_dem, nb = S->n_b;
     vs.n = ns; vd.n = nd; vb.n = nb;
     const float3 z = f3(0.f, 0.f, 0.f);
+    if (LAMBDA && blockIdx.x == 0 && threadIdx.x == 0) S->far_move = 0u;   // the lists are new
     GRID_LOOP(t, ns + nd + nb) {
         float rho, gs = dot3(z, z);
         const snowb_particle_data* D;
@@ -671,6 +672,13 @@ __global__ void __launch_bounds__(256) k_interlink(DevParams P, const DevState* 
     }
 }
 
+// The friction pass replays the density+lambda pass's neighbour lists when they still hold
+// every contact: the friction sort point kept the snow set's sort (same cells, same order)
+// and no snow particle moved more than FR_LIST_MOVE since the lists were built.  A pair
+// within 2r now was then within 2r + 2 FR_LIST_MOVE = 0.028 m < h of each other (r = 0.01,
+// h = 0.04; the bound is checked against the parameters on the host).
+constexpr float FR_LIST_MOVE = 0.004f;
+
 // ======================================================================= apply
 // apply_correction (:1342-1380); limits carry the reference's launch sizes (Q12).
 __device__ __forceinline__ uint32_t launch_limit(const DevParams& P, uint32_t n0, uint32_t n)
@@ -679,7 +687,7 @@ __device__ __forceinline__ uint32_t launch_limit(const DevParams& P, uint32_t n0
 }
 // ts, td: a particle that leaves its cell marks its set for a full sort at the next sort
 // point (key null: not tracked).
-__global__ void k_apply(DevParams P, const DevState* __restrict__ S, SetView vs, SetView vd, Sets X, int do_sph,
+__global__ void k_apply(DevParams P, DevState* __restrict__ S, SetView vs, SetView vd, Sets X, int do_sph,
                         int do_dem, SortTrack ts, SortTrack td)
 {
     const uint32_t ls = do_sph ? launch_limit(P, S->n0_sph, S->n_sph) : 0u;
@@ -690,12 +698,17 @@ __global__ void k_apply(DevParams P, const DevState* __restrict__ S, SetView vs,
         const SetView& v = w ? vs : vd;
         const snowb_particle_data& D = w ? X.sph : X.dem;
         const uint32_t o = v.gi[i];
-        float3 np = add3(xyz(v.p4[i]), sc3(P.sor, ldv3(D.correction, o)));
+        const float3 q = xyz(v.p4[i]);
+        float3 np = add3(q, sc3(P.sor, ldv3(D.correction, o)));
         st3(D.new_positions, o, np);
         st3(D.predict_positions, o, np);
         st3(D.correction, o, f3(0.f, 0.f, 0.f));
         const SortTrack& T = w ? ts : td;
         if (T.key) track_move(P, T, o, np, v.scene(i));
+        if (!w) {
+            const float3 dp = sub3(np, q);
+            if (!(dot3(dp, dp) <= FR_LIST_MOVE * FR_LIST_MOVE)) S->far_move = 1u;
+        }
     }
 }
 
@@ -723,21 +736,27 @@ __device__ __forceinline__ float3 friction_term(const DevParams& P, float3 dx, f
 // then evaluate the costly term together instead of once per lane that found a contact.
 // More than FR_K contacts fall back to the single traversal.
 constexpr uint32_t FR_K = 16;
+// lists: the replay of the neighbour lists is allowed (see FR_LIST_MOVE); each particle
+// then takes its snow and boundary contacts from its list entries, in list order, instead
+// of traversing the cells (same contacts, same order: the list holds every candidate with
+// d < h in traversal order with its cell).
 __global__ void __launch_bounds__(256) k_friction(DevParams P, const DevState* __restrict__ S, SetView vd, SetView vb,
-                                                  Sets X, Sorted sd, Sorted sb)
+                                                  Sets X, Sorted sd, Sorted sb, NList L, int lists)
 {
     __shared__ uint32_t rec_sh[FR_K * 256];
     uint32_t* const rec = rec_sh + threadIdx.x;     // entry k at rec[k * blockDim.x]
     const uint32_t bd = blockDim.x;
     vd.n = S->n_dem; vb.n = S->n_b;
     const uint32_t ld = launch_limit(P, S->n0_dem, S->n_dem);
+    const bool list_ok = lists && S->resort[1] == 0u && S->far_move == 0u;
     GRID_LOOP(i, ld) {
         const uint32_t o = vd.gi[i];
         float3 p = xyz(vd.p4[i]);
         float3 op0 = ldv3(X.dem.positions, o);
         const float w0 = X.dem.massInv[o];
-        GCell g = grid_pos(P, p, vd.scene(i));
-        const Nbhd nb = make_nbhd(P, g, p, P.r2_cull);
+        Seg so, sx, sbn;
+        const bool use_list = list_ok && segments(L, L.cap + i, so, sx, sbn);
+        const Nbhd nb = use_list ? Nbhd{} : make_nbhd(P, grid_pos(P, p, vd.scene(i)), p, P.r2_cull);
         float3 c = f3(0.f, 0.f, 0.f);
         // snow-snow contacts (current entries screened two at a time with packed arithmetic
         // against the slightly larger r2_cull, then the exact scalar test, as in the density
@@ -748,7 +767,13 @@ __global__ void __launch_bounds__(256) k_friction(DevParams P, const DevState* _
             if (n < FR_K) rec[n * bd] = j | (cell << 25);
             ++n;
         };
-        FOR27 {
+        if (use_list) {
+            for (uint32_t k = so.k0; k < so.k1; ++k) {
+                const uint32_t en = so.at(k), j = en & NL_J_MASK;
+                const float3 v = sub3(p, vd.pos(j));
+                if (dot3(v, v) < P.r2_le) record(j, (en >> 25) & 31u);
+            }
+        } else FOR27 {
             uint32_t s, e;
             if (vd.range_nb(nb, ox, oy, oz, s, e)) {
                 const uint32_t cell = (uint32_t)CELL27;
@@ -793,11 +818,12 @@ __global__ void __launch_bounds__(256) k_friction(DevParams P, const DevState* _
                 cs = add3(cs, friction_term(P, dx, w0, vd.attr(sd.invm, X.dem.massInv, j), sqrtf(d2), v));
             }
             if (cur != 0xFFu) c = add3(c, cs);
-        } else {
+        } else {   // more contacts than the record holds: the traversal evaluates them
+            const Nbhd nbf = use_list ? make_nbhd(P, grid_pos(P, p, vd.scene(i)), p, P.r2_cull) : nb;
             FOR27 {
                 float3 cs = f3(0.f, 0.f, 0.f);
                 uint32_t s, e;
-                if (vd.range_nb(nb, ox, oy, oz, s, e))
+                if (vd.range_nb(nbf, ox, oy, oz, s, e))
                     for (uint32_t j = s; j < e; ++j) {
                         if (j == i) continue;
                         float3 pp1 = vd.pos(j);
@@ -815,7 +841,13 @@ __global__ void __launch_bounds__(256) k_friction(DevParams P, const DevState* _
         }
         // snow-boundary contacts
         n = 0;
-        FOR27 {
+        if (use_list) {
+            for (uint32_t k = sbn.k0; k < sbn.k1; ++k) {
+                const uint32_t en = sbn.at(k), j = en & NL_J_MASK;
+                const float3 v = sub3(p, vb.pos(j));
+                if (dot3(v, v) < P.r2_le) record(j, (en >> 25) & 31u);
+            }
+        } else FOR27 {
             uint32_t s, e;
             if (vb.range_nb(nb, ox, oy, oz, s, e)) {
                 const uint32_t cell = (uint32_t)CELL27;
@@ -858,10 +890,11 @@ __global__ void __launch_bounds__(256) k_friction(DevParams P, const DevState* _
             }
             if (cur != 0xFFu) c = add3(c, cs);
         } else {
+            const Nbhd nbf = use_list ? make_nbhd(P, grid_pos(P, p, vd.scene(i)), p, P.r2_cull) : nb;
             FOR27 {
                 float3 cs = f3(0.f, 0.f, 0.f);
                 uint32_t s, e;
-                if (vb.range_nb(nb, ox, oy, oz, s, e))
+                if (vb.range_nb(nbf, ox, oy, oz, s, e))
                     for (uint32_t j = s; j < e; ++j) {
                         float3 v = sub3(p, vb.pos(j));
                         float d2 = dot3(v, v);
@@ -1217,6 +1250,7 @@ __global__ void k_set_state(DevState* S, uint32_t ns, uint32_t nd, uint32_t nb)
         S->tail_dirty = 1u;
         // ... and the particles: the first sort point of a call sorts both sets in full
         for (int k = 0; k < 2; ++k) { S->moved[k] = 1u; S->sorts_full[k] = 0u; S->sorts_kept[k] = 0u; }
+        for (int c = 0; c < 8; ++c) S->sc_count[c] = 0u;
     }
 }
 // batched runs: every live slot's scene id must name a scene of the batch
@@ -1236,6 +1270,7 @@ __global__ void k_begin_substep(DevState* S)
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         S->n0_sph = S->n_sph; S->n0_dem = S->n_dem;
         S->n_freeze = 0; S->n_melt = 0; S->changed = 0; S->n_active = 0; S->n_links = 0; S->n_nl_ovf = 0;
+        for (int c = 0; c < 8; ++c) S->sc_count[c] = 0u;
     }
 }
 

@@ -88,11 +88,11 @@ def test_config3_adjoint_matches_fp64_reference_gradient(cuda):
         return (_oracle_loss(w0, tp, v64, tx64, tT64) - _oracle_loss(w0, tm, v64, tx64, tT64)) / step
 
     rows = []
-    for name, eps, tol in (("k_water", 1e-3, 5e-3), ("k_snow", 1e-3, 5e-3), ("k_stretch", 1e-4, 1e-2)):
+    for name, eps, tol in (("k_water", 1e-3, 5e-3), ("k_snow", 1e-3, 5e-3), ("k_stretch", 1e-6, 2e-2)):
         k = PARAM_NAMES.index(name)
         fd = fd_param(k, eps)
         rows.append((name, float(g_th[k]), fd, abs(g_th[k] - fd) / abs(fd), tol))
-    e = 1e-3   # m/s along a seeded direction (the water starts at rest)
+    e = 1e-6   # m/s along a seeded direction (the water starts at rest)
     fd_v = (_oracle_loss(w0, theta0, v64 + e * direction, tx64, tT64)
             - _oracle_loss(w0, theta0, v64 - e * direction, tx64, tT64)) / (2 * e)
     ad_v = float((g_v * direction).sum())
