@@ -47,7 +47,10 @@ def kernel_bytes(name, n_water, n_snow, n_boundary):
         "k_lambda": p["L"] * (n_water + n_snow + n_boundary),
         "k_pbf": (p["P"] + p["X"]) * n_water + p["P"] * n_snow,
         "k_dem_corr": p["X"] * n_snow,
-        "k_interlink": p["I"] * n_snow,
+        # the interlink pass: the per-slot terms (25 slots x 8 B, the particle's position and
+        # inverse mass) and their sum into the correction (16 B read + 16 B written)
+        "k_link_terms": (p["I"] - 32) * n_snow,
+        "k_link_sum": 32 * n_snow,
         "k_friction": p["F"] * n_snow,
         "k_heat": p["H"] * (n_water + n_snow),
         "k_integrate": p["G"] * (n_water + n_snow),

@@ -38,6 +38,12 @@ struct DevParams {
     // walls at x = wx0, wx1 and z = wz0, wz1, floor at y = floor_y (the reference: +-1, 0)
     float wx0, wx1, wz0, wz1, floor_y;
     int quirks;
+    // scorr_coeff is +0 (the reference's setting) and the s_corr quotient stays finite: the
+    // s_corr term is then -0 at every distance inside the support (for dt > 0), and adding
+    // -0 leaves a sum unchanged, so the PBF passes do not evaluate it.  scorr_cpl_off: the
+    // same for the coupling term of the reference quirk mode, (-scorr_coeff * 0) * x^4 * dt^2,
+    // which is -0 whenever scorr_coeff has no sign bit and the quotient stays finite.
+    int scorr_off, scorr_cpl_off;
 };
 
 // Device-resident counters, one block per library context.
@@ -180,6 +186,34 @@ __device__ __forceinline__ float scorr_of(const DevParams& P, float d, float dt)
     float x = W_poly6(P, d) / P.scorr_div;
     float x4 = (x * x) * (x * x);
     return ((-P.scorr_coeff * x4) * dt) * dt;
+}
+// s_corr of the coupling term (:982-1034); the reference mode multiplies scorr_coeff by 0
+__device__ __forceinline__ float lam_scorr_cpl(const DevParams& P, float lsum, float d, float dt)
+{
+    const bool ref = P.quirks == SNOWB_QUIRKS_REFERENCE;
+    if ((ref ? P.scorr_cpl_off : P.scorr_off) && dt > 0.f) return lsum;
+    float x = W_poly6(P, d) / P.scorr_div;
+    float x4 = (x * x) * (x * x);
+    float sc = ref ? ((((-P.scorr_coeff) * 0.f) * x4) * dt) * dt : ((-P.scorr_coeff * x4) * dt) * dt;
+    return lsum + sc;
+}
+// (li + lj) + s_corr(d), the lambda factor of a PBF term
+__device__ __forceinline__ float lam_scorr(const DevParams& P, float lsum, float d, float dt)
+{
+    return (P.scorr_off && dt > 0.f) ? lsum : lsum + scorr_of(P, d, dt);
+}
+// W_poly6 and G_spiky for a distance that passed the exact support test (0 <= d < h): the
+// same operations without the range test
+__device__ __forceinline__ float W_poly6_in(const DevParams& P, float d)
+{
+    float h2 = P.h * P.h, d2 = d * d, q = h2 - d2;
+    float q3 = q * q * q;
+    return P.poly6 * q3;
+}
+__device__ __forceinline__ float3 G_spiky_in(const DevParams& P, float3 v, float d)
+{
+    float q = P.h - d, q2 = q * q;
+    return sc3(P.spiky_G * (q2 / (d + P.keps)), v);
 }
 
 // ------------------------------------------------------------------ grid :141-157

@@ -107,6 +107,16 @@ static DevParams derive(const snowb_sim_params& s)
     P.h2_cull = P.h2_lt * (1.f + 1e-5f);
     P.r2_cull = P.r2_le * (1.f + 1e-5f);
     P.quirks = SNOWB_QUIRKS_REFERENCE;
+    {   // the s_corr term is -0 inside the support when scorr_coeff is +0 and its quotient
+        // W / scorr_divisor (at most W(0) / scorr_divisor) stays finite to the fourth power
+        uint32_t bits;
+        std::memcpy(&bits, &s.scorr_coeff, sizeof bits);
+        const double xmax = (double)P.W0 / (double)s.scorr_divisor;
+        const bool finite = std::isfinite(s.scorr_coeff) && std::isfinite(s.scorr_divisor) && s.scorr_divisor > 0.f &&
+                            std::isfinite(xmax) && xmax * xmax * xmax * xmax < 1e30;
+        P.scorr_off = bits == 0u && finite;
+        P.scorr_cpl_off = (bits >> 31) == 0u && finite;
+    }
     return P;
 }
 
@@ -130,7 +140,7 @@ struct SetBufs {
 
 struct Ctx {
     int device = -1;
-    uint32_t cap = 0, bcap = 0, ncells = 0;
+    uint32_t cap = 0, bcap = 0, ncells = 0, maxc = 0;
     SetBufs s[2];          // 0 = water (SPH), 1 = snow (DEM)
     SetBufs b;             // boundary
     SetBufs gen;           // scratch for the standalone sort entry points
@@ -141,6 +151,7 @@ struct Ctx {
     uint32_t *fs = nullptr, *fe = nullptr;
     snowb_float3* tmp_vel = nullptr;
     uint32_t *nl_e = nullptr, *nl_cnt = nullptr;
+    float4* link_terms = nullptr;         // one interlink term per slot (k_link_terms)
     double* epart = nullptr;
     double* eout = nullptr;
     DevState* S = nullptr;
@@ -166,7 +177,7 @@ static void free_ctx(Ctx& c)
     free_set(c.b);
     free_set(c.gen);
     void* ptrs[] = {c.fl_s, c.fl_d, c.rk_s, c.rk_d, c.sbsum, c.active, c.sc_flag, c.sc_list, c.fs, c.fe, c.tmp_vel,
-                    c.epart, c.eout,
+                    c.epart, c.eout, c.link_terms,
                     c.S, c.err_dev, c.nl_e, c.nl_cnt};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -196,7 +207,8 @@ static int ensure_ctx(uint32_t full, uint32_t nb, uint32_t ncells)
     int dev = 0;
     CUDA_TRY(cudaGetDevice(&dev));
     Ctx& c = g_ctx;
-    if (c.device == dev && c.cap >= full && c.bcap >= nb && c.ncells == ncells) return SNOWB_OK;
+    const uint32_t maxc = g_sim.maximum_connection > 0 ? g_sim.maximum_connection : 1;
+    if (c.device == dev && c.cap >= full && c.bcap >= nb && c.ncells == ncells && c.maxc >= maxc) return SNOWB_OK;
     free_ctx(c);
     ++g_ctx_gen;
     c.device = dev;
@@ -215,6 +227,8 @@ static int ensure_ctx(uint32_t full, uint32_t nb, uint32_t ncells)
     TRY(dalloc(&c.tmp_vel, c.cap));
     TRY(dalloc(&c.nl_e, (size_t)NLIST_K * 2 * c.cap));
     TRY(dalloc(&c.nl_cnt, 2 * (size_t)c.cap));
+    c.maxc = maxc;
+    TRY(dalloc(&c.link_terms, (size_t)c.cap * maxc));
     TRY(dalloc(&c.epart, 4 * 1024)); TRY(dalloc(&c.eout, 4));
     TRY(dalloc(&c.S, 1)); TRY(dalloc(&c.err_dev, 1));
     CUDA_TRY(cudaMemset(c.S, 0, sizeof(DevState)));
@@ -424,6 +438,7 @@ struct StepArgs {
     int stop_after;
     const uint32_t *sid_sph, *sid_dem, *sid_bnd;   // batched runs: scene id per slot (else null)
     uint32_t* sid_buf;
+    int xsph_thread[2];   // XSPH of the water / snow set in the one-thread form (sizes at the call)
 };
 
 
@@ -680,7 +695,10 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
         TLAUNCH_IF(!ref, k_pbf, 256, 2 * full, 128, P, S, vs, vd, vb, X, ss, sd, sb, a.dt, F, NL);
         STOP(base + 3);
         TLAUNCH(k_dem_corr, 256, full, 128, P, S, vs, vd, vb, X, ss, sd, sb, F, NL);
-        if (a.interlink) TLAUNCH(k_interlink, 1024, full, 128, P, S, *a.dem);
+        if (a.interlink) {
+            TLAUNCH(k_link_terms, 256, (uint64_t)P.maxc * full, 256, P, S, *a.dem, c.link_terms);
+            TLAUNCH(k_link_sum, 256, full, 128, P, S, *a.dem, c.link_terms);
+        }
         STOP(base + 5);
         if (step_sph || step_dem) {
             TLAUNCH(k_apply, 1024, 2 * full, 256, P, S, vs, vd, X, step_sph ? 1 : 0, step_dem ? 1 : 0, track_s,
@@ -703,13 +721,20 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
     TAPE_HOOK(4, 0);
     STOP(90);
     // apply_XSPH_viscosity (:3663-3711), Jacobi
+    // both forms give the same results; the choice only follows the set sizes at the call
     if (step_sph) {
-        TLAUNCH(k_xsph_warp, 256, (uint64_t)full * 32, 128, P, S, vs, vd, *a.sph, *a.dem, 1, P.sph_visc, c.tmp_vel);
+        if (a.xsph_thread[0])
+            TLAUNCH(k_xsph_thread, 256, full, 128, P, S, vs, vd, *a.sph, *a.dem, 1, P.sph_visc, c.tmp_vel);
+        else
+            TLAUNCH(k_xsph_warp, 256, (uint64_t)full * 32, 128, P, S, vs, vd, *a.sph, *a.dem, 1, P.sph_visc, c.tmp_vel);
         LAUNCH(k_xsph_commit, full, 256, P, S, vs, 1, c.tmp_vel, a.sph->velocity);
     }
     TAPE_HOOK(5, 0);
     if (a.dem_visc && step_dem) {
-        TLAUNCH(k_xsph_warp, 256, (uint64_t)full * 32, 128, P, S, vd, vs, *a.dem, *a.sph, 0, P.dem_visc, c.tmp_vel);
+        if (a.xsph_thread[1])
+            TLAUNCH(k_xsph_thread, 256, full, 128, P, S, vd, vs, *a.dem, *a.sph, 0, P.dem_visc, c.tmp_vel);
+        else
+            TLAUNCH(k_xsph_warp, 256, (uint64_t)full * 32, 128, P, S, vd, vs, *a.dem, *a.sph, 0, P.dem_visc, c.tmp_vel);
         LAUNCH(k_xsph_commit, full, 256, P, S, vd, 0, c.tmp_vel, a.dem->velocity);
     }
     TAPE_HOOK(6, 0);
@@ -1154,10 +1179,15 @@ static int run_steps(snowb_particle_data* sph, uint32_t* sph_size, snowb_particl
     Ctx& c = g_ctx;
     if (g_tape.recording) TRY(tape_start_call(P, sph, *sph_size, dem, *dem_size, bnd, nb, full, bcd, dt, iterations,
                                               fl, opt, batch));
+    // XSPH's thread form for sets past XSPH_WARP_MAX (the snow set's reference-mode launch
+    // covers only the water set's launch size, Q6)
+    const uint32_t xs_s = *sph_size;
+    const uint32_t xs_d = opt.quirks == SNOWB_QUIRKS_REFERENCE ? umin32(coverage(*sph_size), *dem_size) : *dem_size;
     StepArgs a{sph, dem, bnd, buf, nb, full, scd, dcd, bcd, dt, iterations,
                fl[0], fl[1], fl[2], fl[3], fl[4], fl[5], fl[6], fl[7], fl[8], fl[9], fl[10], dTe, opt.stop_after,
                batch ? batch->scene_sph : nullptr, batch ? batch->scene_dem : nullptr,
-               batch ? batch->scene_boundary : nullptr, batch ? batch->scene_buffer : nullptr};
+               batch ? batch->scene_boundary : nullptr, batch ? batch->scene_buffer : nullptr,
+               {xs_s > XSPH_WARP_MAX ? 1 : 0, xs_d > XSPH_WARP_MAX ? 1 : 0}};
     LAUNCH1(k_set_state, c.S, *sph_size, *dem_size, nb);
     if (batch)
         LAUNCH(k_check_scenes, full > nb ? full : nb, 256, P, c.S, a.sid_sph, a.sid_dem, a.sid_bnd);

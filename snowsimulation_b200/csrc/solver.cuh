@@ -68,10 +68,9 @@ __device__ __forceinline__ float3 pbf_own_cell(const DevParams& P, const SetView
             float d2 = dot3(dv, dv);
             if (d2 < P.h2_lt) {
                 float d = sqrtf(d2);
-                float3 gr = G_spiky(P, dv, d);
-                float sc = scorr_of(P, d, dt);
+                float3 gr = G_spiky_in(P, dv, d);
                 float lj = v.attr(lam_s, lam_o, j), cj = v.attr(con_s, con_o, j);
-                cs = add3(cs, sc3(cj * ((li + lj) + sc), gr));
+                cs = add3(cs, sc3(cj * lam_scorr(P, li + lj, d, dt), gr));
             }
         }
     return cs;
@@ -95,9 +94,8 @@ __device__ __forceinline__ float3 pbf_bnd_cell(const DevParams& P, const SetView
             float d2 = dot3(dv, dv);
             if (d2 < P.h2_lt) {
                 float d = sqrtf(d2);
-                float3 gr = G_spiky(P, dv, d);
-                float sc = scorr_of(P, d, dt);
-                cs = add3(cs, sc3((li + v.attr(lam_s, lam_o, j)) + sc, gr));
+                float3 gr = G_spiky_in(P, dv, d);
+                cs = add3(cs, sc3(lam_scorr(P, li + v.attr(lam_s, lam_o, j), d, dt), gr));
             }
         }
     return cs;
@@ -125,11 +123,7 @@ __device__ __forceinline__ float3 pbf_cpl_cell(const DevParams& P, const SetView
             if (d2 < P.r2_le) {
                 float d = sqrtf(d2);
                 float3 gr = G_poly6(P, dv, d);
-                float x = W_poly6(P, d) / P.scorr_div;
-                float x4 = (x * x) * (x * x);
-                float sc = ref ? ((((-P.scorr_coeff) * 0.f) * x4) * dt) * dt
-                               : ((-P.scorr_coeff * x4) * dt) * dt;
-                cs = add3(cs, sc3((li + v.attr(lam_s, lam_o, j)) + sc, gr));
+                cs = add3(cs, sc3(lam_scorr_cpl(P, li + v.attr(lam_s, lam_o, j), d, dt), gr));
             }
         }
     return cs;
@@ -190,11 +184,10 @@ __device__ __forceinline__ float3 seg_pbf_own(const DevParams& P, float3 acc, co
         const uint32_t en = S.at(k), j = en & NL_J_MASK, cell = (en >> 25) & 31u;
         if (cell != cur) { if (cur != 0xFFu) acc = add3(acc, cs); cs = f3(0.f, 0.f, 0.f); cur = cell; }
         float3 dv = sub3(p, v.pos(j));
-        float d = sqrtf(dot3(dv, dv));
-        float3 gr = G_spiky(P, dv, d);
-        float sc = scorr_of(P, d, dt);
+        float d = sqrtf(dot3(dv, dv));   // a recorded candidate: d < h
+        float3 gr = G_spiky_in(P, dv, d);
         float lj = v.attr(lam_s, lam_o, j), cj = v.attr(con_s, con_o, j);
-        cs = add3(cs, sc3(cj * ((li + lj) + sc), gr));
+        cs = add3(cs, sc3(cj * lam_scorr(P, li + lj, d, dt), gr));
     }
     if (cur != 0xFFu) acc = add3(acc, cs);
     return acc;
@@ -208,10 +201,9 @@ __device__ __forceinline__ float3 seg_pbf_bnd(const DevParams& P, float3 acc, co
         const uint32_t en = S.at(k), j = en & NL_J_MASK, cell = (en >> 25) & 31u;
         if (cell != cur) { if (cur != 0xFFu) acc = add3(acc, cs); cs = f3(0.f, 0.f, 0.f); cur = cell; }
         float3 dv = sub3(p, v.pos(j));
-        float d = sqrtf(dot3(dv, dv));
-        float3 gr = G_spiky(P, dv, d);
-        float sc = scorr_of(P, d, dt);
-        cs = add3(cs, sc3((li + v.attr(lam_s, lam_o, j)) + sc, gr));
+        float d = sqrtf(dot3(dv, dv));   // a recorded candidate: d < h
+        float3 gr = G_spiky_in(P, dv, d);
+        cs = add3(cs, sc3(lam_scorr(P, li + v.attr(lam_s, lam_o, j), d, dt), gr));
     }
     if (cur != 0xFFu) acc = add3(acc, cs);
     return acc;
@@ -232,10 +224,7 @@ __device__ __forceinline__ float3 seg_pbf_cpl(const DevParams& P, float3 acc, co
         if (d2 < P.r2_le) {
             float d = sqrtf(d2);
             float3 gr = G_poly6(P, dv, d);
-            float x = W_poly6(P, d) / P.scorr_div;
-            float x4 = (x * x) * (x * x);
-            float sc = ref ? ((((-P.scorr_coeff) * 0.f) * x4) * dt) * dt : ((-P.scorr_coeff * x4) * dt) * dt;
-            cs = add3(cs, sc3((li + v.attr(lam_s, lam_o, j)) + sc, gr));
+            cs = add3(cs, sc3(lam_scorr_cpl(P, li + v.attr(lam_s, lam_o, j), d, dt), gr));
         }
     }
     if (cur != 0xFFu) acc = add3(acc, cs);
@@ -318,9 +307,9 @@ __device__ __forceinline__ void wg_term(const DevParams& P, float& cs, float& cg
     float d2 = dot3(dv, dv);
     if (d2 < P.h2_lt) {
         if (wr) wr->push(j, cell, set);
-        float d = sqrtf(d2);
+        float d = sqrtf(d2);   // d < h: d2 passed the exact support test
         float w = vol ? P.rho0 * q.w : q.w;
-        cs += w * W_poly6(P, d);
+        cs += w * W_poly6_in(P, d);
         if (LAMBDA) {
             float sc;
             if (mode == 0) sc = P.inv_rho0;
@@ -328,7 +317,7 @@ __device__ __forceinline__ void wg_term(const DevParams& P, float& cs, float& cg
                 float m = mode == 1 ? m_self : m_j;
                 sc = P.inv_rho0 * ((P.rho0 * q.w) / m);
             }
-            float3 gc = sc3(sc, G_spiky(P, dv, d));
+            float3 gc = sc3(sc, G_spiky_in(P, dv, d));
             cg += dot3(gc, gc);
         }
     }
@@ -579,7 +568,7 @@ __device__ __forceinline__ void delete_record(const snowb_particle_data& D, uint
 }
 // compute_dem_sph_distance_correction (:2112-2162) and compute_dem_distance_correction
 // (:1765-1834) for snow particle o, added to its correction in the reference's kernel
-// order (after the PBF pass; the interlink terms of k_interlink follow).
+// order (after the PBF pass; the interlink terms of k_link_sum follow).
 __global__ void __launch_bounds__(256) k_dem_corr(DevParams P, const DevState* __restrict__ S, SetView vs, SetView vd,
                                                   SetView vb, Sets X, Sorted ss, Sorted sd, Sorted sb, StageFlags F,
                                                   NList L)
@@ -615,57 +604,61 @@ __global__ void __launch_bounds__(256) k_dem_corr(DevParams P, const DevState* _
     (void)ns; (void)nb;
 }
 // solve_snow_interlink_constraint_d (:4742-4765) with compute_interlink_correction
-// (:4661-4739) per filled slot, one thread per snow particle in original order (consecutive
-// threads read consecutive slot blocks; linked partners are near in index), added to the
-// correction after the contact terms as in the reference.  Both ends of a link hold the same length and see the same distance, so whichever end breaks it first (delete_record),
-// neither adds a correction.  The particle's own position, inverse mass and k_ref * -w0 are
-// loaded once, and 1 / (w0 + w1) is kept while the partner's inverse mass repeats (the same
-// operands give the same quotient); every other operation is the reference's, in its order.
-__global__ void __launch_bounds__(256) k_interlink(DevParams P, const DevState* __restrict__ S,
-                                                   snowb_particle_data dem)
+// (:4661-4739), in two passes.  Each particle's slots are summed in slot order, which one
+// thread per particle walking its slots does with about 11 dependent link terms in a row
+// (a record load, the partner's position, a square root and four divisions each), so the
+// pass waited on memory.  Here k_link_terms evaluates every slot's term with one thread per
+// slot, all independent, and k_link_sum adds each particle's terms in slot order to its
+// correction, after the contact terms as in the reference.  Both ends of a link hold the
+// same length and see the same distance, so whichever end breaks it first (delete_record),
+// neither adds a correction; a slot whose record a partner has deleted adds nothing, and a
+// zero term added to the sum leaves it unchanged (the sum of nonzero terms is never -0), so
+// the result does not depend on which thread deletes first.
+__device__ __forceinline__ float3 link_term(const DevParams& P, const snowb_particle_data& D, uint32_t i0, uint32_t i1,
+                                           float L, uint32_t n)
+{
+    const float3 z = f3(0.f, 0.f, 0.f);
+    if (i0 == i1 || i0 >= n || i1 >= n || L == 0.f) return z;
+    const float3 v = sub3(ldv3(D.predict_positions, i0), ldv3(D.predict_positions, i1));
+    const float dist = len3(v);
+    if (dist > P.brk * L || dist > P.h) { delete_record(D, P.maxc, i0, i1); return z; }
+    const float w0 = D.massInv[i0], w1 = D.massInv[i1];
+    const float ws = w0 + w1, C = dist - L;
+    const float3 n3 = div3(v, dist + P.pbd_eps);
+    const float3 r = sc3(((P.k_ref * -w0) * (1.f / ws)) * C, n3);
+    // len3(r) > 1 without the square root: sqrtf is monotone and correctly rounded, and the
+    // smallest float whose root rounds above 1 is 1 + 2^-22, so the test is d2 > 1 + 2^-23
+    if (dot3(r, r) > 0x1.000002p+0f || nan3(r) || inf3(r)) return z;
+    return r;
+}
+// term of slot s: (x, y, z, 1) for a filled slot, w = 0 for an empty one
+__global__ void __launch_bounds__(256) k_link_terms(DevParams P, const DevState* __restrict__ S,
+                                                    snowb_particle_data dem, float4* __restrict__ terms)
+{
+    const uint32_t nd = S->n_dem, M = P.maxc;
+    // Plain (cached) loads: a record that a partner deletes during the pass is one whose term
+    // is zero at both ends, so whether this thread still sees it, or sees its length already
+    // zeroed, the term is the same zero.
+    GRID_LOOP(s, nd * M) {
+        const uint32_t j = dem.connect_record[s];
+        float4 t = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (j != SNOWB_UMAX) {
+            const float3 r = link_term(P, dem, s / M, j, dem.connect_length[s], nd);
+            t = make_float4(r.x, r.y, r.z, 1.f);
+        }
+        terms[s] = t;
+    }
+}
+__global__ void __launch_bounds__(256) k_link_sum(DevParams P, const DevState* __restrict__ S,
+                                                  snowb_particle_data dem, const float4* __restrict__ terms)
 {
     const uint32_t nd = S->n_dem, M = P.maxc;
     const float3 z = f3(0.f, 0.f, 0.f);
-    // Plain (cached) loads: a record that a partner deletes during the pass is one whose term
-    // is zero at both ends (same length, same distance), so whether this thread still sees it,
-    // or sees its length already zeroed, the term it adds is the same zero.
-    const uint32_t* rec = dem.connect_record;
-    const float* len = dem.connect_length;
     GRID_LOOP(o, nd) {
-        const float3 p0 = ldv3(dem.predict_positions, o);
-        const float w0 = dem.massInv[o];
-        const float kw0 = P.k_ref * -w0;
-        uint32_t w1_last = 0u;     // bits of the partner inverse mass inv_ws was taken for
-        float inv_ws = 0.f;
-        bool have_ws = false;
         float3 d = z;
         for (uint32_t s = M * o; s < M * (o + 1); ++s) {
-            const uint32_t j = rec[s];
-            if (j == SNOWB_UMAX) continue;   // an empty slot adds nothing
-            const float L = len[s];
-            float3 r = z;
-            if (!(o == j || j >= nd || L == 0.f)) {
-                const float3 v = sub3(p0, ldv3(dem.predict_positions, j));
-                const float dist = len3(v);
-                if (dist > P.brk * L || dist > P.h) {
-                    delete_record(dem, M, o, j);
-                } else {
-                    const float w1 = dem.massInv[j];
-                    if (!have_ws || __float_as_uint(w1) != w1_last) {
-                        inv_ws = 1.f / (w0 + w1);
-                        w1_last = __float_as_uint(w1);
-                        have_ws = true;
-                    }
-                    const float C = dist - L;
-                    const float3 n3 = div3(v, dist + P.pbd_eps);
-                    const float3 t = sc3((kw0 * inv_ws) * C, n3);
-                    // len3(t) > 1 without the square root: sqrtf is monotone and correctly
-                    // rounded, and the smallest float whose root rounds above 1 is 1 + 2^-22,
-                    // so the test is d2 > 1 + 2^-23
-                    if (!(dot3(t, t) > 0x1.000002p+0f) && !nan3(t) && !inf3(t)) r = t;
-                }
-            }
-            d = add3(d, r);
+            const float4 t = __ldg(terms + s);
+            if (t.w != 0.f) d = add3(d, xyz(t));
         }
         if (nan3(d)) d = z;
         st3(dem.correction, o, add3(ldv3(dem.correction, o), d));
@@ -1183,6 +1176,33 @@ __global__ void __launch_bounds__(256) k_xsph_warp(DevParams P, const DevState* 
     }
 }
 // write the Jacobi results back (only the processed particles)
+// The same sums with one thread per particle, for sets large enough to fill the GPU with
+// threads (the warp form's 27-way split then costs more than it hides): the cell partials
+// are added in the same cell order as warp_ordered_sum adds them.
+__global__ void __launch_bounds__(256) k_xsph_thread(DevParams P, const DevState* __restrict__ S, SetView vown,
+                                                     SetView voth, snowb_particle_data A, snowb_particle_data B,
+                                                     int own_is_sph, float visc, snowb_float3* __restrict__ out_vel)
+{
+    const uint32_t ns = S->n_sph, nd = S->n_dem;
+    vown.n = own_is_sph ? ns : nd;
+    voth.n = own_is_sph ? nd : ns;
+    const uint32_t limit = own_is_sph ? ns
+                         : (P.quirks == SNOWB_QUIRKS_REFERENCE ? umin32(coverage(ns), nd) : nd);
+    const float3 z = f3(0.f, 0.f, 0.f);
+    GRID_LOOP(i, limit) {
+        const uint32_t o = vown.gi[i];
+        const float3 p = xyz(vown.p4[i]);
+        const GCell g = grid_pos(P, p, vown.scene(i));
+        const float3 vi = ldv3(A.velocity, o);
+        float3 c = z;
+        FOR27 c = add3(c, xsph_cell(P, vown, A, A.velocity, p, g, ox, oy, oz, i, vi));
+        FOR27 c = add3(c, xsph_cell(P, voth, B, B.velocity, p, g, ox, oy, oz, SNOWB_UMAX, vi));
+        c = sc3(visc, c);
+        st3(out_vel, o, add3(vi, c));
+    }
+}
+// Sets processed by XSPH above this many particles take the one-thread form.
+constexpr uint32_t XSPH_WARP_MAX = 65536;
 __global__ void k_xsph_commit(DevParams P, const DevState* __restrict__ S, SetView vown, int own_is_sph,
                               const snowb_float3* __restrict__ in_vel, snowb_float3* __restrict__ vel)
 {

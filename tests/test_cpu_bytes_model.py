@@ -29,5 +29,6 @@ def test_one_entry_per_pass_kernel():
     # each stage's bytes belong to the kernel that runs it: contact and interlink are
     # separate launches
     assert bm.kernel_bytes("k_dem_corr", NW, NS, NB) == bm.PASS["X"] * NS
-    assert bm.kernel_bytes("k_interlink", NW, NS, NB) == bm.PASS["I"] * NS
+    assert (bm.kernel_bytes("k_link_terms", NW, NS, NB) + bm.kernel_bytes("k_link_sum", NW, NS, NB)
+            == bm.PASS["I"] * NS)
     assert bm.kernel_bytes("k_not_a_kernel", NW, NS, NB) is None

@@ -89,6 +89,16 @@ def test_config1_substep_bit_exact(cuda):
     _assert_same(o, g, "config1 substep")
 
 
+def test_config1_fixed_quirks_substeps_bit_exact(cuda):
+    """Config 1 in the fixed-quirk mode: the snow set's XSPH covers all 147,928 snow particles
+    (the reference mode limits it to the water set's launch size), which takes the one-thread
+    XSPH form above 65,536 particles."""
+    o, g = _pair(scene.config1(), QUIRKS_FIXED)
+    for k in range(2):
+        o.step(); g.step()
+        _assert_same(o, g, "config1 fixed, substep %d" % k)
+
+
 def test_multi_substep_call_matches_single_calls(cuda):
     """substeps=4 in one call (sizes kept on the device) equals four calls."""
     from snowsimulation_b200.world import Simulation
