@@ -69,7 +69,6 @@ struct DevState {
     // were built (set by k_apply, cleared by the density+lambda pass)
     uint32_t far_move;
     uint32_t sc_count[8];           // super-cells listed for each link colour (SCList)
-    uint32_t phase_prev;            // the previous substep's phase-change chain compacted the sets
 };
 #define SNOWB_DEVERR_SCATTER 1u
 #define SNOWB_DEVERR_SCENE 2u      // a batched scene id >= the scene count

@@ -4,9 +4,8 @@
 // Phase change.  The reference claims target slots with atomicAdd, so their order is
 // scheduling dependent (Q8); here a particle's target is its rank among the particles
 // changing phase (ascending index).  Compaction always runs in the reference; when no
-// particle changed phase it rewrites what the state already holds, so the chain's single
-// cooperative launch (k_phase_chain) ends after the predicates (no host round trip is
-// needed).
+// particle changed phase it is an identity, so every compaction kernel returns early
+// unless DevState::changed is set (no host round trip is needed).
 //
 // Interlink formation.  The reference lets every snow particle claim slots with atomics
 // while others read the same slots (Q10), so the topology depends on scheduling.  Here
@@ -20,7 +19,6 @@
 // links are never removed during the pass and counts only grow, so a particle whose
 // count already reaches its cap, or whose candidates are all linked already, is a no-op.
 #pragma once
-#include <cooperative_groups.h>
 #include "common.cuh"
 #include "sort.cuh"
 
@@ -62,245 +60,153 @@ __device__ __forceinline__ void reset_records(const snowb_particle_data& d, uint
     d.iter_end[t] = M * t;
 }
 
+// freeze / melt predicates (:4425, :4396)
+__global__ void k_phase_flags(DevParams P, const DevState* __restrict__ S, snowb_particle_data sph,
+                              snowb_particle_data dem, int freeze, int melt, uint32_t* __restrict__ fl_s,
+                              uint32_t* __restrict__ fl_d)
+{
+    const uint32_t ns = S->n_sph, nd = S->n_dem;
+    GRID_LOOP(t, ns + nd) {
+        if (t < ns) fl_s[t] = (freeze && sph.T[t] <= P.Tf && sph.contrib[t] >= 0.99f) ? 1u : 0u;
+        else {
+            const uint32_t i = t - ns;
+            fl_d[i] = (melt && dem.T[i] > P.Tf && dem.contrib[i] >= 0.99f) ? 1u : 0u;
+        }
+    }
+}
+__global__ void k_phase_count(DevState* S)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) S->changed = (S->n_freeze + S->n_melt) != 0u;
+}
+// freezing (:4416-4449) and melting (:4387-4414) with ranked targets
 // scene ids of batched runs travel with the particles (null pointers: one scene)
 struct SceneIds {
     uint32_t *sph, *dem, *buf;
 };
-
-// ============================================================ the phase-change chain
-// The whole chain above -- predicates, the ranks of the particles changing phase, their
-// moves, the predicate scans that define scan_index, record clean-up, the two-stage
-// compaction of each set, the tail clean-up, the new sizes and the record remap -- as one
-// cooperative launch whose stages are separated by grid barriers instead of launches.
-// After the predicates the grid knows whether anything changes: with no particle changing
-// phase, a clean tail and no compaction in the previous substep, every later stage would
-// rewrite what the state already holds (predicates 1 below n, 0 above; scan_index the
-// identity below n, 0 above; the same sizes), so the launch ends there.
-struct PhaseBufs {
-    uint32_t *fl_s, *fl_d, *rk_s, *rk_d;
-    uint32_t* bsum;      // four regions of `bstride` block sums, one per scan
-    uint32_t bstride;
-};
-// block sum of chunk c of in[0, n) (k_scan_sums for one chunk)
-__device__ __forceinline__ void chunk_sum(const uint32_t* in, uint32_t n, uint32_t c, uint32_t* bsum, uint32_t* sm)
+__global__ void k_phase_move(DevParams P, const DevState* __restrict__ S, snowb_particle_data sph,
+                             snowb_particle_data dem, const uint32_t* __restrict__ fl_s,
+                             const uint32_t* __restrict__ rk_s, const uint32_t* __restrict__ fl_d,
+                             const uint32_t* __restrict__ rk_d, SceneIds sc)
 {
-    const uint32_t base = c * SCAN_CHUNK + threadIdx.x * SCAN_ITEMS;
-    uint32_t s = 0;
-#pragma unroll
-    for (int k = 0; k < SCAN_ITEMS; ++k)
-        if (base + k < n) s += in[base + k];
-    s = warp_sum(s);
-    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = s;
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        uint32_t v = threadIdx.x < SCAN_TPB / 32 ? sm[threadIdx.x] : 0u;
-        v = warp_sum(v);
-        if (threadIdx.x == 0) bsum[c] = v;
-    }
-    __syncthreads();
-}
-// exclusive scan of chunk c of in[0, n) into out, total of all n into *total (k_scan_apply
-// for one chunk)
-__device__ __forceinline__ void chunk_apply(const uint32_t* in, uint32_t n, uint32_t c, const uint32_t* bsum,
-                                            uint32_t* out, uint32_t* total, uint32_t* sm, uint32_t* s_prefix)
-{
-    if (threadIdx.x < 32) {
-        const uint32_t pfx = prefix_of_blocks(bsum, c);
-        if (threadIdx.x == 0) *s_prefix = pfx;
-    }
-    const uint32_t base = c * SCAN_CHUNK + threadIdx.x * SCAN_ITEMS;
-    uint32_t v[SCAN_ITEMS], t = 0;
-#pragma unroll
-    for (int k = 0; k < SCAN_ITEMS; ++k) {
-        v[k] = base + k < n ? in[base + k] : 0u;
-        t += v[k];
-    }
-    uint32_t tot;
-    __syncthreads();
-    uint32_t ex = block_excl_scan(t, sm, tot) + *s_prefix;
-#pragma unroll
-    for (int k = 0; k < SCAN_ITEMS; ++k) {
-        if (base + k < n) {
-            out[base + k] = ex;
-            if (base + k == n - 1) *total = ex + v[k];
-        }
-        ex += v[k];
-    }
-    __syncthreads();
-}
-__device__ __forceinline__ uint32_t chunks_of(uint32_t n) { return (n + SCAN_CHUNK - 1) / SCAN_CHUNK; }
-
-// launched with SCAN_TPB threads per block and at most as many blocks as fit on the GPU at
-// once (a cooperative launch)
-__global__ void __launch_bounds__(SCAN_TPB) k_phase_chain(DevParams P, DevState* S, snowb_particle_data sph,
-                                                          snowb_particle_data dem, snowb_particle_data buf,
-                                                          uint32_t full, int freeze, int melt, PhaseBufs B,
-                                                          SceneIds sc, int rebase_dem)
-{
-    namespace cg = cooperative_groups;
-    cg::grid_group grid = cg::this_grid();
-    __shared__ uint32_t sm[SCAN_TPB / 32 + 1];
-    __shared__ uint32_t s_prefix;
+    if (S->changed == 0) return;
     const uint32_t ns = S->n_sph, nd = S->n_dem, M = P.maxc;
-    const uint32_t lane = threadIdx.x & 31u;
-    // freeze / melt predicates (:4425, :4396), counted one atomic per warp and kind
     GRID_LOOP(t, ns + nd) {
-        bool f = false, m = false;
         if (t < ns) {
-            f = freeze && sph.T[t] <= P.Tf && sph.contrib[t] >= 0.99f;
-            B.fl_s[t] = f ? 1u : 0u;
+            if (!fl_s[t]) continue;
+            const uint32_t i = t, tg = nd + rk_s[i];
+            sph.contrib[i] = 0.f;
+            copy_info(sph, dem, i, tg, M);
+            if (sc.sph) sc.dem[tg] = sc.sph[i];
+            sph.predicate[i] = 0; sph.trackId[i] = 0;
+            dem.predicate[tg] = 1;
+            reset_records(dem, tg, M);
         } else {
             const uint32_t i = t - ns;
-            m = melt && dem.T[i] > P.Tf && dem.contrib[i] >= 0.99f;
-            B.fl_d[i] = m ? 1u : 0u;
+            if (!fl_d[i]) continue;
+            const uint32_t tg = ns + rk_d[i];
+            dem.contrib[i] = 0.f;
+            copy_info(dem, sph, i, tg, M);
+            if (sc.sph) sc.sph[tg] = sc.dem[i];
+            dem.predicate[i] = 0; dem.trackId[i] = 0;
+            sph.predicate[tg] = 1;
         }
-        const uint32_t am = __activemask();
-        const uint32_t bf = __ballot_sync(am, f), bm = __ballot_sync(am, m);
-        if (lane == (uint32_t)(__ffs(am) - 1)) {
-            if (bf) atomicAdd(&S->n_freeze, (uint32_t)__popc(bf));
-            if (bm) atomicAdd(&S->n_melt, (uint32_t)__popc(bm));
-        }
     }
-    grid.sync();
-    const bool ch = (S->n_freeze + S->n_melt) != 0u;
-    const bool tail = S->tail_dirty != 0u;
-    if (!ch && !tail && S->phase_prev == 0u) {
-        if (blockIdx.x == 0 && threadIdx.x == 0) S->changed = 0u;
-        return;
-    }
-    // ranks among the particles changing phase (exclusive scans of the predicates)
-    uint32_t* bs0 = B.bsum;
-    uint32_t* bs1 = B.bsum + B.bstride;
-    uint32_t* bs2 = B.bsum + 2 * B.bstride;
-    uint32_t* bs3 = B.bsum + 3 * B.bstride;
-    const uint32_t c_s = chunks_of(ns), c_d = chunks_of(nd), c_f = chunks_of(full);
-    for (uint32_t c = blockIdx.x; c < c_s + c_d; c += gridDim.x) {
-        if (c < c_s) chunk_sum(B.fl_s, ns, c, bs0, sm);
-        else chunk_sum(B.fl_d, nd, c - c_s, bs1, sm);
-    }
-    grid.sync();
-    for (uint32_t c = blockIdx.x; c < c_s + c_d; c += gridDim.x) {
-        if (c < c_s) chunk_apply(B.fl_s, ns, c, bs0, B.rk_s, &S->n_freeze, sm, &s_prefix);
-        else chunk_apply(B.fl_d, nd, c - c_s, bs1, B.rk_d, &S->n_melt, sm, &s_prefix);
-    }
-    if (blockIdx.x == 0 && threadIdx.x == 0) S->changed = ch ? 1u : 0u;
-    grid.sync();
-    // freezing (:4416-4449) and melting (:4387-4414) with ranked targets
-    if (ch) {
-        GRID_LOOP(t, ns + nd) {
-            if (t < ns) {
-                if (!B.fl_s[t]) continue;
-                const uint32_t i = t, tg = nd + B.rk_s[i];
-                sph.contrib[i] = 0.f;
-                copy_info(sph, dem, i, tg, M);
-                if (sc.sph) sc.dem[tg] = sc.sph[i];
-                sph.predicate[i] = 0; sph.trackId[i] = 0;
-                dem.predicate[tg] = 1;
-                reset_records(dem, tg, M);
-            } else {
-                const uint32_t i = t - ns;
-                if (!B.fl_d[i]) continue;
-                const uint32_t tg = ns + B.rk_d[i];
-                dem.contrib[i] = 0.f;
-                copy_info(dem, sph, i, tg, M);
-                if (sc.sph) sc.sph[tg] = sc.dem[i];
-                dem.predicate[i] = 0; dem.trackId[i] = 0;
-                sph.predicate[tg] = 1;
+}
+// shuffle_useless_record (:4068-4111): drop links to particles that left the snow set
+__global__ void k_shuffle_records(DevParams P, const DevState* __restrict__ S, snowb_particle_data dem)
+{
+    if (S->changed == 0) return;
+    const uint32_t nd = S->n_dem, M = P.maxc;
+    GRID_LOOP(i, nd) {
+        for (uint32_t s = M * i; s < (i + 1) * M; ++s) {
+            const uint32_t r = dem.connect_record[s];
+            if (r < nd && dem.predicate[r] == 0) {
+                dem.connect_record[s] = SNOWB_UMAX;
+                dem.connect_length[s] = 0.f;
+                dem.iter_end[i]--;
             }
         }
-        grid.sync();
     }
-    // compact_and_clean (:4495-4589): the predicate scans define scan_index
-    for (uint32_t c = blockIdx.x; c < 2 * c_f; c += gridDim.x) {
-        if (c < c_f) chunk_sum(sph.predicate, full, c, bs2, sm);
-        else chunk_sum(dem.predicate, full, c - c_f, bs3, sm);
+}
+// copy_to_target (:4451-4460) into the caller's phase-change buffer
+__global__ void k_copy_to_buffer(DevParams P, const DevState* __restrict__ S, snowb_particle_data d,
+                                 snowb_particle_data buf, uint32_t full, const uint32_t* __restrict__ sid,
+                                 uint32_t* __restrict__ sid_buf)
+{
+    if (S->changed == 0) return;
+    GRID_LOOP(i, full) {
+        copy_info(d, buf, i, i, P.maxc);
+        if (sid) sid_buf[i] = sid[i];
     }
-    grid.sync();
-    for (uint32_t c = blockIdx.x; c < 2 * c_f; c += gridDim.x) {
-        if (c < c_f) chunk_apply(sph.predicate, full, c, bs2, sph.scan_index, &S->new_sph, sm, &s_prefix);
-        else chunk_apply(dem.predicate, full, c - c_f, bs3, dem.scan_index, &S->new_dem, sm, &s_prefix);
+}
+// scatter (:4462-4480).  rebase (fixed quirks, snow set): a moved particle keeps its link
+// count, iter_end = t*M + count; the reference copies iter_end verbatim (Q13).
+__global__ void k_scatter_set(DevParams P, DevState* S, snowb_particle_data d, snowb_particle_data buf, uint32_t full,
+                              uint32_t* __restrict__ sid, const uint32_t* __restrict__ sid_buf, int rebase)
+{
+    if (S->changed == 0) return;
+    GRID_LOOP(i, full) {
+        if (d.predicate[i] == 1) {
+            const uint32_t t = d.scan_index[i];
+            if (t >= full) { atomicOr(&S->err, SNOWB_DEVERR_SCATTER); continue; }
+            copy_info(buf, d, i, t, P.maxc);
+            if (rebase) d.iter_end[t] = P.maxc * t + (buf.iter_end[i] - P.maxc * i);
+            if (sid) sid[t] = sid_buf[i];
+            d.new_index[i] = t;
+        } else d.new_index[i] = SNOWB_UMAX;
     }
-    grid.sync();
-    if (ch) {
-        // shuffle_useless_record (:4068-4111): drop links to particles that left the snow set
-        GRID_LOOP(i, nd) {
-            for (uint32_t s = M * i; s < (i + 1) * M; ++s) {
-                const uint32_t r = dem.connect_record[s];
-                if (r < nd && dem.predicate[r] == 0) {
-                    dem.connect_record[s] = SNOWB_UMAX;
-                    dem.connect_length[s] = 0.f;
-                    dem.iter_end[i]--;
-                }
+}
+// setSize / new_end (:4545-4551), predicate fill (:4555-4556), clean_tail (:4482-4493).
+// The reference compacts every substep; without a phase change that is an identity except
+// that it zeroes scan_index in the tail and, if a link pass wrote into tail slots, resets
+// them (`full_clean`), which is what this kernel does in that case.
+__global__ void k_compact_finish(DevParams P, DevState* S, snowb_particle_data sph, snowb_particle_data dem,
+                                 uint32_t full)
+{
+    const bool full_clean = S->changed || S->tail_dirty;
+    const uint32_t sn = S->new_sph, dn = S->new_dem, M = P.maxc;
+    GRID_LOOP(t, 2 * full) {
+        const bool w = t < full;
+        const uint32_t i = w ? t : t - full;
+        const snowb_particle_data& d = w ? sph : dem;
+        const uint32_t n = w ? sn : dn;
+        if (i < n) {
+            if (full_clean) d.predicate[i] = 1;
+        } else {
+            d.scan_index[i] = 0;
+            if (full_clean) {
+                d.predicate[i] = 0; d.trackId[i] = 0;
+                reset_records(d, i, M);
             }
         }
-        grid.sync();
-        // copy_to_target (:4451-4460) and scatter (:4462-4480), water then snow, through the
-        // caller's phase-change buffer
-        for (int set = 0; set < 2; ++set) {
-            const snowb_particle_data& d = set ? dem : sph;
-            uint32_t* sid = set ? sc.dem : sc.sph;
-            GRID_LOOP(i, full) {
-                copy_info(d, buf, i, i, M);
-                if (sid) sc.buf[i] = sid[i];
-            }
-            grid.sync();
-            const int rebase = set ? rebase_dem : 0;
-            GRID_LOOP(i, full) {
-                if (d.predicate[i] == 1) {
-                    const uint32_t t = d.scan_index[i];
-                    if (t >= full) { atomicOr(&S->err, SNOWB_DEVERR_SCATTER); continue; }
-                    copy_info(buf, d, i, t, M);
-                    if (rebase) d.iter_end[t] = M * t + (buf.iter_end[i] - M * i);
-                    if (sid) sid[t] = sc.buf[i];
-                    d.new_index[i] = t;
-                } else d.new_index[i] = SNOWB_UMAX;
-            }
-            grid.sync();
-        }
+        if (i == 0 && full_clean) *d.new_end = n;
     }
-    // setSize / new_end, predicate fill, clean_tail (k_compact_finish)
-    {
-        const bool full_clean = ch || tail;
-        const uint32_t sn = S->new_sph, dn = S->new_dem;
-        GRID_LOOP(t, 2 * full) {
-            const bool w = t < full;
-            const uint32_t i = w ? t : t - full;
-            const snowb_particle_data& d = w ? sph : dem;
-            const uint32_t n = w ? sn : dn;
-            if (i < n) {
-                if (full_clean) d.predicate[i] = 1;
-            } else {
-                d.scan_index[i] = 0;
-                if (full_clean) {
-                    d.predicate[i] = 0; d.trackId[i] = 0;
-                    reset_records(d, i, M);
-                }
-            }
-            if (i == 0 && full_clean) *d.new_end = n;
-        }
-    }
-    grid.sync();
-    if (ch && blockIdx.x == 0 && threadIdx.x == 0) {   // the new sizes (:4545-4546)
+}
+__global__ void k_commit_sizes(DevState* S)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0 && S->changed) {
         S->n_sph = S->new_sph; S->n_dem = S->new_dem;
         S->moved[0] = 1u; S->moved[1] = 1u;   // compacted sets: sort both in full
     }
-    grid.sync();
-    // update_record_index (:4114-4125); without a phase change only a dirty tail needs it
-    if (ch || tail) {
-        const uint32_t ndn = S->n_dem, total = M * ndn;
-        GRID_LOOP(s, total) {
-            const uint32_t r = dem.connect_record[s];
-            if (r != SNOWB_UMAX) dem.connect_record[s] = ch ? dem.new_index[r] : (r < ndn ? r : SNOWB_UMAX);
-        }
-    }
-    grid.sync();
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        S->tail_dirty = 0u;
-        S->phase_prev = ch ? 1u : 0u;
+}
+__global__ void k_clear_tail_flag(DevState* S)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) S->tail_dirty = 0;
+}
+// update_record_index (:4114-4125)
+__global__ void k_update_records(DevParams P, const DevState* __restrict__ S, snowb_particle_data dem)
+{
+    if (S->changed == 0 && S->tail_dirty == 0) return;
+    // without a phase change the reference's new_index is the identity below n, empty above
+    const bool moved = S->changed != 0;
+    const uint32_t nd = S->n_dem, total = P.maxc * nd;
+    GRID_LOOP(s, total) {
+        const uint32_t r = dem.connect_record[s];
+        if (r != SNOWB_UMAX) dem.connect_record[s] = moved ? dem.new_index[r] : (r < nd ? r : SNOWB_UMAX);
     }
 }
 
-// ======================================================================= links// ======================================================================= links
+// ======================================================================= links
 __device__ __forceinline__ uint32_t link_tolerance(const DevParams& P, float T, int dynamic)
 {
     uint32_t tol = dynamic ? __float2uint_rz(((T - P.Tf) / (P.Th - P.Tf)) * (float)P.maxc) : P.maxc;

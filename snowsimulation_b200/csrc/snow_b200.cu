@@ -386,37 +386,15 @@ static void tune_pick(const char* name, uint64_t work, int tpb0, int max_tpb, in
     } while (0)
 #define LAUNCH1(kernel, ...) KL(kernel, 1, 32, __VA_ARGS__)
 
+static inline unsigned scan_blocks(uint32_t n) { return (n + SCAN_CHUNK - 1) / SCAN_CHUNK + (n == 0); }
 
-// k_phase_chain as a cooperative launch: SCAN_TPB threads per block, as many blocks as fit
-// on the GPU at once (its stages wait for each other at grid barriers)
-static int g_phase_blocks = 0;
-static int launch_phase_chain(const DevParams& P, DevState* S, snowb_particle_data sph, snowb_particle_data dem,
-                              snowb_particle_data buf, uint32_t full, int freeze, int melt, PhaseBufs pb,
-                              SceneIds scn, int rebase_dem)
+// exclusive scan of in[0, n) (n from the device when n_ptr is set; `cap` bounds it)
+static int scan(const uint32_t* in, const uint32_t* n_ptr, uint32_t n_fixed, uint32_t cap, uint32_t* bsum,
+                uint32_t* out, uint32_t* total, const uint32_t* cond)
 {
-    if (g_phase_blocks == 0) {
-        int per_sm = 0;
-        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_phase_chain, SCAN_TPB, 0));
-        if (per_sm < 1) return fail(SNOWB_ERR_CUDA, "k_phase_chain does not fit on a multiprocessor");
-        g_phase_blocks = per_sm * g_sms;
-    }
-    uint64_t want = (2ull * full + SCAN_TPB - 1) / SCAN_TPB;
-    if (want < 1) want = 1;
-    const unsigned grid = (unsigned)(want < (uint64_t)g_phase_blocks ? want : (uint64_t)g_phase_blocks);
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(SCAN_TPB);
-    cfg.stream = g_stream;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeCooperative;
-    at[0].val.cooperative = 1;
-    cfg.attrs = at;
-    cfg.numAttrs = 1;
-    prof_begin("k_phase_chain");
-    const cudaError_t e = cudaLaunchKernelEx(&cfg, k_phase_chain, P, S, sph, dem, buf, full, freeze, melt, pb, scn,
-                                             rebase_dem);
-    prof_end();
-    if (e != cudaSuccess) return fail(SNOWB_ERR_CUDA, std::string("k_phase_chain: ") + cudaGetErrorString(e));
+    const uint32_t nb = scan_blocks(n_ptr ? cap : n_fixed);
+    KL(k_scan_sums, nb, SCAN_TPB, in, n_ptr, n_fixed, bsum, cond);
+    KL(k_scan_apply, nb, SCAN_TPB, in, n_ptr, n_fixed, bsum, out, total, cond);
     return SNOWB_OK;
 }
 
@@ -620,10 +598,10 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
     // latency-bound launches overlaps the large one's.  after_phase: the sort point after
     // the phase change, where only a compaction (which marks both sets moved) alters the
     // result.
-    auto sort_pair = [&](bool after_phase, bool begin = false) -> int {
+    auto sort_pair = [&](bool after_phase) -> int {
         const bool need_s = dirty_s || after_phase, need_d = dirty_d || after_phase;
         if (!need_s && !need_d) return SNOWB_OK;
-        LAUNCH1(k_sort_gate, S, (need_s ? 1u : 0u) | (need_d ? 2u : 0u), begin ? 1 : 0);
+        LAUNCH1(k_sort_gate, S, (need_s ? 1u : 0u) | (need_d ? 2u : 0u));
         const cudaStream_t main_stream = g_stream;
         if (need_s) {
             CUDA_TRY(cudaEventRecord(c.fork, main_stream));
@@ -644,7 +622,8 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
 #define STOP(k) do { if (a.stop_after == (k)) return SNOWB_OK; } while (0)
 
     TAPE_HOOK(0, 0);
-    TRY(sort_pair(false, true));   // its gate also opens the substep (both sets are dirty here)
+    LAUNCH1(k_begin_substep, S);
+    TRY(sort_pair(false));
     STOP(1);
     TLAUNCH(k_density<false>, 256, work3, 128, P, S, vs, vd, vb, X, ss, sd, sb, NL);
     STOP(2);
@@ -654,10 +633,25 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
     }
     STOP(3);
     if (a.change_phase) {
-        // the whole chain in one cooperative launch (k_phase_chain)
+        LAUNCH(k_phase_flags, 2 * full, 256, P, S, *a.sph, *a.dem, a.freezing, a.melting, c.fl_s, c.fl_d);
         const uint32_t sb_stride = cap / SCAN_CHUNK + 2;
-        const PhaseBufs pb{c.fl_s, c.fl_d, c.rk_s, c.rk_d, c.sbsum, sb_stride};
-        TRY(launch_phase_chain(P, S, *a.sph, *a.dem, *a.buf, full, a.freezing, a.melting, pb, scn, ref ? 0 : 1));
+        TRY(scan(c.fl_s, n_s, 0, cap, c.sbsum, c.rk_s, &S->n_freeze, nullptr));
+        TRY(scan(c.fl_d, n_d, 0, cap, c.sbsum + sb_stride, c.rk_d, &S->n_melt, nullptr));
+        LAUNCH1(k_phase_count, S);
+        LAUNCH(k_phase_move, 2 * full, 256, P, S, *a.sph, *a.dem, c.fl_s, c.rk_s, c.fl_d, c.rk_d, scn);
+        // compact_and_clean (:4495-4589): predicate scans run every substep (they define
+        // scan_index), the data movement only after a phase change.
+        TRY(scan(a.sph->predicate, nullptr, full, full, c.sbsum, a.sph->scan_index, &S->new_sph, nullptr));
+        TRY(scan(a.dem->predicate, nullptr, full, full, c.sbsum + sb_stride, a.dem->scan_index, &S->new_dem, nullptr));
+        LAUNCH(k_shuffle_records, full, 256, P, S, *a.dem);
+        LAUNCH(k_copy_to_buffer, full, 256, P, S, *a.sph, *a.buf, full, scn.sph, scn.buf);
+        LAUNCH(k_scatter_set, full, 256, P, S, *a.sph, *a.buf, full, scn.sph, scn.buf, 0);
+        LAUNCH(k_copy_to_buffer, full, 256, P, S, *a.dem, *a.buf, full, scn.dem, scn.buf);
+        LAUNCH(k_scatter_set, full, 256, P, S, *a.dem, *a.buf, full, scn.dem, scn.buf, ref ? 0 : 1);
+        LAUNCH(k_compact_finish, 2 * full, 256, P, S, *a.sph, *a.dem, full);
+        LAUNCH1(k_commit_sizes, S);
+        LAUNCH(k_update_records, (uint64_t)P.maxc * full, 256, P, S, *a.dem);
+        LAUNCH1(k_clear_tail_flag, S);
     }
     STOP(4);
     if (a.change_phase) {   // the reference sorts again; only a phase change alters the result

@@ -1271,7 +1271,6 @@ __global__ void k_set_state(DevState* S, uint32_t ns, uint32_t nd, uint32_t nb)
         // ... and the particles: the first sort point of a call sorts both sets in full
         for (int k = 0; k < 2; ++k) { S->moved[k] = 1u; S->sorts_full[k] = 0u; S->sorts_kept[k] = 0u; }
         for (int c = 0; c < 8; ++c) S->sc_count[c] = 0u;
-        S->phase_prev = 0u;
     }
 }
 // batched runs: every live slot's scene id must name a scene of the batch
@@ -1284,6 +1283,14 @@ __global__ void k_check_scenes(DevParams P, DevState* S, const uint32_t* __restr
         bool bad = (i < ns && sph[i] > P.scene_mask) || (i < nd && dem[i] > P.scene_mask) ||
                    (i < nb && bnd[i] > P.scene_mask);
         if (bad) atomicOr(&S->err, SNOWB_DEVERR_SCENE);
+    }
+}
+__global__ void k_begin_substep(DevState* S)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        S->n0_sph = S->n_sph; S->n0_dem = S->n_dem;
+        S->n_freeze = 0; S->n_melt = 0; S->changed = 0; S->n_active = 0; S->n_links = 0; S->n_nl_ovf = 0;
+        for (int c = 0; c < 8; ++c) S->sc_count[c] = 0u;
     }
 }
 

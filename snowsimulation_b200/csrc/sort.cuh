@@ -231,23 +231,13 @@ __global__ void k_rank_reorder(const uint32_t* __restrict__ key_o, const uint32_
         if (sid_s) sid_s[p] = sid_o[o];
     }
 }
-// substep start: launch sizes, phase-change and link counters
-__device__ __forceinline__ void begin_substep(DevState* S)
-{
-    S->n0_sph = S->n_sph; S->n0_dem = S->n_dem;
-    S->n_freeze = 0; S->n_melt = 0; S->changed = 0; S->n_active = 0; S->n_links = 0; S->n_nl_ovf = 0;
-    for (int c = 0; c < 8; ++c) S->sc_count[c] = 0u;
-}
 // Decision of one sort point for the sets in `sets` (bit k: set k is sorted here): a set
 // whose particles all kept their cells since its last sort (moved[k] clear) keeps its
 // permutation and cell table: the hash, scan and scatter launches return at once and
 // k_rank_reorder only refreshes the gathered outputs.  moved[k] is consumed; the writers
 // set it again.
-// begin: the first sort point of a substep, which also opens the substep (the launch sizes
-// and the per-substep counters, begin_substep).
-__global__ void k_sort_gate(DevState* S, uint32_t sets, int begin)
+__global__ void k_sort_gate(DevState* S, uint32_t sets)
 {
-    if (blockIdx.x == 0 && threadIdx.x == 0 && begin) begin_substep(S);
     if (blockIdx.x == 0 && threadIdx.x == 0)
         for (int k = 0; k < 2; ++k)
             if ((sets >> k) & 1u) {
@@ -318,6 +308,64 @@ __global__ void k_fresh_ranges(const uint32_t* __restrict__ hash, uint32_t n, ui
         const uint32_t h = hash[i];
         if (i == 0 || hash[i - 1] != h) fs[h] = i;
         if (i == n - 1 || hash[i + 1] != h) fe[h] = i + 1;
+    }
+}
+
+// ------------------------------------------------------------------ generic scan
+// Exclusive scan of in[0, n) into out (n from device or fixed), total into *total.
+__global__ void k_scan_sums(const uint32_t* __restrict__ in, const uint32_t* n_ptr, uint32_t n_fixed,
+                            uint32_t* __restrict__ bsum, const uint32_t* cond)
+{
+    if (cond && *cond == 0) return;
+    const uint32_t n = n_ptr ? *n_ptr : n_fixed;
+    __shared__ uint32_t sm[SCAN_TPB / 32];
+    const uint32_t base = blockIdx.x * SCAN_CHUNK + threadIdx.x * SCAN_ITEMS;
+    if (blockIdx.x * SCAN_CHUNK >= n && blockIdx.x != 0) { if (threadIdx.x == 0) bsum[blockIdx.x] = 0; return; }
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k)
+        if (base + k < n) s += in[base + k];
+    s = warp_sum(s);
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        uint32_t v = threadIdx.x < SCAN_TPB / 32 ? sm[threadIdx.x] : 0u;
+        v = warp_sum(v);
+        if (threadIdx.x == 0) bsum[blockIdx.x] = v;
+    }
+}
+__global__ void k_scan_apply(const uint32_t* __restrict__ in, const uint32_t* n_ptr, uint32_t n_fixed,
+                             const uint32_t* __restrict__ bsum, uint32_t* __restrict__ out, uint32_t* total,
+                             const uint32_t* cond)
+{
+    if (cond && *cond == 0) return;
+    const uint32_t n = n_ptr ? *n_ptr : n_fixed;
+    const uint32_t nblocks = (n + SCAN_CHUNK - 1) / SCAN_CHUNK;
+    if (n == 0) { if (blockIdx.x == 0 && threadIdx.x == 0 && total) *total = 0; return; }
+    if (blockIdx.x >= nblocks) return;
+    __shared__ uint32_t sm[SCAN_TPB / 32 + 1];
+    __shared__ uint32_t s_prefix;
+    if (threadIdx.x < 32) {
+        uint32_t p = prefix_of_blocks(bsum, blockIdx.x);
+        if (threadIdx.x == 0) s_prefix = p;
+    }
+    const uint32_t base = blockIdx.x * SCAN_CHUNK + threadIdx.x * SCAN_ITEMS;
+    uint32_t v[SCAN_ITEMS], t = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+        v[k] = base + k < n ? in[base + k] : 0u;
+        t += v[k];
+    }
+    uint32_t tot;
+    __syncthreads();
+    uint32_t ex = block_excl_scan(t, sm, tot) + s_prefix;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+        if (base + k < n) {
+            if (out) out[base + k] = ex;
+            if (base + k == n - 1 && total) *total = ex + v[k];
+        }
+        ex += v[k];
     }
 }
 
