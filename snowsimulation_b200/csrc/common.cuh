@@ -62,7 +62,8 @@ struct DevState {
     // Sort skipping.  moved[k]: set k must be sorted in full at its next sort point (a
     // particle's cell differs from its key at the set's last sort, the set was compacted, or
     // a call started).  resort[k]: the decision of the current sort point, taken from moved
-    // by k_sort_gate.  sorts_full/sorts_kept count the decisions since the call started.
+    // by the set's hash pass.  sorts_full/sorts_kept count the decisions since the call
+    // started.
     uint32_t moved[2], resort[2];
     uint32_t sorts_full[2], sorts_kept[2];
     // a snow particle moved more than FR_LIST_MOVE since the iteration's neighbour lists

@@ -400,15 +400,19 @@ static int scan(const uint32_t* in, const uint32_t* n_ptr, uint32_t n_fixed, uin
 
 // hash + stable sort + reorder of one set (sort_and_reorder :398-420), writing the
 // caller's cell data and the compact sorted copies.  cond: skip unless *cond != 0.
+// gate.S set: a sort point of the substep, which decides for itself whether the set keeps
+// its last sort (cond then points at that decision, DevState::resort)
 static int sort_set(const DevParams& P, SetBufs& B, const snowb_particle_data& D, const snowb_cell_data& cd,
                     const uint32_t* n_ptr, uint32_t cap, const uint32_t* cond, bool clear_all,
-                    const uint32_t* sid_o = nullptr)
+                    const uint32_t* sid_o = nullptr, SortGate gate = SortGate{nullptr, 0, 0})
 {
     const uint32_t nc = P.ncells;
     const unsigned nb = (nc + SCAN_CHUNK - 1) / SCAN_CHUNK;
     // chunk counts come from the hash pass (bsum is all zero between sorts)
-    LAUNCH(k_hash_count, cap, 256, P, D.predict_positions, n_ptr, 0u, B.key, B.slot, B.cnt, cond, sid_o, B.bsum);
-    KL(k_cell_scan, nb, SCAN_TPB, B.cnt, B.bsum, nc, B.off, cd.cell_start, n_ptr, 0u, clear_all ? 1 : 0, cond);
+    LAUNCH(k_hash_count, cap, 256, P, D.predict_positions, n_ptr, 0u, B.key, B.slot, B.cnt, cond, sid_o, B.bsum,
+           gate);
+    KL(k_cell_scan, nb, SCAN_TPB, B.cnt, B.bsum, nc, B.off, cd.cell_start, n_ptr, 0u, clear_all ? 1 : 0, cond,
+       gate.S ? &gate.S->moved[gate.set] : nullptr);
     LAUNCH(k_scatter, cap, 256, B.key, B.slot, B.off, B.tmp, n_ptr, 0u, cond, B.bsum, nb);
     LAUNCH(k_rank_reorder, cap, 256, B.key, B.off, B.tmp, D.predict_positions, D.mass, D.massInv, D.contrib, cd, B.p4,
            B.invm, B.contrib, n_ptr, 0u, cond, sid_o, sid_o ? B.sid : nullptr);
@@ -580,17 +584,18 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
     const uint32_t* n_d = &S->n_dem;
     const uint32_t work3 = 2 * full + a.nb;
     // dirty_*: the host knows the set may have moved since its last sort (no launch at all
-    // otherwise).  On the device, k_sort_gate turns the writers' moved flags into the sort
-    // point's decision: a set whose particles all kept their cells keeps its sort outputs
-    // (the writers updated its sorted copies) and its sort launches return at once.
+    // otherwise).  On the device, each sort point's hash pass turns the writers' moved flag
+    // into the decision: a set whose particles all kept their cells keeps its permutation and
+    // cell table, its hash, scan and scatter launches return at once and the rank pass only
+    // refreshes the gathered outputs.
     bool dirty_s = true, dirty_d = true;
     auto track = [&](int set) { return SortTrack{c.s[set].key, set ? a.sid_dem : a.sid_sph, &S->moved[set]}; };
     const SortTrack track_s = track(0), track_d = track(1);
-    // a sort point of one set: the full sort when the gate's decision is set, else only the
-    // refresh of the gathered outputs (the hash, scan and scatter launches return at once)
-    auto sort_if = [&](int set) -> int {
+    // a sort point of one set: the full sort when the set moved, else only the refresh of the
+    // gathered outputs
+    auto sort_if = [&](int set, bool begin) -> int {
         TRY(sort_set(P, c.s[set], set ? *a.dem : *a.sph, set ? a.dcd : a.scd, set ? n_d : n_s, cap, &S->resort[set],
-                     !ref, set ? a.sid_dem : a.sid_sph));
+                     !ref, set ? a.sid_dem : a.sid_sph, SortGate{S, set, begin ? 1 : 0}));
         return SNOWB_OK;
     };
     // The two sets' sorts share no buffer: the water sort runs on a side stream beside the
@@ -598,20 +603,21 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
     // latency-bound launches overlaps the large one's.  after_phase: the sort point after
     // the phase change, where only a compaction (which marks both sets moved) alters the
     // result.
-    auto sort_pair = [&](bool after_phase) -> int {
+    // begin: the substep's first sort point, whose snow hash pass also opens the substep
+    // (both sets are dirty there)
+    auto sort_pair = [&](bool after_phase, bool begin = false) -> int {
         const bool need_s = dirty_s || after_phase, need_d = dirty_d || after_phase;
         if (!need_s && !need_d) return SNOWB_OK;
-        LAUNCH1(k_sort_gate, S, (need_s ? 1u : 0u) | (need_d ? 2u : 0u));
         const cudaStream_t main_stream = g_stream;
         if (need_s) {
             CUDA_TRY(cudaEventRecord(c.fork, main_stream));
             CUDA_TRY(cudaStreamWaitEvent(c.side, c.fork, 0));
             g_stream = c.side;
-            const int rc = sort_if(0);
+            const int rc = sort_if(0, false);
             g_stream = main_stream;
             TRY(rc);
         }
-        if (need_d) TRY(sort_if(1));
+        if (need_d) TRY(sort_if(1, begin));
         if (need_s) {
             CUDA_TRY(cudaEventRecord(c.join, c.side));
             CUDA_TRY(cudaStreamWaitEvent(main_stream, c.join, 0));
@@ -622,8 +628,7 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
 #define STOP(k) do { if (a.stop_after == (k)) return SNOWB_OK; } while (0)
 
     TAPE_HOOK(0, 0);
-    LAUNCH1(k_begin_substep, S);
-    TRY(sort_pair(false));
+    TRY(sort_pair(false, true));
     STOP(1);
     TLAUNCH(k_density<false>, 256, work3, 128, P, S, vs, vd, vb, X, ss, sd, sb, NL);
     STOP(2);

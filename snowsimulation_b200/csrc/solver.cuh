@@ -1285,14 +1285,6 @@ __global__ void k_check_scenes(DevParams P, DevState* S, const uint32_t* __restr
         if (bad) atomicOr(&S->err, SNOWB_DEVERR_SCENE);
     }
 }
-__global__ void k_begin_substep(DevState* S)
-{
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        S->n0_sph = S->n_sph; S->n0_dem = S->n_dem;
-        S->n_freeze = 0; S->n_melt = 0; S->changed = 0; S->n_active = 0; S->n_links = 0; S->n_nl_ovf = 0;
-        for (int c = 0; c < 8; ++c) S->sc_count[c] = 0u;
-    }
-}
 
 // FP64 heat-energy and momentum partial sums (deterministic two-level reduction)
 __global__ void k_energy_partial(const snowb_particle_data sph, uint32_t ns, const snowb_particle_data dem,

@@ -71,12 +71,36 @@ __device__ __forceinline__ uint32_t prefix_of_blocks(const uint32_t* bsum, uint3
 // Fused path: hash of pos[o] for o < n (calcHashD :194-212).  Also adds every particle to
 // the count of its scan chunk (bsum, SCAN_CHUNK cells each, one atomic per chunk and warp),
 // which the cell scan needs; the scatter pass re-zeroes bsum for the next sort.
+// Sort points of a substep decide for themselves (gate.S set): the hash pass turns the
+// set's moved flag into the decision (DevState::resort, read by the later passes; the scan
+// pass clears the flag), and returns at once when the set keeps its last sort.  The first
+// sort point of a substep also opens it (begin).  gate.S null: `cond` alone decides.
+struct SortGate {
+    DevState* S;
+    int set, begin;
+};
+// substep start: launch sizes, phase-change and link counters
+__device__ __forceinline__ void begin_substep(DevState* S)
+{
+    S->n0_sph = S->n_sph; S->n0_dem = S->n_dem;
+    S->n_freeze = 0; S->n_melt = 0; S->changed = 0; S->n_active = 0; S->n_links = 0; S->n_nl_ovf = 0;
+    for (int c = 0; c < 8; ++c) S->sc_count[c] = 0u;
+}
 __global__ void k_hash_count(DevParams P, const snowb_float3* __restrict__ pos, const uint32_t* n_ptr,
                              uint32_t n_fixed, uint32_t* __restrict__ key_o, uint32_t* __restrict__ slot_o,
                              uint32_t* __restrict__ cnt, const uint32_t* cond, const uint32_t* __restrict__ sid_o,
-                             uint32_t* __restrict__ bsum)
+                             uint32_t* __restrict__ bsum, SortGate gate)
 {
-    if (cond && *cond == 0) return;
+    if (gate.S) {
+        const uint32_t m = gate.S->moved[gate.set];
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            if (gate.begin) begin_substep(gate.S);
+            gate.S->resort[gate.set] = m;
+            if (m) ++gate.S->sorts_full[gate.set];
+            else ++gate.S->sorts_kept[gate.set];
+        }
+        if (m == 0) return;
+    } else if (cond && *cond == 0) return;
     const uint32_t n = n_ptr ? *n_ptr : n_fixed;
     const uint32_t lane = threadIdx.x & 31u;
     // whole warps iterate together so the chunk counts can be aggregated with warp votes
@@ -133,10 +157,13 @@ __global__ void k_block_sums(const uint32_t* __restrict__ cnt, uint32_t ncells, 
 
 // off[c] = exclusive prefix of cnt; off[ncells] = total; cnt re-zeroed; cell_start cleared
 // for c < clear (clear = min(n, ncells) reproduces the reference's partial memset, Q1).
+// moved: the set's moved flag, cleared here once the hash pass has read it (null: none)
 __global__ void k_cell_scan(uint32_t* __restrict__ cnt, const uint32_t* __restrict__ bsum, uint32_t ncells,
                             uint32_t* __restrict__ off, uint32_t* __restrict__ cell_start,
-                            const uint32_t* n_ptr, uint32_t n_fixed, int clear_all, const uint32_t* cond)
+                            const uint32_t* n_ptr, uint32_t n_fixed, int clear_all, const uint32_t* cond,
+                            uint32_t* moved = nullptr)
 {
+    if (moved && blockIdx.x == 0 && threadIdx.x == 0) *moved = 0u;
     if (cond && *cond == 0) return;
     __shared__ uint32_t sm[SCAN_TPB / 32 + 1];
     __shared__ uint32_t s_prefix;
@@ -231,24 +258,6 @@ __global__ void k_rank_reorder(const uint32_t* __restrict__ key_o, const uint32_
         if (sid_s) sid_s[p] = sid_o[o];
     }
 }
-// Decision of one sort point for the sets in `sets` (bit k: set k is sorted here): a set
-// whose particles all kept their cells since its last sort (moved[k] clear) keeps its
-// permutation and cell table: the hash, scan and scatter launches return at once and
-// k_rank_reorder only refreshes the gathered outputs.  moved[k] is consumed; the writers
-// set it again.
-__global__ void k_sort_gate(DevState* S, uint32_t sets)
-{
-    if (blockIdx.x == 0 && threadIdx.x == 0)
-        for (int k = 0; k < 2; ++k)
-            if ((sets >> k) & 1u) {
-                const uint32_t m = S->moved[k];
-                S->resort[k] = m;
-                S->moved[k] = 0u;
-                if (m) ++S->sorts_full[k];
-                else ++S->sorts_kept[k];
-            }
-}
-
 // A set whose particles all kept their cells since its last sort sorts to the same
 // permutation and cell table, so only the gathered outputs change: the kernels that move
 // particles compare each new cell with the particle's key at the last sort and mark the
