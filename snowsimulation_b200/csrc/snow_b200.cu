@@ -159,6 +159,8 @@ struct Ctx {
     uint32_t* err_dev = nullptr;
     cudaStream_t side = nullptr;          // second stream for the water sort (see sort_pair)
     cudaEvent_t fork = nullptr, join = nullptr;
+    cudaStream_t side2 = nullptr;         // third stream (the water PBF pass beside the snow passes)
+    cudaEvent_t fork2 = nullptr, join2 = nullptr;
 };
 static Ctx g_ctx;
 static uint64_t g_ctx_gen = 0;   // bumped whenever the scratch buffers are (re)allocated
@@ -185,6 +187,9 @@ static void free_ctx(Ctx& c)
     if (c.side) cudaStreamDestroy(c.side);
     if (c.fork) cudaEventDestroy(c.fork);
     if (c.join) cudaEventDestroy(c.join);
+    if (c.side2) cudaStreamDestroy(c.side2);
+    if (c.fork2) cudaEventDestroy(c.fork2);
+    if (c.join2) cudaEventDestroy(c.join2);
     c = Ctx();
 }
 static int alloc_sort(SetBufs& s, uint32_t cap, uint32_t ncells, bool attrs)
@@ -237,6 +242,9 @@ static int ensure_ctx(uint32_t full, uint32_t nb, uint32_t ncells)
     CUDA_TRY(cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking));
     CUDA_TRY(cudaEventCreateWithFlags(&c.fork, cudaEventDisableTiming));
     CUDA_TRY(cudaEventCreateWithFlags(&c.join, cudaEventDisableTiming));
+    CUDA_TRY(cudaStreamCreateWithFlags(&c.side2, cudaStreamNonBlocking));
+    CUDA_TRY(cudaEventCreateWithFlags(&c.fork2, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventCreateWithFlags(&c.join2, cudaEventDisableTiming));
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     g_max_blocks = sms * 16;
@@ -625,6 +633,27 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
         dirty_s = dirty_d = false;
         return SNOWB_OK;
     };
+    // launches on a side stream forked from the main one; join_side makes the main stream
+    // wait for them
+    auto on_side = [&](cudaStream_t st, cudaEvent_t ev, auto&& launch) -> int {
+        const cudaStream_t main_stream = g_stream;
+        CUDA_TRY(cudaEventRecord(ev, main_stream));
+        CUDA_TRY(cudaStreamWaitEvent(st, ev, 0));
+        g_stream = st;
+        const int rc = launch();
+        g_stream = main_stream;
+        return rc;
+    };
+    auto join_side = [&](cudaStream_t st, cudaEvent_t ev) -> int {
+        CUDA_TRY(cudaEventRecord(ev, st));
+        CUDA_TRY(cudaStreamWaitEvent(g_stream, ev, 0));
+        return SNOWB_OK;
+    };
+    // Inside an iteration the water PBF pass (water corrections) and the interlink terms (the
+    // per-slot term buffer, link deletions) share no buffer with the density, snow PBF and
+    // contact passes, so they run beside them on the side streams when the substep runs
+    // whole (a stage stop keeps every launch on the main stream).
+    const bool beside = a.stop_after == 0;
 #define STOP(k) do { if (a.stop_after == (k)) return SNOWB_OK; } while (0)
 
     TAPE_HOOK(0, 0);
@@ -691,19 +720,33 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
         TRY(sort_pair(false));
         TAPE_HOOK(2, it);
         STOP(base + 0);
+        // the interlink terms read the predicted positions and the link records only
+        auto link_terms = [&]() -> int {
+            TLAUNCH(k_link_terms, 256, (uint64_t)P.maxc * full, 256, P, S, *a.dem, c.link_terms);
+            return SNOWB_OK;
+        };
+        const bool links_beside = beside && a.interlink;
+        if (links_beside) TRY(on_side(c.side, c.fork, link_terms));
         // density + lambda in one pass (stage boundaries base+1 and base+2 coincide)
         TLAUNCH(k_density<true>, 256, work3, 128, P, S, vs, vd, vb, X, ss, sd, sb, NL);
         STOP(base + 2);
+        auto pbf_water = [&]() -> int {
+            TLAUNCH(k_pbf_water_warp, 256, (uint64_t)full * 32, 128, P, S, vs, vd, vb, X, ss, sd, sb, a.dt, F);
+            return SNOWB_OK;
+        };
+        if (beside) TRY(on_side(c.side2, c.fork2, pbf_water));
+        else TRY(pbf_water());
         // the reference's snow PBF pass adds into repeated targets with float atomics (Q3):
         // its order follows the launch shape, so that pass keeps the built-in shape
-        TLAUNCH(k_pbf_water_warp, 256, (uint64_t)full * 32, 128, P, S, vs, vd, vb, X, ss, sd, sb, a.dt, F);
         TLAUNCH_IF(!ref, k_pbf, 256, 2 * full, 128, P, S, vs, vd, vb, X, ss, sd, sb, a.dt, F, NL);
         STOP(base + 3);
         TLAUNCH(k_dem_corr, 256, full, 128, P, S, vs, vd, vb, X, ss, sd, sb, F, NL);
         if (a.interlink) {
-            TLAUNCH(k_link_terms, 256, (uint64_t)P.maxc * full, 256, P, S, *a.dem, c.link_terms);
+            if (links_beside) TRY(join_side(c.side, c.join));
+            else TRY(link_terms());
             TLAUNCH(k_link_sum, 256, full, 128, P, S, *a.dem, c.link_terms);
         }
+        if (beside) TRY(join_side(c.side2, c.join2));
         STOP(base + 5);
         if (step_sph || step_dem) {
             TLAUNCH(k_apply, 1024, 2 * full, 256, P, S, vs, vd, X, step_sph ? 1 : 0, step_dem ? 1 : 0, track_s,
