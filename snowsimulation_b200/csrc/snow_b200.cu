@@ -606,33 +606,6 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
                      !ref, set ? a.sid_dem : a.sid_sph, SortGate{S, set, begin ? 1 : 0}));
         return SNOWB_OK;
     };
-    // The two sets' sorts share no buffer: the water sort runs on a side stream beside the
-    // snow sort (a fork and a join of the captured graph), so the small set's chain of
-    // latency-bound launches overlaps the large one's.  after_phase: the sort point after
-    // the phase change, where only a compaction (which marks both sets moved) alters the
-    // result.
-    // begin: the substep's first sort point, whose snow hash pass also opens the substep
-    // (both sets are dirty there)
-    auto sort_pair = [&](bool after_phase, bool begin = false) -> int {
-        const bool need_s = dirty_s || after_phase, need_d = dirty_d || after_phase;
-        if (!need_s && !need_d) return SNOWB_OK;
-        const cudaStream_t main_stream = g_stream;
-        if (need_s) {
-            CUDA_TRY(cudaEventRecord(c.fork, main_stream));
-            CUDA_TRY(cudaStreamWaitEvent(c.side, c.fork, 0));
-            g_stream = c.side;
-            const int rc = sort_if(0, false);
-            g_stream = main_stream;
-            TRY(rc);
-        }
-        if (need_d) TRY(sort_if(1, begin));
-        if (need_s) {
-            CUDA_TRY(cudaEventRecord(c.join, c.side));
-            CUDA_TRY(cudaStreamWaitEvent(main_stream, c.join, 0));
-        }
-        dirty_s = dirty_d = false;
-        return SNOWB_OK;
-    };
     // launches on a side stream forked from the main one; join_side makes the main stream
     // wait for them
     auto on_side = [&](cudaStream_t st, cudaEvent_t ev, auto&& launch) -> int {
@@ -654,12 +627,46 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
     // contact passes, so they run beside them on the side streams when the substep runs
     // whole (a stage stop keeps every launch on the main stream).
     const bool beside = a.stop_after == 0;
+    // The two sets' sorts share no buffer: the water sort runs on a side stream beside the
+    // snow sort (a fork and a join of the captured graph), so the small set's chain of
+    // latency-bound launches overlaps the large one's.  after_phase: the sort point after
+    // the phase change, where only a compaction (which marks both sets moved) alters the
+    // result.
+    // begin: the substep's first sort point, whose snow hash pass also opens the substep
+    // (both sets are dirty there)
+    // defer_water: the friction sort point, whose passes read no water data: its water sort
+    // stays on the side stream beside the friction and apply passes, joined by the next
+    // sort point or by join_water
+    bool water_pending = false;
+    auto join_water = [&]() -> int {
+        if (water_pending) TRY(join_side(c.side, c.join));
+        water_pending = false;
+        return SNOWB_OK;
+    };
+    auto sort_pair = [&](bool after_phase, bool begin = false, bool defer_water = false) -> int {
+        TRY(join_water());
+        const bool need_s = dirty_s || after_phase, need_d = dirty_d || after_phase;
+        if (!need_s && !need_d) return SNOWB_OK;
+        if (need_s) TRY(on_side(c.side, c.fork, [&]() { return sort_if(0, false); }));
+        if (need_d) TRY(sort_if(1, begin));
+        if (need_s) {
+            if (defer_water) water_pending = true;
+            else TRY(join_side(c.side, c.join));
+        }
+        dirty_s = dirty_d = false;
+        return SNOWB_OK;
+    };
 #define STOP(k) do { if (a.stop_after == (k)) return SNOWB_OK; } while (0)
 
     TAPE_HOOK(0, 0);
     TRY(sort_pair(false, true));
     STOP(1);
-    TLAUNCH(k_density<false>, 256, work3, 128, P, S, vs, vd, vb, X, ss, sd, sb, NL);
+    // The substep's first density pass feeds the heat pass and the link formation, which
+    // read the water and snow densities only; the boundary's values are rewritten by the
+    // iterations' density+lambda passes before anything reads them, so a whole substep with
+    // iterations leaves the boundary out here.
+    const int bnd_first = !(beside && a.iterations > 0);
+    TLAUNCH(k_density<false>, 256, bnd_first ? work3 : 2 * full, 128, P, S, vs, vd, vb, X, ss, sd, sb, NL, bnd_first);
     STOP(2);
     if (a.temperature) {
         TLAUNCH(k_heat, 256, 2 * full, 128, P, S, vs, vd, X, a.dt);
@@ -728,7 +735,7 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
         const bool links_beside = beside && a.interlink;
         if (links_beside) TRY(on_side(c.side, c.fork, link_terms));
         // density + lambda in one pass (stage boundaries base+1 and base+2 coincide)
-        TLAUNCH(k_density<true>, 256, work3, 128, P, S, vs, vd, vb, X, ss, sd, sb, NL);
+        TLAUNCH(k_density<true>, 256, work3, 128, P, S, vs, vd, vb, X, ss, sd, sb, NL, 1);
         STOP(base + 2);
         auto pbf_water = [&]() -> int {
             TLAUNCH(k_pbf_water_warp, 256, (uint64_t)full * 32, 128, P, S, vs, vd, vb, X, ss, sd, sb, a.dt, F);
@@ -757,13 +764,14 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
         TAPE_HOOK(3, it);
         STOP(base + 6);
         if (a.friction && step_dem) {
-            TRY(sort_pair(false));
+            TRY(sort_pair(false, false, beside));
             TLAUNCH(k_friction, 256, full, 128, P, S, vd, vb, X, sd, sb, NL, fr_lists ? 1 : 0);
             TLAUNCH(k_apply, 1024, full, 256, P, S, vs, vd, X, 0, 1, track_s, track_d);
             dirty_d = true;
         }
         STOP(base + 7);
     }
+    TRY(join_water());
     if (step_sph || step_dem)
         LAUNCH(k_finalize, 2 * full, 256, P, S, X, a.dt, step_sph ? 1 : 0, step_dem ? 1 : 0);
     TAPE_HOOK(4, 0);
