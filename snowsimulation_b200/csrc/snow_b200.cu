@@ -152,6 +152,7 @@ struct Ctx {
     snowb_float3* tmp_vel = nullptr;
     uint32_t *nl_e = nullptr, *nl_cnt = nullptr;
     float4* link_terms = nullptr;         // one interlink term per slot (k_link_terms)
+    float4* contact = nullptr;            // two snow contact sums per particle (k_dem_corr<true>)
     double* epart = nullptr;
     double* eout = nullptr;
     DevState* S = nullptr;
@@ -161,6 +162,8 @@ struct Ctx {
     cudaEvent_t fork = nullptr, join = nullptr;
     cudaStream_t side2 = nullptr;         // third stream (the water PBF pass beside the snow passes)
     cudaEvent_t fork2 = nullptr, join2 = nullptr;
+    cudaStream_t side3 = nullptr;         // fourth stream (the snow contact sums beside the snow PBF pass)
+    cudaEvent_t fork3 = nullptr, join3 = nullptr;
 };
 static Ctx g_ctx;
 static uint64_t g_ctx_gen = 0;   // bumped whenever the scratch buffers are (re)allocated
@@ -179,7 +182,7 @@ static void free_ctx(Ctx& c)
     free_set(c.b);
     free_set(c.gen);
     void* ptrs[] = {c.fl_s, c.fl_d, c.rk_s, c.rk_d, c.sbsum, c.active, c.sc_flag, c.sc_list, c.fs, c.fe, c.tmp_vel,
-                    c.epart, c.eout, c.link_terms,
+                    c.epart, c.eout, c.link_terms, c.contact,
                     c.S, c.err_dev, c.nl_e, c.nl_cnt};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -190,6 +193,9 @@ static void free_ctx(Ctx& c)
     if (c.side2) cudaStreamDestroy(c.side2);
     if (c.fork2) cudaEventDestroy(c.fork2);
     if (c.join2) cudaEventDestroy(c.join2);
+    if (c.side3) cudaStreamDestroy(c.side3);
+    if (c.fork3) cudaEventDestroy(c.fork3);
+    if (c.join3) cudaEventDestroy(c.join3);
     c = Ctx();
 }
 static int alloc_sort(SetBufs& s, uint32_t cap, uint32_t ncells, bool attrs)
@@ -234,6 +240,7 @@ static int ensure_ctx(uint32_t full, uint32_t nb, uint32_t ncells)
     TRY(dalloc(&c.nl_cnt, 2 * (size_t)c.cap));
     c.maxc = maxc;
     TRY(dalloc(&c.link_terms, (size_t)c.cap * maxc));
+    TRY(dalloc(&c.contact, (size_t)c.cap * 2));
     TRY(dalloc(&c.epart, 4 * 1024)); TRY(dalloc(&c.eout, 4));
     TRY(dalloc(&c.S, 1)); TRY(dalloc(&c.err_dev, 1));
     CUDA_TRY(cudaMemset(c.S, 0, sizeof(DevState)));
@@ -245,6 +252,9 @@ static int ensure_ctx(uint32_t full, uint32_t nb, uint32_t ncells)
     CUDA_TRY(cudaStreamCreateWithFlags(&c.side2, cudaStreamNonBlocking));
     CUDA_TRY(cudaEventCreateWithFlags(&c.fork2, cudaEventDisableTiming));
     CUDA_TRY(cudaEventCreateWithFlags(&c.join2, cudaEventDisableTiming));
+    CUDA_TRY(cudaStreamCreateWithFlags(&c.side3, cudaStreamNonBlocking));
+    CUDA_TRY(cudaEventCreateWithFlags(&c.fork3, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventCreateWithFlags(&c.join3, cudaEventDisableTiming));
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     g_max_blocks = sms * 16;
@@ -743,15 +753,26 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
         };
         if (beside) TRY(on_side(c.side2, c.fork2, pbf_water));
         else TRY(pbf_water());
+        // the snow contact sums, kept apart for k_link_sum, beside the snow PBF pass
+        if (links_beside)
+            TRY(on_side(c.side3, c.fork3, [&]() -> int {
+                TLAUNCH(k_dem_corr<true>, 256, full, 128, P, S, vs, vd, vb, X, ss, sd, sb, F, NL, c.contact);
+                return SNOWB_OK;
+            }));
         // the reference's snow PBF pass adds into repeated targets with float atomics (Q3):
         // its order follows the launch shape, so that pass keeps the built-in shape
         TLAUNCH_IF(!ref, k_pbf, 256, 2 * full, 128, P, S, vs, vd, vb, X, ss, sd, sb, a.dt, F, NL);
         STOP(base + 3);
-        TLAUNCH(k_dem_corr, 256, full, 128, P, S, vs, vd, vb, X, ss, sd, sb, F, NL);
+        if (!links_beside) TLAUNCH(k_dem_corr<false>, 256, full, 128, P, S, vs, vd, vb, X, ss, sd, sb, F, NL, nullptr);
         if (a.interlink) {
-            if (links_beside) TRY(join_side(c.side, c.join));
-            else TRY(link_terms());
-            TLAUNCH(k_link_sum, 256, full, 128, P, S, *a.dem, c.link_terms);
+            if (links_beside) {
+                TRY(join_side(c.side3, c.join3));
+                TRY(join_side(c.side, c.join));
+            } else {
+                TRY(link_terms());
+            }
+            TLAUNCH(k_link_sum, 256, full, 128, P, S, *a.dem, c.link_terms, links_beside ? c.contact : nullptr,
+                    F.correct_dem);
         }
         if (beside) TRY(join_side(c.side2, c.join2));
         STOP(base + 5);

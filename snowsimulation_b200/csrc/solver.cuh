@@ -571,10 +571,15 @@ __device__ __forceinline__ void delete_record(const snowb_particle_data& D, uint
 }
 // compute_dem_sph_distance_correction (:2112-2162) and compute_dem_distance_correction
 // (:1765-1834) for snow particle o, added to its correction in the reference's kernel
-// order (after the PBF pass; the interlink terms of k_link_sum follow).
+// order (after the PBF pass; the interlink terms of k_link_sum follow).  SUMS: the two
+// contact sums are kept apart instead: sums[2o] the water contact (scaled by k_stretch *
+// contrib; +0 without correct_dem), sums[2o+1] the snow-then-boundary contact (scaled by
+// contrib).  That pass reads no correction, so it can run beside the snow PBF pass, and
+// k_link_sum adds both to the correction after the PBF term, in this order.
+template <bool SUMS>
 __global__ void __launch_bounds__(256) k_dem_corr(DevParams P, const DevState* __restrict__ S, SetView vs, SetView vd,
                                                   SetView vb, Sets X, Sorted ss, Sorted sd, Sorted sb, StageFlags F,
-                                                  NList L)
+                                                  NList L, float4* __restrict__ sums)
 {
     const uint32_t ns = S->n_sph, nd = S->n_dem, nb = S->n_b;
     vs.n = ns; vd.n = nd; vb.n = nb;
@@ -583,7 +588,7 @@ __global__ void __launch_bounds__(256) k_dem_corr(DevParams P, const DevState* _
         const uint32_t o = vd.gi[i];
         float3 p = xyz(vd.p4[i]); GCell g = grid_pos(P, p, vd.scene(i));
         const float w0 = X.dem.massInv[o], ci = X.dem.contrib[o];
-        float3 acc = ldv3(X.dem.correction, o);
+        float3 acc = SUMS ? z : ldv3(X.dem.correction, o);
         Seg so, sx, sbn;
         const bool lst = segments(L, L.cap + i, so, sx, sbn);
         if (F.correct_dem) {
@@ -591,7 +596,10 @@ __global__ void __launch_bounds__(256) k_dem_corr(DevParams P, const DevState* _
                            : acc_contact(P, z, vs, p, g, SNOWB_UMAX, w0, ss.invm, X.sph.massInv);
             d = sc3(P.k_stretch * ci, d);
             if (nan3(d)) d = z;
-            acc = add3(acc, d);
+            if (SUMS) sums[2 * (size_t)o] = make_float4(d.x, d.y, d.z, 0.f);
+            else acc = add3(acc, d);
+        } else if (SUMS) {
+            sums[2 * (size_t)o] = make_float4(0.f, 0.f, 0.f, 0.f);
         }
         {
             float3 d = lst ? seg_contact(P, z, so, vd, p, w0, sd.invm, X.dem.massInv)
@@ -600,9 +608,9 @@ __global__ void __launch_bounds__(256) k_dem_corr(DevParams P, const DevState* _
                     : acc_contact(P, d, vb, p, g, SNOWB_UMAX, w0, sb.invm, X.bnd.massInv);
             d = sc3(ci, d);
             if (nan3(d)) d = z;
-            acc = add3(acc, d);
+            if (SUMS) sums[2 * (size_t)o + 1] = make_float4(d.x, d.y, d.z, 0.f);
+            else st3(X.dem.correction, o, add3(acc, d));
         }
-        st3(X.dem.correction, o, acc);
     }
     (void)ns; (void)nb;
 }
@@ -652,8 +660,11 @@ __global__ void __launch_bounds__(256) k_link_terms(DevParams P, const DevState*
         terms[s] = t;
     }
 }
+// sums: the contact sums k_dem_corr kept apart (null: it added them itself), added first,
+// the water one only with correct_dem, as k_dem_corr adds them
 __global__ void __launch_bounds__(256) k_link_sum(DevParams P, const DevState* __restrict__ S,
-                                                  snowb_particle_data dem, const float4* __restrict__ terms)
+                                                  snowb_particle_data dem, const float4* __restrict__ terms,
+                                                  const float4* __restrict__ sums, int correct_dem)
 {
     const uint32_t nd = S->n_dem, M = P.maxc;
     const float3 z = f3(0.f, 0.f, 0.f);
@@ -664,7 +675,12 @@ __global__ void __launch_bounds__(256) k_link_sum(DevParams P, const DevState* _
             if (t.w != 0.f) d = add3(d, xyz(t));
         }
         if (nan3(d)) d = z;
-        st3(dem.correction, o, add3(ldv3(dem.correction, o), d));
+        float3 acc = ldv3(dem.correction, o);
+        if (sums) {
+            if (correct_dem) acc = add3(acc, xyz(__ldg(sums + 2 * (size_t)o)));
+            acc = add3(acc, xyz(__ldg(sums + 2 * (size_t)o + 1)));
+        }
+        st3(dem.correction, o, add3(acc, d));
     }
 }
 
