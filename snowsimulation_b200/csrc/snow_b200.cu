@@ -786,8 +786,13 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
         STOP(base + 6);
         if (a.friction && step_dem) {
             TRY(sort_pair(false, false, beside));
-            TLAUNCH(k_friction, 256, full, 128, P, S, vd, vb, X, sd, sb, NL, fr_lists ? 1 : 0);
-            TLAUNCH(k_apply, 1024, full, 256, P, S, vs, vd, X, 0, 1, track_s, track_d);
+            // a whole substep applies the friction correction in the friction pass itself
+            if (beside) {
+                TLAUNCH(k_friction<true>, 256, full, 128, P, S, vd, vb, X, sd, sb, NL, fr_lists ? 1 : 0, track_d);
+            } else {
+                TLAUNCH(k_friction<false>, 256, full, 128, P, S, vd, vb, X, sd, sb, NL, fr_lists ? 1 : 0, track_d);
+                TLAUNCH(k_apply, 1024, full, 256, P, S, vs, vd, X, 0, 1, track_s, track_d);
+            }
             dirty_d = true;
         }
         STOP(base + 7);

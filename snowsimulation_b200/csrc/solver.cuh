@@ -752,8 +752,13 @@ constexpr uint32_t FR_K = 16;
 // then takes its snow and boundary contacts from its list entries, in list order, instead
 // of traversing the cells (same contacts, same order: the list holds every candidate with
 // d < h in traversal order with its cell).
+// APPLY: the friction correction is applied at once (the snow part of k_apply, whose
+// position it reads is this pass's p: new and predicted positions, a zero correction, the
+// moved mark of the set), without k_apply's far-move flag, which the next density+lambda
+// pass clears before any friction pass reads it.
+template <bool APPLY>
 __global__ void __launch_bounds__(256) k_friction(DevParams P, const DevState* __restrict__ S, SetView vd, SetView vb,
-                                                  Sets X, Sorted sd, Sorted sb, NList L, int lists)
+                                                  Sets X, Sorted sd, Sorted sb, NList L, int lists, SortTrack td)
 {
     __shared__ uint32_t rec_sh[FR_K * 256];
     uint32_t* const rec = rec_sh + threadIdx.x;     // entry k at rec[k * blockDim.x]
@@ -917,7 +922,15 @@ __global__ void __launch_bounds__(256) k_friction(DevParams P, const DevState* _
             }
         }
         if (nan3(c)) c = f3(0.f, 0.f, 0.f);
-        st3(X.dem.correction, o, c);
+        if (APPLY) {
+            const float3 np = add3(p, sc3(P.sor, c));
+            st3(X.dem.new_positions, o, np);
+            st3(X.dem.predict_positions, o, np);
+            st3(X.dem.correction, o, f3(0.f, 0.f, 0.f));
+            if (td.key) track_move(P, td, o, np, vd.scene(i));
+        } else {
+            st3(X.dem.correction, o, c);
+        }
     }
 }
 

@@ -19,9 +19,11 @@ def test_tuned_results_bit_exact(cuda, quirks):
     sim = Simulation(scene.config0(), quirks=quirks).setup()
     table = autotune.tune(sim, substeps=2)
     names = {line.split()[0] for line in table.splitlines()}
-    assert {"k_density<true>", "k_friction", "k_link_colour_warp"} <= names
-    # whole substeps take the snow contact sums apart, beside the snow PBF pass
-    assert any(n.startswith("k_dem_corr") for n in names)
+    assert {"k_density<true>", "k_link_colour_warp"} <= names
+    # whole substeps take the snow contact sums apart, beside the snow PBF pass, and apply
+    # the friction correction inside the friction pass (the template argument says which)
+    assert any(n.startswith("k_dem_corr<") for n in names)
+    assert any(n.startswith("k_friction<") for n in names)
     # the reference's snow PBF pass adds into repeated targets with float atomics (Q3), so
     # its launch shape stays fixed in the reference quirk mode
     assert ("k_pbf" in names) == (quirks == QUIRKS_FIXED)
