@@ -747,8 +747,12 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
         // density + lambda in one pass (stage boundaries base+1 and base+2 coincide)
         TLAUNCH(k_density<true>, 256, work3, 128, P, S, vs, vd, vb, X, ss, sd, sb, NL, 1);
         STOP(base + 2);
+        // with the interlink pass beside, the passes that finish a correction apply it (no
+        // k_apply launch): the water PBF passes for the water, k_link_apply for the snow
+        const int apply_w = links_beside && step_sph ? 1 : 0;
         auto pbf_water = [&]() -> int {
-            TLAUNCH(k_pbf_water_warp, 256, (uint64_t)full * 32, 128, P, S, vs, vd, vb, X, ss, sd, sb, a.dt, F);
+            TLAUNCH(k_pbf_water_warp, 256, (uint64_t)full * 32, 128, P, S, vs, vd, vb, X, ss, sd, sb, a.dt, F, apply_w,
+                    track_s);
             return SNOWB_OK;
         };
         if (beside) TRY(on_side(c.side2, c.fork2, pbf_water));
@@ -761,7 +765,7 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
             }));
         // the reference's snow PBF pass adds into repeated targets with float atomics (Q3):
         // its order follows the launch shape, so that pass keeps the built-in shape
-        TLAUNCH_IF(!ref, k_pbf, 256, 2 * full, 128, P, S, vs, vd, vb, X, ss, sd, sb, a.dt, F, NL);
+        TLAUNCH_IF(!ref, k_pbf, 256, 2 * full, 128, P, S, vs, vd, vb, X, ss, sd, sb, a.dt, F, NL, apply_w, track_s);
         STOP(base + 3);
         if (!links_beside) TLAUNCH(k_dem_corr<false>, 256, full, 128, P, S, vs, vd, vb, X, ss, sd, sb, F, NL, nullptr);
         if (a.interlink) {
@@ -771,12 +775,18 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
             } else {
                 TRY(link_terms());
             }
-            TLAUNCH(k_link_sum, 256, full, 128, P, S, *a.dem, c.link_terms, links_beside ? c.contact : nullptr,
-                    F.correct_dem);
+            if (links_beside)
+                TLAUNCH(k_link_apply, 256, full, 128, P, S, vd, *a.dem, c.link_terms, c.contact, F.correct_dem,
+                        step_dem ? 1 : 0, track_d);
+            else
+                TLAUNCH(k_link_sum, 256, full, 128, P, S, *a.dem, c.link_terms, nullptr, F.correct_dem);
         }
         if (beside) TRY(join_side(c.side2, c.join2));
         STOP(base + 5);
-        if (step_sph || step_dem) {
+        if (links_beside) {
+            if (step_sph) dirty_s = true;
+            if (step_dem) dirty_d = true;
+        } else if (step_sph || step_dem) {
             TLAUNCH(k_apply, 1024, 2 * full, 256, P, S, vs, vd, X, step_sph ? 1 : 0, step_dem ? 1 : 0, track_s,
                     track_d);
             if (step_sph) dirty_s = true;

@@ -458,6 +458,26 @@ __global__ void __launch_bounds__(256) k_density(DevParams P, DevState* __restri
     }
 }
 
+// ======================================================== applying a correction
+// apply_correction (:1342-1380) for one particle: new and predicted position q + sor * corr,
+// the correction cleared, the set marked when the particle left its cell.  Passes that
+// finish a particle's correction apply it themselves where k_apply would come next; limits
+// carry the reference's launch sizes (Q12).
+__device__ __forceinline__ uint32_t launch_limit(const DevParams& P, uint32_t n0, uint32_t n)
+{
+    return P.quirks == SNOWB_QUIRKS_REFERENCE ? umin32(coverage(n0), n) : n;
+}
+__device__ __forceinline__ float3 apply_one(const DevParams& P, const snowb_particle_data& D, const SortTrack& T,
+                                            uint32_t o, float3 q, float3 corr, uint32_t scene)
+{
+    const float3 np = add3(q, sc3(P.sor, corr));
+    st3(D.new_positions, o, np);
+    st3(D.predict_positions, o, np);
+    st3(D.correction, o, f3(0.f, 0.f, 0.f));
+    if (T.key) track_move(P, T, o, np, scene);
+    return np;
+}
+
 // ==================================================== PBF + water-side contact corrections
 // compute_pbf_sph_correction (:3070-3184) fused with compute_sph_dem_distance_correction
 // (:2061-2110) and compute_sph_sph_distance_correction (:2164-2217) for water, and
@@ -470,9 +490,10 @@ struct StageFlags {
 // with few particles one thread each leaves the GPU idle while each thread walks its
 // neighbours; above it, threads fill the GPU and the warp form's extra work would cost more.
 constexpr uint32_t PBF_WARP_MAX_WATER = 65536;
-__global__ void __launch_bounds__(256) k_pbf(DevParams P, const DevState* __restrict__ S, SetView vs, SetView vd,
+// apply: as in k_pbf_water_warp, for the water particles this pass takes
+__global__ void __launch_bounds__(256) k_pbf(DevParams P, DevState* __restrict__ S, SetView vs, SetView vd,
                                              SetView vb, Sets X, Sorted ss, Sorted sd, Sorted sb, float dt,
-                                             StageFlags F, NList L)
+                                             StageFlags F, NList L, int apply, SortTrack ts)
 {
     const uint32_t ns = S->n_sph, nd = S->n_dem, nb = S->n_b;
     vs.n = ns; vd.n = nd; vb.n = nb;
@@ -521,7 +542,8 @@ __global__ void __launch_bounds__(256) k_pbf(DevParams P, const DevState* __rest
                 if (nan3(d)) d = z;
                 acc = add3(acc, d);
             }
-            st3(X.sph.correction, o, acc);
+            if (apply && i < launch_limit(P, S->n0_sph, ns)) apply_one(P, X.sph, ts, o, p, acc, vs.scene(i));
+            else st3(X.sph.correction, o, acc);
         } else {
             const uint32_t i = t - ns;
             const uint32_t o = ref ? vs.gi[i] : vd.gi[i];   // Q3: SPH grid_index in the reference
@@ -691,12 +713,46 @@ __global__ void __launch_bounds__(256) k_link_sum(DevParams P, const DevState* _
 // h = 0.04; the bound is checked against the parameters on the host).
 constexpr float FR_LIST_MOVE = 0.004f;
 
+// k_link_sum and the snow part of k_apply in one pass over the sorted snow particles (the
+// order k_apply takes them in; o = grid_index[i] runs over the same particles as k_link_sum's
+// o): the contact sums and the interlink terms join the correction, which is applied to the
+// particles within the launch limit and kept for the others, as k_apply leaves it.
+__global__ void __launch_bounds__(256) k_link_apply(DevParams P, DevState* __restrict__ S, SetView vd,
+                                                    snowb_particle_data dem, const float4* __restrict__ terms,
+                                                    const float4* __restrict__ sums, int correct_dem, int apply,
+                                                    SortTrack td)
+{
+    const uint32_t nd = S->n_dem, M = P.maxc;
+    const uint32_t ld = apply ? launch_limit(P, S->n0_dem, nd) : 0u;
+    const float3 z = f3(0.f, 0.f, 0.f);
+    GRID_LOOP(i, nd) {
+        const uint32_t o = vd.gi[i];
+        float3 d = z;
+        for (uint32_t s = M * o; s < M * (o + 1); ++s) {
+            const float4 t = __ldg(terms + s);
+            if (t.w != 0.f) d = add3(d, xyz(t));
+        }
+        if (nan3(d)) d = z;
+        float3 acc = ldv3(dem.correction, o);
+        if (sums) {
+            if (correct_dem) acc = add3(acc, xyz(__ldg(sums + 2 * (size_t)o)));
+            acc = add3(acc, xyz(__ldg(sums + 2 * (size_t)o + 1)));
+        }
+        acc = add3(acc, d);
+        if (i < ld) {
+            const float3 q = xyz(vd.p4[i]);
+            const float3 np = apply_one(P, dem, td, o, q, acc, vd.scene(i));
+            const float3 dp = sub3(np, q);
+            if (!(dot3(dp, dp) <= FR_LIST_MOVE * FR_LIST_MOVE)) S->far_move = 1u;
+        } else {
+            st3(dem.correction, o, acc);
+        }
+    }
+}
+
+
 // ======================================================================= apply
 // apply_correction (:1342-1380); limits carry the reference's launch sizes (Q12).
-__device__ __forceinline__ uint32_t launch_limit(const DevParams& P, uint32_t n0, uint32_t n)
-{
-    return P.quirks == SNOWB_QUIRKS_REFERENCE ? umin32(coverage(n0), n) : n;
-}
 // ts, td: a particle that leaves its cell marks its set for a full sort at the next sort
 // point (key null: not tracked).
 __global__ void k_apply(DevParams P, DevState* __restrict__ S, SetView vs, SetView vd, Sets X, int do_sph,
@@ -711,12 +767,7 @@ __global__ void k_apply(DevParams P, DevState* __restrict__ S, SetView vs, SetVi
         const snowb_particle_data& D = w ? X.sph : X.dem;
         const uint32_t o = v.gi[i];
         const float3 q = xyz(v.p4[i]);
-        float3 np = add3(q, sc3(P.sor, ldv3(D.correction, o)));
-        st3(D.new_positions, o, np);
-        st3(D.predict_positions, o, np);
-        st3(D.correction, o, f3(0.f, 0.f, 0.f));
-        const SortTrack& T = w ? ts : td;
-        if (T.key) track_move(P, T, o, np, v.scene(i));
+        const float3 np = apply_one(P, D, w ? ts : td, o, q, ldv3(D.correction, o), v.scene(i));
         if (!w) {
             const float3 dp = sub3(np, q);
             if (!(dot3(dp, dp) <= FR_LIST_MOVE * FR_LIST_MOVE)) S->far_move = 1u;
@@ -923,11 +974,7 @@ __global__ void __launch_bounds__(256) k_friction(DevParams P, const DevState* _
         }
         if (nan3(c)) c = f3(0.f, 0.f, 0.f);
         if (APPLY) {
-            const float3 np = add3(p, sc3(P.sor, c));
-            st3(X.dem.new_positions, o, np);
-            st3(X.dem.predict_positions, o, np);
-            st3(X.dem.correction, o, f3(0.f, 0.f, 0.f));
-            if (td.key) track_move(P, td, o, np, vd.scene(i));
+            apply_one(P, X.dem, td, o, p, c, vd.scene(i));
         } else {
             st3(X.dem.correction, o, c);
         }
@@ -1111,9 +1158,11 @@ __device__ __forceinline__ float3 warp_ordered_sum(float3 acc, float3 part)
 // order with shuffles -- the sums the one-thread loops form, with 27 cells in flight.  The
 // water set is small (a few thousand particles at a time), so one thread per particle
 // left the GPU nearly idle while each thread walked its neighbours.
-__global__ void __launch_bounds__(256) k_pbf_water_warp(DevParams P, const DevState* __restrict__ S, SetView vs,
+// apply: the water part of k_apply follows at once for particles within the launch limit
+// (the pass's p is k_apply's sorted position; the correction it would read is acc)
+__global__ void __launch_bounds__(256) k_pbf_water_warp(DevParams P, DevState* __restrict__ S, SetView vs,
                                                         SetView vd, SetView vb, Sets X, Sorted ss, Sorted sd,
-                                                        Sorted sb, float dt, StageFlags F)
+                                                        Sorted sb, float dt, StageFlags F, int apply, SortTrack ts)
 {
     const uint32_t ns = S->n_sph;
     if (ns > PBF_WARP_MAX_WATER) return;   // k_pbf runs the water terms one thread each
@@ -1156,7 +1205,10 @@ __global__ void __launch_bounds__(256) k_pbf_water_warp(DevParams P, const DevSt
             if (nan3(d)) d = z;
             acc = add3(acc, d);
         }
-        if (lane == 0) st3(X.sph.correction, o, acc);
+        if (lane == 0) {
+            if (apply && i < launch_limit(P, S->n0_sph, ns)) apply_one(P, X.sph, ts, o, p, acc, vs.scene(i));
+            else st3(X.sph.correction, o, acc);
+        }
     }
 }
 __device__ __forceinline__ float3 xsph_cell(const DevParams& P, const SetView& v, const snowb_particle_data& O,
