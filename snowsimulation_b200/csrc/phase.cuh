@@ -729,6 +729,29 @@ __device__ void link_particle(const DevParams& P, const SetView& vd, const snowb
         }
     }
 }
+// Link formation's copy of the snow set's sorted view (the arrays its passes read: the
+// sorted copies, grid index and hash, the cell table and the sort's cell offsets), taken
+// after the sort point before it, so that the first iteration's sort point may rewrite the
+// set's view while link formation runs.  `full` entries of the particle arrays (the
+// caller's arrays hold that many), `ncells` of the cell table.
+__global__ void k_copy_link_view(SetView v, uint32_t full, uint32_t ncells, const uint32_t* __restrict__ off,
+                                 float4* __restrict__ p4, snowb_float3* __restrict__ sp, uint32_t* __restrict__ gi,
+                                 uint32_t* __restrict__ gh, uint32_t* __restrict__ sid, uint32_t* __restrict__ cs,
+                                 uint32_t* __restrict__ ce, uint32_t* __restrict__ off_o)
+{
+    const uint32_t m = full > ncells + 1 ? full : ncells + 1;
+    GRID_LOOP(k, m) {
+        if (k < full) {
+            p4[k] = v.p4[k];
+            sp[k] = v.sp[k];
+            gi[k] = v.gi[k];
+            gh[k] = v.gh[k];
+            if (v.sid) sid[k] = v.sid[k];
+        }
+        if (k < ncells) { cs[k] = v.cs[k]; ce[k] = v.ce[k]; }
+        if (k <= ncells) off_o[k] = off[k];
+    }
+}
 // one colour: one thread per super-cell of that colour; fs/fe give each hash cell's
 // current (non-stale) sorted range
 __global__ void k_link_colour(DevParams P, DevState* S, SetView vd, snowb_particle_data dem,

@@ -151,6 +151,13 @@ struct Ctx {
     uint32_t *fs = nullptr, *fe = nullptr;
     snowb_float3* tmp_vel = nullptr;
     uint32_t *nl_e = nullptr, *nl_cnt = nullptr;
+    uint32_t *nl2_e = nullptr, *nl2_cnt = nullptr;   // the first density pass's snow lists (link formation)
+    // link formation's copy of the snow set's sorted view, taken after the sort point that
+    // precedes it, so that the first iteration's sort may run beside it
+    float4* lf_p4 = nullptr;
+    snowb_float3* lf_sp = nullptr;
+    uint32_t *lf_gi = nullptr, *lf_gh = nullptr, *lf_sid = nullptr, *lf_cs = nullptr, *lf_ce = nullptr,
+             *lf_off = nullptr;
     float4* link_terms = nullptr;         // one interlink term per slot (k_link_terms)
     float4* contact = nullptr;            // two snow contact sums per particle (k_dem_corr<true>)
     double* epart = nullptr;
@@ -164,6 +171,8 @@ struct Ctx {
     cudaEvent_t fork2 = nullptr, join2 = nullptr;
     cudaStream_t side3 = nullptr;         // fourth stream (the snow contact sums beside the snow PBF pass)
     cudaEvent_t fork3 = nullptr, join3 = nullptr;
+    cudaStream_t side4 = nullptr;         // fifth stream (link formation beside the integration and iteration 1)
+    cudaEvent_t fork4 = nullptr, ev_view = nullptr, ev_links = nullptr;
 };
 static Ctx g_ctx;
 static uint64_t g_ctx_gen = 0;   // bumped whenever the scratch buffers are (re)allocated
@@ -183,7 +192,8 @@ static void free_ctx(Ctx& c)
     free_set(c.gen);
     void* ptrs[] = {c.fl_s, c.fl_d, c.rk_s, c.rk_d, c.sbsum, c.active, c.sc_flag, c.sc_list, c.fs, c.fe, c.tmp_vel,
                     c.epart, c.eout, c.link_terms, c.contact,
-                    c.S, c.err_dev, c.nl_e, c.nl_cnt};
+                    c.S, c.err_dev, c.nl_e, c.nl_cnt, c.nl2_e, c.nl2_cnt, c.lf_p4, c.lf_sp, c.lf_gi, c.lf_gh,
+                    c.lf_sid, c.lf_cs, c.lf_ce, c.lf_off};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c.S_host) cudaFreeHost(c.S_host);
@@ -196,6 +206,10 @@ static void free_ctx(Ctx& c)
     if (c.side3) cudaStreamDestroy(c.side3);
     if (c.fork3) cudaEventDestroy(c.fork3);
     if (c.join3) cudaEventDestroy(c.join3);
+    if (c.side4) cudaStreamDestroy(c.side4);
+    if (c.fork4) cudaEventDestroy(c.fork4);
+    if (c.ev_view) cudaEventDestroy(c.ev_view);
+    if (c.ev_links) cudaEventDestroy(c.ev_links);
     c = Ctx();
 }
 static int alloc_sort(SetBufs& s, uint32_t cap, uint32_t ncells, bool attrs)
@@ -238,6 +252,11 @@ static int ensure_ctx(uint32_t full, uint32_t nb, uint32_t ncells)
     TRY(dalloc(&c.tmp_vel, c.cap));
     TRY(dalloc(&c.nl_e, (size_t)NLIST_K * 2 * c.cap));
     TRY(dalloc(&c.nl_cnt, 2 * (size_t)c.cap));
+    TRY(dalloc(&c.nl2_e, (size_t)NLIST_K * 2 * c.cap));
+    TRY(dalloc(&c.nl2_cnt, 2 * (size_t)c.cap));
+    TRY(dalloc(&c.lf_p4, c.cap)); TRY(dalloc(&c.lf_sp, c.cap)); TRY(dalloc(&c.lf_gi, c.cap));
+    TRY(dalloc(&c.lf_gh, c.cap)); TRY(dalloc(&c.lf_sid, c.cap)); TRY(dalloc(&c.lf_cs, (size_t)c.ncells));
+    TRY(dalloc(&c.lf_ce, (size_t)c.ncells)); TRY(dalloc(&c.lf_off, (size_t)c.ncells + 1));
     c.maxc = maxc;
     TRY(dalloc(&c.link_terms, (size_t)c.cap * maxc));
     TRY(dalloc(&c.contact, (size_t)c.cap * 2));
@@ -255,6 +274,10 @@ static int ensure_ctx(uint32_t full, uint32_t nb, uint32_t ncells)
     CUDA_TRY(cudaStreamCreateWithFlags(&c.side3, cudaStreamNonBlocking));
     CUDA_TRY(cudaEventCreateWithFlags(&c.fork3, cudaEventDisableTiming));
     CUDA_TRY(cudaEventCreateWithFlags(&c.join3, cudaEventDisableTiming));
+    CUDA_TRY(cudaStreamCreateWithFlags(&c.side4, cudaStreamNonBlocking));
+    CUDA_TRY(cudaEventCreateWithFlags(&c.fork4, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventCreateWithFlags(&c.ev_view, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventCreateWithFlags(&c.ev_links, cudaEventDisableTiming));
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     g_max_blocks = sms * 16;
@@ -595,6 +618,9 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
     Sorted sb{c.b.invm, nullptr, c.b.lambda, c.b.mass};
     StageFlags F{a.correct_dem, a.sph_sph, a.interlink, step_sph ? 1 : 0, step_dem ? 1 : 0};
     NList NL{c.nl_e, c.nl_cnt, 2 * cap, cap};
+    // the substep's first density pass lists the snow-snow candidates for link formation in
+    // a list of their own, which the iterations' density passes leave alone
+    NList NL2{c.nl2_e, c.nl2_cnt, 2 * cap, cap};
     // the friction pass may replay the density+lambda lists when a contact (d <= 2r) after a
     // move of at most FR_LIST_MOVE per particle was within h before it
     const bool fr_lists = P.two_r + 2.f * FR_LIST_MOVE < 0.9f * P.h;
@@ -653,11 +679,19 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
         water_pending = false;
         return SNOWB_OK;
     };
+    // link formation beside the integration and the first iteration (see below): the snow
+    // sort waits for link formation's copy of the snow view, the first interlink terms for
+    // the links
+    bool view_pending = false, links_pending = false;
     auto sort_pair = [&](bool after_phase, bool begin = false, bool defer_water = false) -> int {
         TRY(join_water());
         const bool need_s = dirty_s || after_phase, need_d = dirty_d || after_phase;
         if (!need_s && !need_d) return SNOWB_OK;
         if (need_s) TRY(on_side(c.side, c.fork, [&]() { return sort_if(0, false); }));
+        if (need_d && view_pending) {
+            CUDA_TRY(cudaStreamWaitEvent(g_stream, c.ev_view, 0));
+            view_pending = false;
+        }
         if (need_d) TRY(sort_if(1, begin));
         if (need_s) {
             if (defer_water) water_pending = true;
@@ -676,7 +710,7 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
     // iterations' density+lambda passes before anything reads them, so a whole substep with
     // iterations leaves the boundary out here.
     const int bnd_first = !(beside && a.iterations > 0);
-    TLAUNCH(k_density<false>, 256, bnd_first ? work3 : 2 * full, 128, P, S, vs, vd, vb, X, ss, sd, sb, NL, bnd_first);
+    TLAUNCH(k_density<false>, 256, bnd_first ? work3 : 2 * full, 128, P, S, vs, vd, vb, X, ss, sd, sb, NL2, bnd_first);
     STOP(2);
     if (a.temperature) {
         TLAUNCH(k_heat, 256, 2 * full, 128, P, S, vs, vd, X, a.dt);
@@ -710,18 +744,43 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
     }
     STOP(5);
     if (a.interlink) {
-        const SCList scl = sc_lists(P);
-        TLAUNCH(k_link_filter, 256, full, 128, P, S, vd, *a.dem, a.dynamic, c.active, NL, scl);
-        const uint32_t nsc = (P.gsx / 4) * (P.gsy / 4) * (P.gsz / 4);   // super-cells per colour
-        for (uint32_t col = 0; col < 8; ++col) {
-            if (P.maxc <= SNOWB_MAXC_FAST)
-                TLAUNCH(k_link_colour_warp, 256, (uint64_t)nsc * 32, 128, P, S, vd, *a.dem, c.s[1].off,
-                        c.s[1].off + 1, c.active, col, a.dynamic, NL, scl);
-            else
-                TLAUNCH(k_link_colour, 128, nsc, 64, P, S, vd, *a.dem, c.s[1].off, c.s[1].off + 1, c.active, col,
-                        a.dynamic);
+        // link formation over a view of the snow set: the set's own, or its copy
+        auto form = [&](const SetView& v, const uint32_t* off) -> int {
+            const SCList scl = sc_lists(P);
+            TLAUNCH(k_link_filter, 256, full, 128, P, S, v, *a.dem, a.dynamic, c.active, NL2, scl);
+            const uint32_t nsc = (P.gsx / 4) * (P.gsy / 4) * (P.gsz / 4);   // super-cells per colour
+            for (uint32_t col = 0; col < 8; ++col) {
+                if (P.maxc <= SNOWB_MAXC_FAST)
+                    TLAUNCH(k_link_colour_warp, 256, (uint64_t)nsc * 32, 128, P, S, v, *a.dem, off, off + 1, c.active,
+                            col, a.dynamic, NL2, scl);
+                else
+                    TLAUNCH(k_link_colour, 128, nsc, 64, P, S, v, *a.dem, off, off + 1, c.active, col, a.dynamic);
+            }
+            if (a.dynamic) LAUNCH1(k_adjust_links, P, S, *a.dem, full);
+            return SNOWB_OK;
+        };
+        // Link formation reads the snow set's sorted view, its links and temperatures and
+        // writes its links; the integration and the first iteration's sort points, density,
+        // PBF and contact passes touch none of the links.  In a whole substep it therefore
+        // runs beside them, over a copy of the view (the first snow sort rewrites the view),
+        // and the first interlink terms wait for it.
+        const bool links_early = beside && a.iterations > 0 && !g_tape.recording;
+        if (links_early) {
+            SetView vl = vd;
+            vl.p4 = c.lf_p4; vl.sp = c.lf_sp; vl.gi = c.lf_gi; vl.gh = c.lf_gh; vl.cs = c.lf_cs; vl.ce = c.lf_ce;
+            vl.sid = vd.sid ? c.lf_sid : nullptr;
+            TRY(on_side(c.side4, c.fork4, [&]() -> int {
+                LAUNCH(k_copy_link_view, (full > P.ncells + 1 ? full : P.ncells + 1), 256, vd, full, P.ncells,
+                       c.s[1].off, c.lf_p4, c.lf_sp, c.lf_gi, c.lf_gh, c.lf_sid, c.lf_cs, c.lf_ce, c.lf_off);
+                CUDA_TRY(cudaEventRecord(c.ev_view, g_stream));
+                TRY(form(vl, c.lf_off));
+                CUDA_TRY(cudaEventRecord(c.ev_links, g_stream));
+                return SNOWB_OK;
+            }));
+            view_pending = links_pending = true;
+        } else {
+            TRY(form(vd, c.s[1].off));
         }
-        if (a.dynamic) LAUNCH1(k_adjust_links, P, S, *a.dem, full);
     }
     STOP(6);
     if (step_sph || step_dem) {
@@ -739,6 +798,10 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
         STOP(base + 0);
         // the interlink terms read the predicted positions and the link records only
         auto link_terms = [&]() -> int {
+            if (links_pending) {
+                CUDA_TRY(cudaStreamWaitEvent(g_stream, c.ev_links, 0));
+                links_pending = false;
+            }
             TLAUNCH(k_link_terms, 256, (uint64_t)P.maxc * full, 256, P, S, *a.dem, c.link_terms);
             return SNOWB_OK;
         };
