@@ -441,6 +441,11 @@ int snowb_launch_count(uint64_t* count);
  * and writes one line per kernel, "name launches total_ms", into out (NUL-terminated). */
 int snowb_profile_begin(void);
 int snowb_profile_end(char* out, size_t cap);
+/* While profiling, after a step: the launches of its last substep (the last replay of its
+ * graph, or the last substep run directly) as a timeline, one line per launch in launch
+ * order, "name start_ms end_ms", times from the start of that substep's first launch
+ * (launches on the library's side streams overlap the others).  NUL-terminated. */
+int snowb_profile_timeline(char* out, size_t cap);
 
 /* Release the library's internal device buffers (they are re-created on demand). */
 int snowb_release(void);

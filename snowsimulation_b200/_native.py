@@ -31,7 +31,7 @@ EXPORTS = (
     "snowb_connect_and_record", "snowb_snow_simulation", "snowb_snow_simulation_ex", "snowb_read_sizes",
     "snowb_set_quirks", "snowb_set_stream", "snowb_synchronize", "snowb_energy_momentum", "snowb_release",
     "snowb_last_error", "snowb_last_error_string", "snowb_launch_count", "snowb_profile_begin",
-    "snowb_profile_end", "snowb_device_counters",
+    "snowb_profile_end", "snowb_profile_timeline", "snowb_device_counters",
     "snowb_sort_particles_static",
     "snowb_batch_num_cells", "snowb_batch_calculate_hash", "snowb_batch_sort_particles",
     "snowb_batch_reorder_data", "snowb_batch_compute_boundary_volume", "snowb_batch_connect_and_record",
@@ -84,6 +84,7 @@ def load(path=LIB_PATH):
         "snowb_launch_count": [C.POINTER(C.c_uint64)],
         "snowb_profile_begin": [],
         "snowb_profile_end": [C.c_char_p, C.c_size_t],
+        "snowb_profile_timeline": [C.c_char_p, C.c_size_t],
         "snowb_device_counters": [C.POINTER(C.c_uint32), C.c_int],
         "snowb_sort_particles_static": [CD, u32],
     }

@@ -70,6 +70,7 @@ struct DevState {
     // were built (set by k_apply, cleared by the density+lambda pass)
     uint32_t far_move;
     uint32_t sc_count[8];           // super-cells listed for each link colour (SCList)
+    uint32_t clean_hi[2];           // per set: every slot from here on is clean (k_commit_sizes)
 };
 #define SNOWB_DEVERR_SCATTER 1u
 #define SNOWB_DEVERR_SCENE 2u      // a batched scene id >= the scene count
@@ -252,6 +253,7 @@ __device__ __host__ __forceinline__ uint32_t coverage(uint32_t n)
     return b * t;
 }
 __device__ __host__ __forceinline__ uint32_t umin32(uint32_t a, uint32_t b) { return a < b ? a : b; }
+__device__ __host__ __forceinline__ uint32_t umax32(uint32_t a, uint32_t b) { return a > b ? a : b; }
 
 // The 27 neighbour cells of a particle, computed once and shared by every set and pass of
 // a kernel: wrapped per-axis hash terms (hash = z term + y term + x term, the value of

@@ -26,9 +26,9 @@ namespace snowb {
 
 #define SNOWB_MAXC_FAST 32   // interlink slots kept in registers (maximum_connection <= 32)
 
-// copy_particle_info (:3974-4002)
-__device__ __forceinline__ void copy_info(const snowb_particle_data& s, const snowb_particle_data& d, uint32_t i,
-                                          uint32_t t, uint32_t M)
+// copy_particle_info (:3974-4002): every per-particle field, then the link slots
+__device__ __forceinline__ void copy_fields(const snowb_particle_data& s, const snowb_particle_data& d, uint32_t i,
+                                            uint32_t t)
 {
     st3(d.positions, t, ldv3(s.positions, i));
     st3(d.predict_positions, t, ldv3(s.predict_positions, i));
@@ -45,11 +45,16 @@ __device__ __forceinline__ void copy_info(const snowb_particle_data& s, const sn
     d.T[t] = s.T[i];
     d.new_T[t] = s.new_T[i];
     d.trackId[t] = s.trackId[i];
+    d.iter_end[t] = s.iter_end[i];
+}
+__device__ __forceinline__ void copy_info(const snowb_particle_data& s, const snowb_particle_data& d, uint32_t i,
+                                          uint32_t t, uint32_t M)
+{
+    copy_fields(s, d, i, t);
     for (uint32_t c = 0; c < M; ++c) {
         d.connect_record[t * M + c] = s.connect_record[i * M + c];
         d.connect_length[t * M + c] = s.connect_length[i * M + c];
     }
-    d.iter_end[t] = s.iter_end[i];
 }
 __device__ __forceinline__ void reset_records(const snowb_particle_data& d, uint32_t t, uint32_t M)
 {
@@ -128,43 +133,84 @@ __global__ void k_shuffle_records(DevParams P, const DevState* __restrict__ S, s
         }
     }
 }
+// Compaction moves the kept particles to their ranks (scan_index).  A kept particle with
+// no removed one before it stays where it is, and copying it out and back, as the
+// reference's copy_to_target and scatter do for every slot, leaves it unchanged; so both
+// passes move only the particles whose slot changes (the phase-change buffer, scratch the
+// reference overwrites at every compaction, holds only those).  Threads k < full take a
+// particle's fields, the others one link slot each (coalesced over the slot arrays).
+__device__ __forceinline__ bool compaction_moves(const snowb_particle_data& d, uint32_t i)
+{
+    return d.predicate[i] == 1 && d.scan_index[i] != i;
+}
 // copy_to_target (:4451-4460) into the caller's phase-change buffer
 __global__ void k_copy_to_buffer(DevParams P, const DevState* __restrict__ S, snowb_particle_data d,
                                  snowb_particle_data buf, uint32_t full, const uint32_t* __restrict__ sid,
                                  uint32_t* __restrict__ sid_buf)
 {
     if (S->changed == 0) return;
-    GRID_LOOP(i, full) {
-        copy_info(d, buf, i, i, P.maxc);
-        if (sid) sid_buf[i] = sid[i];
+    const uint32_t M = P.maxc;
+    GRID_LOOP(k, full * (M + 1)) {
+        if (k < full) {
+            if (!compaction_moves(d, k)) continue;
+            copy_fields(d, buf, k, k);
+            if (sid) sid_buf[k] = sid[k];
+        } else {
+            const uint32_t s = k - full;
+            if (!compaction_moves(d, s / M)) continue;
+            buf.connect_record[s] = d.connect_record[s];
+            buf.connect_length[s] = d.connect_length[s];
+        }
     }
 }
 // scatter (:4462-4480).  rebase (fixed quirks, snow set): a moved particle keeps its link
-// count, iter_end = t*M + count; the reference copies iter_end verbatim (Q13).
+// count, iter_end = t*M + count; the reference copies iter_end verbatim (Q13).  A particle
+// that stays keeps its iter_end either way.
 __global__ void k_scatter_set(DevParams P, DevState* S, snowb_particle_data d, snowb_particle_data buf, uint32_t full,
                               uint32_t* __restrict__ sid, const uint32_t* __restrict__ sid_buf, int rebase)
 {
     if (S->changed == 0) return;
-    GRID_LOOP(i, full) {
-        if (d.predicate[i] == 1) {
+    const uint32_t M = P.maxc;
+    GRID_LOOP(k, full * (M + 1)) {
+        if (k < full) {
+            const uint32_t i = k;
+            if (d.predicate[i] == 1) {
+                const uint32_t t = d.scan_index[i];
+                if (t >= full) { atomicOr(&S->err, SNOWB_DEVERR_SCATTER); continue; }
+                if (t != i) {
+                    copy_fields(buf, d, i, t);
+                    if (rebase) d.iter_end[t] = M * t + (buf.iter_end[i] - M * i);
+                    if (sid) sid[t] = sid_buf[i];
+                }
+                d.new_index[i] = t;
+            } else d.new_index[i] = SNOWB_UMAX;
+        } else {
+            const uint32_t s = k - full, i = s / M;
+            if (d.predicate[i] != 1) continue;
             const uint32_t t = d.scan_index[i];
-            if (t >= full) { atomicOr(&S->err, SNOWB_DEVERR_SCATTER); continue; }
-            copy_info(buf, d, i, t, P.maxc);
-            if (rebase) d.iter_end[t] = P.maxc * t + (buf.iter_end[i] - P.maxc * i);
-            if (sid) sid[t] = sid_buf[i];
-            d.new_index[i] = t;
-        } else d.new_index[i] = SNOWB_UMAX;
+            if (t >= full || t == i) continue;
+            const uint32_t q = t * M + (s - i * M);
+            d.connect_record[q] = buf.connect_record[s];
+            d.connect_length[q] = buf.connect_length[s];
+        }
     }
 }
 // setSize / new_end (:4545-4551), predicate fill (:4555-4556), clean_tail (:4482-4493).
 // The reference compacts every substep; without a phase change that is an identity except
 // that it zeroes scan_index in the tail and, if a link pass wrote into tail slots, resets
 // them (`full_clean`), which is what this kernel does in that case.
+// The tail clean only has to reach the slots that can differ from a clean slot: those that
+// held a particle before this compaction (below the set's size plus the particles it
+// gained) and those not known clean since the last clean (DevState::clean_hi; a call's
+// first compaction and any link pass that wrote past a set's end, tail_dirty, clean the
+// whole tail).  A slot at or above both already holds what the clean writes.
 __global__ void k_compact_finish(DevParams P, DevState* S, snowb_particle_data sph, snowb_particle_data dem,
                                  uint32_t full)
 {
     const bool full_clean = S->changed || S->tail_dirty;
     const uint32_t sn = S->new_sph, dn = S->new_dem, M = P.maxc;
+    const uint32_t hs = S->tail_dirty ? full : umin32(full, umax32(S->clean_hi[0], S->n_sph + S->n_melt));
+    const uint32_t hd = S->tail_dirty ? full : umin32(full, umax32(S->clean_hi[1], S->n_dem + S->n_freeze));
     GRID_LOOP(t, 2 * full) {
         const bool w = t < full;
         const uint32_t i = w ? t : t - full;
@@ -174,7 +220,7 @@ __global__ void k_compact_finish(DevParams P, DevState* S, snowb_particle_data s
             if (full_clean) d.predicate[i] = 1;
         } else {
             d.scan_index[i] = 0;
-            if (full_clean) {
+            if (full_clean && i < (w ? hs : hd)) {
                 d.predicate[i] = 0; d.trackId[i] = 0;
                 reset_records(d, i, M);
             }
@@ -184,9 +230,13 @@ __global__ void k_compact_finish(DevParams P, DevState* S, snowb_particle_data s
 }
 __global__ void k_commit_sizes(DevState* S)
 {
-    if (blockIdx.x == 0 && threadIdx.x == 0 && S->changed) {
-        S->n_sph = S->new_sph; S->n_dem = S->new_dem;
-        S->moved[0] = 1u; S->moved[1] = 1u;   // compacted sets: sort both in full
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        // after a clean every slot past the new sizes is clean
+        if (S->changed || S->tail_dirty) { S->clean_hi[0] = S->new_sph; S->clean_hi[1] = S->new_dem; }
+        if (S->changed) {
+            S->n_sph = S->new_sph; S->n_dem = S->new_dem;
+            S->moved[0] = 1u; S->moved[1] = 1u;   // compacted sets: sort both in full
+        }
     }
 }
 __global__ void k_clear_tail_flag(DevState* S)

@@ -310,6 +310,7 @@ static bool g_prof = false;
 static uint64_t g_launches = 0;
 static std::vector<ProfRec> g_prof_pool;
 static size_t g_prof_used = 0;
+static size_t g_prof_last_substep = 0;   // pool index of the last substep run outside a graph
 static bool g_capturing = false;
 
 static void prof_begin(const char* name)
@@ -603,6 +604,7 @@ static int tape_hook(const StepArgs& a, int kind, int it)
 // Returns SNOWB_OK; stops early after stage `stop_after` (0 = complete).
 static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool step_dem)
 {
+    if (g_prof && !g_capturing) g_prof_last_substep = g_prof_used;
     Ctx& c = g_ctx;
     DevState* S = c.S;
     const uint32_t full = a.full, cap = g_ctx.cap;
@@ -729,10 +731,11 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
         TRY(scan(a.sph->predicate, nullptr, full, full, c.sbsum, a.sph->scan_index, &S->new_sph, nullptr));
         TRY(scan(a.dem->predicate, nullptr, full, full, c.sbsum + sb_stride, a.dem->scan_index, &S->new_dem, nullptr));
         LAUNCH(k_shuffle_records, full, 256, P, S, *a.dem);
-        LAUNCH(k_copy_to_buffer, full, 256, P, S, *a.sph, *a.buf, full, scn.sph, scn.buf);
-        LAUNCH(k_scatter_set, full, 256, P, S, *a.sph, *a.buf, full, scn.sph, scn.buf, 0);
-        LAUNCH(k_copy_to_buffer, full, 256, P, S, *a.dem, *a.buf, full, scn.dem, scn.buf);
-        LAUNCH(k_scatter_set, full, 256, P, S, *a.dem, *a.buf, full, scn.dem, scn.buf, ref ? 0 : 1);
+        const uint64_t cw = (uint64_t)full * (P.maxc + 1);   // a thread per particle and per link slot
+        LAUNCH(k_copy_to_buffer, cw, 256, P, S, *a.sph, *a.buf, full, scn.sph, scn.buf);
+        LAUNCH(k_scatter_set, cw, 256, P, S, *a.sph, *a.buf, full, scn.sph, scn.buf, 0);
+        LAUNCH(k_copy_to_buffer, cw, 256, P, S, *a.dem, *a.buf, full, scn.dem, scn.buf);
+        LAUNCH(k_scatter_set, cw, 256, P, S, *a.dem, *a.buf, full, scn.dem, scn.buf, ref ? 0 : 1);
         LAUNCH(k_compact_finish, 2 * full, 256, P, S, *a.sph, *a.dem, full);
         LAUNCH1(k_commit_sizes, S);
         LAUNCH(k_update_records, (uint64_t)P.maxc * full, 256, P, S, *a.dem);
@@ -2310,6 +2313,31 @@ int snowb_profile_end(char* out, size_t cap)
         out[n] = 0;
         if (txt.size() >= cap) return fail(SNOWB_ERR_INVALID, "profile buffer too small");
     }
+    return SNOWB_OK;
+}
+
+int snowb_profile_timeline(char* out, size_t cap)
+{
+    if (!out || cap == 0) return fail(SNOWB_ERR_INVALID, "null buffer");
+    if (!g_prof) return fail(SNOWB_ERR_INVALID, "profiling is off");
+    CUDA_TRY(cudaStreamSynchronize(g_stream));
+    if (g_graph.stream) CUDA_TRY(cudaStreamSynchronize(g_graph.stream));
+    // a graph replay re-records its events: they hold the last replay's times
+    const size_t n = g_graph.prof_replayed ? g_graph.prof_pairs : g_prof_used;
+    const size_t first = g_graph.prof_replayed ? 0 : (g_prof_last_substep < n ? g_prof_last_substep : 0);
+    std::string txt;
+    for (size_t k = first; k < n; ++k) {
+        float t0 = 0.f, t1 = 0.f;
+        CUDA_TRY(cudaEventElapsedTime(&t0, g_prof_pool[first].a, g_prof_pool[k].a));
+        CUDA_TRY(cudaEventElapsedTime(&t1, g_prof_pool[first].a, g_prof_pool[k].b));
+        char line[160];
+        std::snprintf(line, sizeof line, "%s %.4f %.4f\n", g_prof_pool[k].name, t0, t1);
+        txt += line;
+    }
+    const size_t m = txt.size() < cap - 1 ? txt.size() : cap - 1;
+    std::memcpy(out, txt.data(), m);
+    out[m] = 0;
+    if (txt.size() >= cap) return fail(SNOWB_ERR_INVALID, "timeline buffer too small");
     return SNOWB_OK;
 }
 

@@ -1355,6 +1355,7 @@ __global__ void k_set_state(DevState* S, uint32_t ns, uint32_t nd, uint32_t nb)
         // ... and the particles: the first sort point of a call sorts both sets in full
         for (int k = 0; k < 2; ++k) { S->moved[k] = 1u; S->sorts_full[k] = 0u; S->sorts_kept[k] = 0u; }
         for (int c = 0; c < 8; ++c) S->sc_count[c] = 0u;
+        S->clean_hi[0] = SNOWB_UMAX; S->clean_hi[1] = SNOWB_UMAX;
     }
 }
 // batched runs: every live slot's scene id must name a scene of the batch
