@@ -79,21 +79,20 @@ __global__ void k_phase_flags(DevParams P, const DevState* __restrict__ S, snowb
         }
     }
 }
-__global__ void k_phase_count(DevState* S)
-{
-    if (blockIdx.x == 0 && threadIdx.x == 0) S->changed = (S->n_freeze + S->n_melt) != 0u;
-}
-// freezing (:4416-4449) and melting (:4387-4414) with ranked targets
 // scene ids of batched runs travel with the particles (null pointers: one scene)
 struct SceneIds {
     uint32_t *sph, *dem, *buf;
 };
-__global__ void k_phase_move(DevParams P, const DevState* __restrict__ S, snowb_particle_data sph,
+// freezing (:4416-4449) and melting (:4387-4414) with ranked targets, and the phase-change
+// flag: every block derives it from the counts, block 0 stores it for the later passes
+__global__ void k_phase_move(DevParams P, DevState* __restrict__ S, snowb_particle_data sph,
                              snowb_particle_data dem, const uint32_t* __restrict__ fl_s,
                              const uint32_t* __restrict__ rk_s, const uint32_t* __restrict__ fl_d,
                              const uint32_t* __restrict__ rk_d, SceneIds sc)
 {
-    if (S->changed == 0) return;
+    const bool changed = (S->n_freeze + S->n_melt) != 0u;
+    if (blockIdx.x == 0 && threadIdx.x == 0) S->changed = changed ? 1u : 0u;
+    if (!changed) return;
     const uint32_t ns = S->n_sph, nd = S->n_dem, M = P.maxc;
     GRID_LOOP(t, ns + nd) {
         if (t < ns) {
@@ -117,22 +116,6 @@ __global__ void k_phase_move(DevParams P, const DevState* __restrict__ S, snowb_
         }
     }
 }
-// shuffle_useless_record (:4068-4111): drop links to particles that left the snow set
-__global__ void k_shuffle_records(DevParams P, const DevState* __restrict__ S, snowb_particle_data dem)
-{
-    if (S->changed == 0) return;
-    const uint32_t nd = S->n_dem, M = P.maxc;
-    GRID_LOOP(i, nd) {
-        for (uint32_t s = M * i; s < (i + 1) * M; ++s) {
-            const uint32_t r = dem.connect_record[s];
-            if (r < nd && dem.predicate[r] == 0) {
-                dem.connect_record[s] = SNOWB_UMAX;
-                dem.connect_length[s] = 0.f;
-                dem.iter_end[i]--;
-            }
-        }
-    }
-}
 // Compaction moves the kept particles to their ranks (scan_index).  A kept particle with
 // no removed one before it stays where it is, and copying it out and back, as the
 // reference's copy_to_target and scatter do for every slot, leaves it unchanged; so both
@@ -143,12 +126,13 @@ __device__ __forceinline__ bool compaction_moves(const snowb_particle_data& d, u
 {
     return d.predicate[i] == 1 && d.scan_index[i] != i;
 }
-// copy_to_target (:4451-4460) into the caller's phase-change buffer
+// copy_to_target (:4451-4460) into the caller's phase-change buffer.  removed: the
+// number of particles the set loses (none: no particle moves)
 __global__ void k_copy_to_buffer(DevParams P, const DevState* __restrict__ S, snowb_particle_data d,
                                  snowb_particle_data buf, uint32_t full, const uint32_t* __restrict__ sid,
-                                 uint32_t* __restrict__ sid_buf)
+                                 uint32_t* __restrict__ sid_buf, const uint32_t* __restrict__ removed)
 {
-    if (S->changed == 0) return;
+    if (S->changed == 0 || *removed == 0) return;
     const uint32_t M = P.maxc;
     GRID_LOOP(k, full * (M + 1)) {
         if (k < full) {
@@ -167,11 +151,13 @@ __global__ void k_copy_to_buffer(DevParams P, const DevState* __restrict__ S, sn
 // count, iter_end = t*M + count; the reference copies iter_end verbatim (Q13).  A particle
 // that stays keeps its iter_end either way.
 __global__ void k_scatter_set(DevParams P, DevState* S, snowb_particle_data d, snowb_particle_data buf, uint32_t full,
-                              uint32_t* __restrict__ sid, const uint32_t* __restrict__ sid_buf, int rebase)
+                              uint32_t* __restrict__ sid, const uint32_t* __restrict__ sid_buf, int rebase,
+                              const uint32_t* __restrict__ removed)
 {
     if (S->changed == 0) return;
     const uint32_t M = P.maxc;
-    GRID_LOOP(k, full * (M + 1)) {
+    // with nothing removed every kept particle stays: only new_index is written
+    GRID_LOOP(k, *removed ? full * (M + 1) : full) {
         if (k < full) {
             const uint32_t i = k;
             if (d.predicate[i] == 1) {
@@ -228,6 +214,8 @@ __global__ void k_compact_finish(DevParams P, DevState* S, snowb_particle_data s
         if (i == 0 && full_clean) *d.new_end = n;
     }
 }
+// The compaction's last launch: the new sizes (a compacted set is sorted in full next),
+// the clean mark of the tails, and the tail flag cleared.
 __global__ void k_commit_sizes(DevState* S)
 {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -235,24 +223,36 @@ __global__ void k_commit_sizes(DevState* S)
         if (S->changed || S->tail_dirty) { S->clean_hi[0] = S->new_sph; S->clean_hi[1] = S->new_dem; }
         if (S->changed) {
             S->n_sph = S->new_sph; S->n_dem = S->new_dem;
-            S->moved[0] = 1u; S->moved[1] = 1u;   // compacted sets: sort both in full
+            S->moved[0] = 1u; S->moved[1] = 1u;
         }
+        S->tail_dirty = 0;
     }
 }
-__global__ void k_clear_tail_flag(DevState* S)
-{
-    if (blockIdx.x == 0 && threadIdx.x == 0) S->tail_dirty = 0;
-}
-// update_record_index (:4114-4125)
+// update_record_index (:4114-4125), after the compaction, with shuffle_useless_record
+// (:4068-4111) folded in: the reference clears, before the compaction, each link to a
+// partner that left the snow set (its record, its length, one off the owner's count).  The
+// link's slot moves with its owner and the partner's new index is then empty, so the same
+// slot is cleared here at the owner's new place; the count's decrement commutes with the
+// compaction's copy or rebase of it.
 __global__ void k_update_records(DevParams P, const DevState* __restrict__ S, snowb_particle_data dem)
 {
     if (S->changed == 0 && S->tail_dirty == 0) return;
     // without a phase change the reference's new_index is the identity below n, empty above
     const bool moved = S->changed != 0;
-    const uint32_t nd = S->n_dem, total = P.maxc * nd;
-    GRID_LOOP(s, total) {
+    const uint32_t nd_old = S->n_dem, nd = moved ? S->new_dem : S->n_dem, M = P.maxc;
+    GRID_LOOP(s, M * nd) {
         const uint32_t r = dem.connect_record[s];
-        if (r != SNOWB_UMAX) dem.connect_record[s] = moved ? dem.new_index[r] : (r < nd ? r : SNOWB_UMAX);
+        if (r == SNOWB_UMAX) continue;
+        if (moved) {
+            const uint32_t nr = dem.new_index[r];
+            if (r < nd_old && nr == SNOWB_UMAX) {
+                dem.connect_length[s] = 0.f;
+                atomicSub(dem.iter_end + s / M, 1u);
+            }
+            dem.connect_record[s] = nr;
+        } else {
+            dem.connect_record[s] = r < nd ? r : SNOWB_UMAX;
+        }
     }
 }
 

@@ -722,24 +722,38 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
     if (a.change_phase) {
         LAUNCH(k_phase_flags, 2 * full, 256, P, S, *a.sph, *a.dem, a.freezing, a.melting, c.fl_s, c.fl_d);
         const uint32_t sb_stride = cap / SCAN_CHUNK + 2;
-        TRY(scan(c.fl_s, n_s, 0, cap, c.sbsum, c.rk_s, &S->n_freeze, nullptr));
-        TRY(scan(c.fl_d, n_d, 0, cap, c.sbsum + sb_stride, c.rk_d, &S->n_melt, nullptr));
-        LAUNCH1(k_phase_count, S);
+        // the two sets' scans share nothing: in a whole substep the snow set's runs beside
+        auto scan_pair = [&](auto&& scan_s, auto&& scan_d) -> int {
+            if (beside) {
+                TRY(on_side(c.side, c.fork, scan_d));
+                TRY(scan_s());
+                TRY(join_side(c.side, c.join));
+            } else {
+                TRY(scan_s());
+                TRY(scan_d());
+            }
+            return SNOWB_OK;
+        };
+        TRY(scan_pair([&]() { return scan(c.fl_s, n_s, 0, cap, c.sbsum, c.rk_s, &S->n_freeze, nullptr); },
+                      [&]() { return scan(c.fl_d, n_d, 0, cap, c.sbsum + sb_stride, c.rk_d, &S->n_melt, nullptr); }));
         LAUNCH(k_phase_move, 2 * full, 256, P, S, *a.sph, *a.dem, c.fl_s, c.rk_s, c.fl_d, c.rk_d, scn);
         // compact_and_clean (:4495-4589): predicate scans run every substep (they define
         // scan_index), the data movement only after a phase change.
-        TRY(scan(a.sph->predicate, nullptr, full, full, c.sbsum, a.sph->scan_index, &S->new_sph, nullptr));
-        TRY(scan(a.dem->predicate, nullptr, full, full, c.sbsum + sb_stride, a.dem->scan_index, &S->new_dem, nullptr));
-        LAUNCH(k_shuffle_records, full, 256, P, S, *a.dem);
+        TRY(scan_pair(
+            [&]() { return scan(a.sph->predicate, nullptr, full, full, c.sbsum, a.sph->scan_index, &S->new_sph, nullptr); },
+            [&]() {
+                return scan(a.dem->predicate, nullptr, full, full, c.sbsum + sb_stride, a.dem->scan_index, &S->new_dem,
+                            nullptr);
+            }));
         const uint64_t cw = (uint64_t)full * (P.maxc + 1);   // a thread per particle and per link slot
-        LAUNCH(k_copy_to_buffer, cw, 256, P, S, *a.sph, *a.buf, full, scn.sph, scn.buf);
-        LAUNCH(k_scatter_set, cw, 256, P, S, *a.sph, *a.buf, full, scn.sph, scn.buf, 0);
-        LAUNCH(k_copy_to_buffer, cw, 256, P, S, *a.dem, *a.buf, full, scn.dem, scn.buf);
-        LAUNCH(k_scatter_set, cw, 256, P, S, *a.dem, *a.buf, full, scn.dem, scn.buf, ref ? 0 : 1);
+        // the water set loses the freezing particles, the snow set the melting ones
+        LAUNCH(k_copy_to_buffer, cw, 256, P, S, *a.sph, *a.buf, full, scn.sph, scn.buf, &S->n_freeze);
+        LAUNCH(k_scatter_set, cw, 256, P, S, *a.sph, *a.buf, full, scn.sph, scn.buf, 0, &S->n_freeze);
+        LAUNCH(k_copy_to_buffer, cw, 256, P, S, *a.dem, *a.buf, full, scn.dem, scn.buf, &S->n_melt);
+        LAUNCH(k_scatter_set, cw, 256, P, S, *a.dem, *a.buf, full, scn.dem, scn.buf, ref ? 0 : 1, &S->n_melt);
         LAUNCH(k_compact_finish, 2 * full, 256, P, S, *a.sph, *a.dem, full);
-        LAUNCH1(k_commit_sizes, S);
         LAUNCH(k_update_records, (uint64_t)P.maxc * full, 256, P, S, *a.dem);
-        LAUNCH1(k_clear_tail_flag, S);
+        LAUNCH1(k_commit_sizes, S);
     }
     STOP(4);
     if (a.change_phase) {   // the reference sorts again; only a phase change alters the result
