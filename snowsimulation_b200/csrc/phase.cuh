@@ -66,17 +66,27 @@ __device__ __forceinline__ void reset_records(const snowb_particle_data& d, uint
 }
 
 // freeze / melt predicates (:4425, :4396)
+// commit: the heat pass's commit (k_heat_commit: T from new_T, plus the environment
+// term) first, each particle its own, so the flags read the committed temperature
 __global__ void k_phase_flags(DevParams P, const DevState* __restrict__ S, snowb_particle_data sph,
                               snowb_particle_data dem, int freeze, int melt, uint32_t* __restrict__ fl_s,
-                              uint32_t* __restrict__ fl_d)
+                              uint32_t* __restrict__ fl_d, int commit, float dTe, int env_sph, int env_dem)
 {
     const uint32_t ns = S->n_sph, nd = S->n_dem;
     GRID_LOOP(t, ns + nd) {
-        if (t < ns) fl_s[t] = (freeze && sph.T[t] <= P.Tf && sph.contrib[t] >= 0.99f) ? 1u : 0u;
-        else {
-            const uint32_t i = t - ns;
-            fl_d[i] = (melt && dem.T[i] > P.Tf && dem.contrib[i] >= 0.99f) ? 1u : 0u;
+        const bool w = t < ns;
+        const uint32_t i = w ? t : t - ns;
+        const snowb_particle_data& D = w ? sph : dem;
+        float T;
+        if (commit) {
+            T = D.new_T[i];
+            if (w ? env_sph : env_dem) T += dTe;
+            D.T[i] = T;
+        } else {
+            T = D.T[i];
         }
+        if (w) fl_s[i] = (freeze && T <= P.Tf && sph.contrib[i] >= 0.99f) ? 1u : 0u;
+        else fl_d[i] = (melt && T > P.Tf && dem.contrib[i] >= 0.99f) ? 1u : 0u;
     }
 }
 // scene ids of batched runs travel with the particles (null pointers: one scene)
@@ -190,14 +200,25 @@ __global__ void k_scatter_set(DevParams P, DevState* S, snowb_particle_data d, s
 // gained) and those not known clean since the last clean (DevState::clean_hi; a call's
 // first compaction and any link pass that wrote past a set's end, tail_dirty, clean the
 // whole tail).  A slot at or above both already holds what the clean writes.
+// records: also k_update_records' pass (its slots, below the new snow size, are none of
+// the tail slots this pass cleans), in the same launch
+__device__ __forceinline__ void update_record(const DevParams& P, const DevState* S, const snowb_particle_data& dem,
+                                              uint32_t s, bool moved, uint32_t nd_old, uint32_t nd);
 __global__ void k_compact_finish(DevParams P, DevState* S, snowb_particle_data sph, snowb_particle_data dem,
-                                 uint32_t full)
+                                 uint32_t full, int records)
 {
     const bool full_clean = S->changed || S->tail_dirty;
     const uint32_t sn = S->new_sph, dn = S->new_dem, M = P.maxc;
     const uint32_t hs = S->tail_dirty ? full : umin32(full, umax32(S->clean_hi[0], S->n_sph + S->n_melt));
     const uint32_t hd = S->tail_dirty ? full : umin32(full, umax32(S->clean_hi[1], S->n_dem + S->n_freeze));
-    GRID_LOOP(t, 2 * full) {
+    const bool moved = S->changed != 0;
+    const uint32_t nd_old = S->n_dem, nd_rec = moved ? S->new_dem : S->n_dem;
+    const uint32_t nrec = records && full_clean ? M * nd_rec : 0u;
+    GRID_LOOP(t, 2 * full + nrec) {
+        if (t >= 2 * full) {
+            update_record(P, S, dem, t - 2 * full, moved, nd_old, nd_rec);
+            continue;
+        }
         const bool w = t < full;
         const uint32_t i = w ? t : t - full;
         const snowb_particle_data& d = w ? sph : dem;
@@ -234,25 +255,21 @@ __global__ void k_commit_sizes(DevState* S)
 // link's slot moves with its owner and the partner's new index is then empty, so the same
 // slot is cleared here at the owner's new place; the count's decrement commutes with the
 // compaction's copy or rebase of it.
-__global__ void k_update_records(DevParams P, const DevState* __restrict__ S, snowb_particle_data dem)
+__device__ __forceinline__ void update_record(const DevParams& P, const DevState* S, const snowb_particle_data& dem,
+                                              uint32_t s, bool moved, uint32_t nd_old, uint32_t nd)
 {
-    if (S->changed == 0 && S->tail_dirty == 0) return;
-    // without a phase change the reference's new_index is the identity below n, empty above
-    const bool moved = S->changed != 0;
-    const uint32_t nd_old = S->n_dem, nd = moved ? S->new_dem : S->n_dem, M = P.maxc;
-    GRID_LOOP(s, M * nd) {
-        const uint32_t r = dem.connect_record[s];
-        if (r == SNOWB_UMAX) continue;
-        if (moved) {
-            const uint32_t nr = dem.new_index[r];
-            if (r < nd_old && nr == SNOWB_UMAX) {
-                dem.connect_length[s] = 0.f;
-                atomicSub(dem.iter_end + s / M, 1u);
-            }
-            dem.connect_record[s] = nr;
-        } else {
-            dem.connect_record[s] = r < nd ? r : SNOWB_UMAX;
+    const uint32_t r = dem.connect_record[s];
+    if (r == SNOWB_UMAX) return;
+    if (moved) {
+        const uint32_t nr = dem.new_index[r];
+        if (r < nd_old && nr == SNOWB_UMAX) {
+            dem.connect_length[s] = 0.f;
+            atomicSub(dem.iter_end + s / P.maxc, 1u);
         }
+        dem.connect_record[s] = nr;
+    } else {
+        // without a phase change the reference's new_index is the identity below n, empty above
+        dem.connect_record[s] = r < nd ? r : SNOWB_UMAX;
     }
 }
 

@@ -160,6 +160,10 @@ struct Ctx {
              *lf_off = nullptr;
     float4* link_terms = nullptr;         // one interlink term per slot (k_link_terms)
     float4* contact = nullptr;            // two snow contact sums per particle (k_dem_corr<true>)
+    // the snow set's phase-change buffer (the caller's serves the water set), so that the two
+    // sets' compactions run side by side
+    snowb_particle_data pbuf{};
+    uint32_t* psid = nullptr;
     double* epart = nullptr;
     double* eout = nullptr;
     DevState* S = nullptr;
@@ -191,7 +195,11 @@ static void free_ctx(Ctx& c)
     free_set(c.b);
     free_set(c.gen);
     void* ptrs[] = {c.fl_s, c.fl_d, c.rk_s, c.rk_d, c.sbsum, c.active, c.sc_flag, c.sc_list, c.fs, c.fe, c.tmp_vel,
-                    c.epart, c.eout, c.link_terms, c.contact,
+                    c.epart, c.eout, c.link_terms, c.contact, c.psid,
+                    c.pbuf.positions, c.pbuf.predict_positions, c.pbuf.new_positions, c.pbuf.velocity, c.pbuf.force,
+                    c.pbuf.correction, c.pbuf.mass, c.pbuf.massInv, c.pbuf.contrib, c.pbuf.density, c.pbuf.C,
+                    c.pbuf.lambda, c.pbuf.T, c.pbuf.new_T, c.pbuf.trackId, c.pbuf.iter_end, c.pbuf.connect_record,
+                    c.pbuf.connect_length,
                     c.S, c.err_dev, c.nl_e, c.nl_cnt, c.nl2_e, c.nl2_cnt, c.lf_p4, c.lf_sp, c.lf_gi, c.lf_gh,
                     c.lf_sid, c.lf_cs, c.lf_ce, c.lf_off};
     for (void* p : ptrs)
@@ -260,6 +268,17 @@ static int ensure_ctx(uint32_t full, uint32_t nb, uint32_t ncells)
     c.maxc = maxc;
     TRY(dalloc(&c.link_terms, (size_t)c.cap * maxc));
     TRY(dalloc(&c.contact, (size_t)c.cap * 2));
+    {
+        snowb_particle_data& b = c.pbuf;
+        snowb_float3** v3[] = {&b.positions, &b.predict_positions, &b.new_positions, &b.velocity, &b.force,
+                               &b.correction};
+        for (auto p : v3) TRY(dalloc(p, c.cap));
+        float** f1[] = {&b.mass, &b.massInv, &b.contrib, &b.density, &b.C, &b.lambda, &b.T, &b.new_T};
+        for (auto p : f1) TRY(dalloc(p, c.cap));
+        TRY(dalloc(&b.trackId, c.cap)); TRY(dalloc(&b.iter_end, c.cap));
+        TRY(dalloc(&b.connect_record, (size_t)c.cap * maxc)); TRY(dalloc(&b.connect_length, (size_t)c.cap * maxc));
+        TRY(dalloc(&c.psid, c.cap));
+    }
     TRY(dalloc(&c.epart, 4 * 1024)); TRY(dalloc(&c.eout, 4));
     TRY(dalloc(&c.S, 1)); TRY(dalloc(&c.err_dev, 1));
     CUDA_TRY(cudaMemset(c.S, 0, sizeof(DevState)));
@@ -714,13 +733,16 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
     const int bnd_first = !(beside && a.iterations > 0);
     TLAUNCH(k_density<false>, 256, bnd_first ? work3 : 2 * full, 128, P, S, vs, vd, vb, X, ss, sd, sb, NL2, bnd_first);
     STOP(2);
+    // in a whole substep the phase flags pass commits the new temperatures itself
+    const int commit_in_flags = beside && a.temperature && a.change_phase;
     if (a.temperature) {
         TLAUNCH(k_heat, 256, 2 * full, 128, P, S, vs, vd, X, a.dt);
-        LAUNCH(k_heat_commit, 2 * full, 256, S, X, a.dTe, step_sph ? 1 : 0, step_dem ? 1 : 0);
+        if (!commit_in_flags) LAUNCH(k_heat_commit, 2 * full, 256, S, X, a.dTe, step_sph ? 1 : 0, step_dem ? 1 : 0);
     }
     STOP(3);
     if (a.change_phase) {
-        LAUNCH(k_phase_flags, 2 * full, 256, P, S, *a.sph, *a.dem, a.freezing, a.melting, c.fl_s, c.fl_d);
+        LAUNCH(k_phase_flags, 2 * full, 256, P, S, *a.sph, *a.dem, a.freezing, a.melting, c.fl_s, c.fl_d,
+               commit_in_flags, a.dTe, step_sph ? 1 : 0, step_dem ? 1 : 0);
         const uint32_t sb_stride = cap / SCAN_CHUNK + 2;
         // the two sets' scans share nothing: in a whole substep the snow set's runs beside
         auto scan_pair = [&](auto&& scan_s, auto&& scan_d) -> int {
@@ -746,13 +768,22 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
                             nullptr);
             }));
         const uint64_t cw = (uint64_t)full * (P.maxc + 1);   // a thread per particle and per link slot
-        // the water set loses the freezing particles, the snow set the melting ones
-        LAUNCH(k_copy_to_buffer, cw, 256, P, S, *a.sph, *a.buf, full, scn.sph, scn.buf, &S->n_freeze);
-        LAUNCH(k_scatter_set, cw, 256, P, S, *a.sph, *a.buf, full, scn.sph, scn.buf, 0, &S->n_freeze);
-        LAUNCH(k_copy_to_buffer, cw, 256, P, S, *a.dem, *a.buf, full, scn.dem, scn.buf, &S->n_melt);
-        LAUNCH(k_scatter_set, cw, 256, P, S, *a.dem, *a.buf, full, scn.dem, scn.buf, ref ? 0 : 1, &S->n_melt);
-        LAUNCH(k_compact_finish, 2 * full, 256, P, S, *a.sph, *a.dem, full);
-        LAUNCH(k_update_records, (uint64_t)P.maxc * full, 256, P, S, *a.dem);
+        // the water set loses the freezing particles, the snow set the melting ones; in a whole
+        // substep the water set compacts through the caller's buffer beside the snow set
+        // compacting through the library's
+        auto compact_water = [&]() -> int {
+            LAUNCH(k_copy_to_buffer, cw, 256, P, S, *a.sph, *a.buf, full, scn.sph, scn.buf, &S->n_freeze);
+            LAUNCH(k_scatter_set, cw, 256, P, S, *a.sph, *a.buf, full, scn.sph, scn.buf, 0, &S->n_freeze);
+            return SNOWB_OK;
+        };
+        const snowb_particle_data& dbuf = beside ? c.pbuf : *a.buf;
+        uint32_t* dsid = beside ? c.psid : scn.buf;
+        if (beside) TRY(on_side(c.side, c.fork, compact_water));
+        else TRY(compact_water());
+        LAUNCH(k_copy_to_buffer, cw, 256, P, S, *a.dem, dbuf, full, scn.dem, dsid, &S->n_melt);
+        LAUNCH(k_scatter_set, cw, 256, P, S, *a.dem, dbuf, full, scn.dem, dsid, ref ? 0 : 1, &S->n_melt);
+        if (beside) TRY(join_side(c.side, c.join));
+        LAUNCH(k_compact_finish, 2 * full + (uint64_t)P.maxc * full, 256, P, S, *a.sph, *a.dem, full, 1);
         LAUNCH1(k_commit_sizes, S);
     }
     STOP(4);
