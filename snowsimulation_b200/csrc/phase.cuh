@@ -200,8 +200,8 @@ __global__ void k_scatter_set(DevParams P, DevState* S, snowb_particle_data d, s
 // gained) and those not known clean since the last clean (DevState::clean_hi; a call's
 // first compaction and any link pass that wrote past a set's end, tail_dirty, clean the
 // whole tail).  A slot at or above both already holds what the clean writes.
-// records: also k_update_records' pass (its slots, below the new snow size, are none of
-// the tail slots this pass cleans), in the same launch
+// records: also the record update below (update_record_index; its slots, below the new
+// snow size, are none of the tail slots this pass cleans), in the same launch
 __device__ __forceinline__ void update_record(const DevParams& P, const DevState* S, const snowb_particle_data& dem,
                                               uint32_t s, bool moved, uint32_t nd_old, uint32_t nd);
 __global__ void k_compact_finish(DevParams P, DevState* S, snowb_particle_data sph, snowb_particle_data dem,

@@ -868,7 +868,7 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
         };
         if (beside) TRY(on_side(c.side2, c.fork2, pbf_water));
         else TRY(pbf_water());
-        // the snow contact sums, kept apart for k_link_sum, beside the snow PBF pass
+        // the snow contact sums, kept apart for k_link_apply, beside the snow PBF pass
         if (links_beside)
             TRY(on_side(c.side3, c.fork3, [&]() -> int {
                 TLAUNCH(k_dem_corr<true>, 256, full, 128, P, S, vs, vd, vb, X, ss, sd, sb, F, NL, c.contact);
@@ -890,7 +890,7 @@ static int substep(const DevParams& P, const StepArgs& a, bool step_sph, bool st
                 TLAUNCH(k_link_apply, 256, full, 128, P, S, vd, *a.dem, c.link_terms, c.contact, F.correct_dem,
                         step_dem ? 1 : 0, track_d);
             else
-                TLAUNCH(k_link_sum, 256, full, 128, P, S, *a.dem, c.link_terms, nullptr, F.correct_dem);
+                TLAUNCH(k_link_sum, 256, full, 128, P, S, *a.dem, c.link_terms);
         }
         if (beside) TRY(join_side(c.side2, c.join2));
         STOP(base + 5);

@@ -597,7 +597,7 @@ __device__ __forceinline__ void delete_record(const snowb_particle_data& D, uint
 // contact sums are kept apart instead: sums[2o] the water contact (scaled by k_stretch *
 // contrib; +0 without correct_dem), sums[2o+1] the snow-then-boundary contact (scaled by
 // contrib).  That pass reads no correction, so it can run beside the snow PBF pass, and
-// k_link_sum adds both to the correction after the PBF term, in this order.
+// k_link_apply adds both to the correction after the PBF term, in this order.
 template <bool SUMS>
 __global__ void __launch_bounds__(256) k_dem_corr(DevParams P, const DevState* __restrict__ S, SetView vs, SetView vd,
                                                   SetView vb, Sets X, Sorted ss, Sorted sd, Sorted sb, StageFlags F,
@@ -682,11 +682,8 @@ __global__ void __launch_bounds__(256) k_link_terms(DevParams P, const DevState*
         terms[s] = t;
     }
 }
-// sums: the contact sums k_dem_corr kept apart (null: it added them itself), added first,
-// the water one only with correct_dem, as k_dem_corr adds them
 __global__ void __launch_bounds__(256) k_link_sum(DevParams P, const DevState* __restrict__ S,
-                                                  snowb_particle_data dem, const float4* __restrict__ terms,
-                                                  const float4* __restrict__ sums, int correct_dem)
+                                                  snowb_particle_data dem, const float4* __restrict__ terms)
 {
     const uint32_t nd = S->n_dem, M = P.maxc;
     const float3 z = f3(0.f, 0.f, 0.f);
@@ -697,12 +694,7 @@ __global__ void __launch_bounds__(256) k_link_sum(DevParams P, const DevState* _
             if (t.w != 0.f) d = add3(d, xyz(t));
         }
         if (nan3(d)) d = z;
-        float3 acc = ldv3(dem.correction, o);
-        if (sums) {
-            if (correct_dem) acc = add3(acc, xyz(__ldg(sums + 2 * (size_t)o)));
-            acc = add3(acc, xyz(__ldg(sums + 2 * (size_t)o + 1)));
-        }
-        st3(dem.correction, o, add3(acc, d));
+        st3(dem.correction, o, add3(ldv3(dem.correction, o), d));
     }
 }
 
