@@ -293,7 +293,12 @@ static int ensure_ctx(uint32_t full, uint32_t nb, uint32_t ncells)
     CUDA_TRY(cudaStreamCreateWithFlags(&c.side3, cudaStreamNonBlocking));
     CUDA_TRY(cudaEventCreateWithFlags(&c.fork3, cudaEventDisableTiming));
     CUDA_TRY(cudaEventCreateWithFlags(&c.join3, cudaEventDisableTiming));
-    CUDA_TRY(cudaStreamCreateWithFlags(&c.side4, cudaStreamNonBlocking));
+    {   // link formation's serial chains run beside the density pass, which would otherwise
+        // take the SMs first: its stream has the highest priority
+        int least = 0, greatest = 0;
+        CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        CUDA_TRY(cudaStreamCreateWithPriority(&c.side4, cudaStreamNonBlocking, greatest));
+    }
     CUDA_TRY(cudaEventCreateWithFlags(&c.fork4, cudaEventDisableTiming));
     CUDA_TRY(cudaEventCreateWithFlags(&c.ev_view, cudaEventDisableTiming));
     CUDA_TRY(cudaEventCreateWithFlags(&c.ev_links, cudaEventDisableTiming));
@@ -1309,7 +1314,8 @@ static int graph_substeps(const DevParams& P, const StepArgs& a, bool step_sph, 
         e.nodes = nodes;
         e.prof = g_prof;
         e.prof_pairs = g_prof_used;
-        cudaError_t e2 = cudaGraphInstantiate(&e.exec, gr, 0);
+        // kernel nodes keep the priorities of the streams they were captured from
+        cudaError_t e2 = cudaGraphInstantiate(&e.exec, gr, cudaGraphInstantiateFlagUseNodePriority);
         if (e2 != cudaSuccess) {
             cudaGraphDestroy(gr);
             return fail(SNOWB_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e2));
