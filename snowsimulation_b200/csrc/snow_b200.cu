@@ -290,7 +290,12 @@ static int ensure_ctx(uint32_t full, uint32_t nb, uint32_t ncells)
     CUDA_TRY(cudaStreamCreateWithFlags(&c.side2, cudaStreamNonBlocking));
     CUDA_TRY(cudaEventCreateWithFlags(&c.fork2, cudaEventDisableTiming));
     CUDA_TRY(cudaEventCreateWithFlags(&c.join2, cudaEventDisableTiming));
-    CUDA_TRY(cudaStreamCreateWithFlags(&c.side3, cudaStreamNonBlocking));
+    {   // the snow contact sums are the longest of the passes after the density pass when the
+        // neighbour lists grow long: their stream has the highest priority too
+        int least = 0, greatest = 0;
+        CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        CUDA_TRY(cudaStreamCreateWithPriority(&c.side3, cudaStreamNonBlocking, greatest));
+    }
     CUDA_TRY(cudaEventCreateWithFlags(&c.fork3, cudaEventDisableTiming));
     CUDA_TRY(cudaEventCreateWithFlags(&c.join3, cudaEventDisableTiming));
     {   // link formation's serial chains run beside the density pass, which would otherwise
