@@ -376,16 +376,17 @@ __device__ __forceinline__ void acc_WG(const DevParams& P, float& rho, float& gs
 }
 template <bool LAMBDA>
 // with_bnd = 0: water and snow only (the boundary particles' density, C and lambda are then
-// left as they were; a later density+lambda pass of the substep rewrites them)
+// left as they were; a later density+lambda pass of the substep rewrites them).  The water
+// and snow sums take the boundary's terms either way, through its compact sorted copies.
 __global__ void __launch_bounds__(256) k_density(DevParams P, DevState* __restrict__ S, SetView vs, SetView vd,
                                                  SetView vb, Sets X, Sorted ss, Sorted sd, Sorted sb, NList L,
                                                  int with_bnd)
 {
-    const uint32_t ns = S->n_sph, nd = S->n_dem, nb = with_bnd ? S->n_b : 0u;
+    const uint32_t ns = S->n_sph, nd = S->n_dem, nb = S->n_b, nbt = with_bnd ? nb : 0u;
     vs.n = ns; vd.n = nd; vb.n = nb;
     const float3 z = f3(0.f, 0.f, 0.f);
     if (LAMBDA && blockIdx.x == 0 && threadIdx.x == 0) S->far_move = 0u;   // the lists are new
-    GRID_LOOP(t, ns + nd + nb) {
+    GRID_LOOP(t, ns + nd + nbt) {
         float rho, gs = dot3(z, z);
         const snowb_particle_data* D;
         float* lam_s;
