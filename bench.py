@@ -14,7 +14,9 @@ the slowest rank's time.
 
 The line also carries "batched": 64 scenes of uneven size (log-uniform 2k-40k particles)
 stepped as one batch, against the same scenes stepped one after another through the
-plain entry point (--no-batched skips it); "adjoint": a differentiable rollout of config 3
+plain entry point (--no-batched skips it; on N ranks the 64 scenes are split between the
+ranks, each stepping its share as one batch with no exchange inside a step, and the block
+reports all scenes' particle-substeps over the slowest rank's time); "adjoint": a differentiable rollout of config 3
 to frame 60 (240 substeps, forward with checkpoints every 10 + backward) against the same
 substeps run plain (--no-adjoint skips it); "large": 3 frames of the 1.18M-particle
 config 4 in a widened domain (--no-large skips it); "long_window": every frame 0-99 of the
@@ -356,19 +358,30 @@ def reference_gpu_runner(scene_name, warmup, frames):
 
 
 # ----------------------------------------------------------------- batched vs plain
-def batched_compare(frames, dev, seed, flush):
-    """64 scenes of uneven size (log-uniform 2k-40k particles) stepped as one batch, and the
-    same scenes stepped one after another through the plain entry point (each with its
-    own cached substep graph).  Both in the fixed-quirks mode, in which the batch equals
-    the independent runs bit for bit.  Device time with CUDA events per frame."""
+def batched_compare(frames, dev, flush, ws=1, rank=0):
+    """The 64 scenes of config 2 (uneven sizes, log-uniform 2k-40k particles) stepped as one
+    batch, and the same scenes stepped one after another through the plain entry point (each
+    with its own cached substep graph).  Both in the fixed-quirks mode, in which the batch
+    equals the independent runs bit for bit.  Device time with CUDA events per frame.  On
+    several ranks the scenes are split between them (batch.shard_scenes), each rank steps
+    its own share with no exchange inside a step, and combine_batched() joins the per-rank
+    figures after the timed region."""
     import torch
     from snowsimulation_b200 import scene
     from snowsimulation_b200.abi import QUIRKS_FIXED
-    from snowsimulation_b200.batch import BatchSimulation
+    from snowsimulation_b200.batch import BatchSimulation, shard_scenes
     from snowsimulation_b200.world import Simulation
 
-    worlds = scene.config2(seed=seed)
-    n_part = sum(w.n_sph + w.n_dem for w in worlds)
+    every = scene.config2(seed=0)
+    sizes = [w.n_sph + w.n_dem for w in every]
+    mine = shard_scenes(sizes, ws, rank)
+    worlds = [every[i] for i in mine]
+    part = {"frames": frames, "scenes_total": len(every), "particles_total": sum(sizes),
+            "boundary_total": sum(w.n_b for w in every), "scenes": mine,
+            "particle_substeps": sum(sizes[i] for i in mine) * SUBSTEPS * frames,
+            "batch_ms": 0.0, "plain_ms": 0.0, "water_after": [], "snow_after": []}
+    if not worlds:   # fewer scenes than ranks
+        return part
     stream = torch.cuda.current_stream(dev)
 
     def timed(fn):
@@ -392,7 +405,7 @@ def batched_compare(frames, dev, seed, flush):
     for _ in range(3):
         plain_frame()
     torch.cuda.synchronize(dev)
-    plain_ms = timed(plain_frame)
+    part["plain_ms"] = timed(plain_frame)
     del plain
     torch.cuda.empty_cache()
 
@@ -404,17 +417,45 @@ def batched_compare(frames, dev, seed, flush):
     for _ in range(3):
         batch_frame()
     torch.cuda.synchronize(dev)
-    batch_ms = timed(batch_frame)
+    part["batch_ms"] = timed(batch_frame)
     batch.read_sizes()
-    n_b = batch.n_b
+    part["water_after"], part["snow_after"] = batch.scene_counts()
     del batch
     torch.cuda.empty_cache()
-    ps = n_part * SUBSTEPS * frames
+    return part
+
+
+def combine_batched(parts):
+    """The batched block of the bench line from every rank's share (rank order): all ranks'
+    particle-substeps over the slowest rank's device time, for the batch and for the plain
+    scene-by-scene runs, and each scene's live particles after the timed frames."""
+    p0 = parts[0]
+    n_sc, frames = p0["scenes_total"], p0["frames"]
+    owner = {}
+    for r, p in enumerate(parts):
+        for i in p["scenes"]:
+            if i in owner:
+                raise RuntimeError("scene %d stepped by ranks %d and %d" % (i, owner[i], r))
+            owner[i] = r
+    if sorted(owner) != list(range(n_sc)):
+        raise RuntimeError("scenes not stepped by any rank: %s" % sorted(set(range(n_sc)) - set(owner)))
+    ps = sum(p["particle_substeps"] for p in parts)
+    b_ms = max(p["batch_ms"] for p in parts)
+    p_ms = max(p["plain_ms"] for p in parts)
+    water, snow = [0] * n_sc, [0] * n_sc
+    for p in parts:
+        for k, i in enumerate(p["scenes"]):
+            water[i], snow[i] = p["water_after"][k], p["snow_after"][k]
     return {"workload": "config2: %d scenes, %d water+snow particles (log-uniform 2k-40k per scene) + %d boundary, "
-                        "1 step = 1 frame = %d substeps, fixed quirks" % (len(worlds), n_part, n_b, SUBSTEPS),
-            "frames": frames, "value": ps / (batch_ms / 1000.0), "unit": UNIT, "ms_per_step": batch_ms / frames,
-            "plain_value": ps / (plain_ms / 1000.0), "plain_ms_per_step": plain_ms / frames,
-            "speedup_vs_plain": plain_ms / batch_ms}
+                        "1 step = 1 frame = %d substeps, fixed quirks" % (n_sc, p0["particles_total"],
+                                                                          p0["boundary_total"], SUBSTEPS),
+            "frames": frames, "value": ps / (b_ms / 1000.0), "unit": UNIT, "ms_per_step": b_ms / frames,
+            "plain_value": ps / (p_ms / 1000.0), "plain_ms_per_step": p_ms / frames,
+            "speedup_vs_plain": p_ms / b_ms,
+            "parallelism": "scenes split over %d ranks" % len(parts) if len(parts) > 1 else "single",
+            "scenes_per_rank": [len(p["scenes"]) for p in parts],
+            "particles_per_rank": [p["particle_substeps"] // (SUBSTEPS * frames) for p in parts],
+            "particles_after": {"water": sum(water), "snow": sum(snow)}}
 
 
 # ----------------------------------------------------------------- large scene
@@ -817,15 +858,12 @@ def main():
     del sim
     batched_res = None
     if not args.no_batched:
-        batched_res = batched_compare(min(args.steps, 5), dev, rank, flush)
-        if ws > 1:
-            b_ms, p_ms = slowest([batched_res["ms_per_step"], batched_res["plain_ms_per_step"]], ws, dev)
-            f = batched_res["frames"]
-            ps_rank = batched_res["value"] * batched_res["ms_per_step"] * f / 1000.0
-            batched_res["value"] = job_rate(ps_rank, ws, b_ms * f)
-            batched_res["plain_value"] = job_rate(ps_rank, ws, p_ms * f)
-            batched_res["ms_per_step"], batched_res["plain_ms_per_step"] = b_ms, p_ms
-            batched_res["speedup_vs_plain"] = p_ms / b_ms
+        part = batched_compare(min(args.steps, 5), dev, flush, ws, rank)
+        parts = [part]
+        if ws > 1:   # after the timed frames: every rank's share to every rank
+            parts = [None] * ws
+            dist.all_gather_object(parts, part)
+        batched_res = combine_batched(parts)
 
     large_res = None
     if not args.no_large:

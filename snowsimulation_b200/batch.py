@@ -44,6 +44,25 @@ def layout(n_scenes):
     return sx, total // sx
 
 
+def shard_scenes(sizes, world_size, rank):
+    """Indices (ascending) of the scenes that rank `rank` of `world_size` steps.  The scenes
+    of a batch are independent, so ranks split them with nothing exchanged inside a step:
+    largest first, each scene to the rank holding the fewest particles so far (the lowest
+    rank on a tie).  The split depends on the scene sizes alone, so every rank computes the
+    same one without communicating; every scene lands on exactly one rank, and a rank may
+    get none when there are fewer scenes than ranks."""
+    if world_size < 1 or not 0 <= rank < world_size:
+        raise ValueError("rank %r outside a world of %r" % (rank, world_size))
+    load = [0] * world_size
+    mine = []
+    for i in sorted(range(len(sizes)), key=lambda k: (-int(sizes[k]), k)):
+        r = min(range(world_size), key=lambda q: (load[q], q))
+        load[r] += int(sizes[i])
+        if r == rank:
+            mine.append(i)
+    return sorted(mine)
+
+
 def _check_compatible(worlds):
     w0 = worlds[0]
     for w in worlds[1:]:
@@ -231,6 +250,15 @@ class BatchSimulation:
         _native.check(self.lib.snowb_read_sizes(C.byref(ns), C.byref(nd)))
         self.n_sph, self.n_dem = ns.value, nd.value
         return self.n_sph, self.n_dem
+
+    def scene_counts(self):
+        """(water, snow) live particles per scene, counted on the device from the scene ids."""
+        torch.cuda.synchronize(self.device)
+        out = []
+        for k, n in (("sph", self.n_sph), ("dem", self.n_dem)):
+            ids = self.sid[k][:n].long()
+            out.append([int(x) for x in torch.bincount(ids, minlength=self.n_scenes).cpu()])
+        return tuple(out)
 
     def to_host(self):
         """(HostWorld of the concatenated sets, scene-id arrays)."""

@@ -1,10 +1,11 @@
-"""Host side of batched scenes: scene layout and the pack/unpack of particle sets
-(interlink records and iter_end rebased per scene)."""
+"""Host side of batched scenes: scene layout, the pack/unpack of particle sets
+(interlink records and iter_end rebased per scene) and the split of a batch's scenes
+between ranks."""
 import numpy as np
 import pytest
 
 from snowsimulation_b200 import scene
-from snowsimulation_b200.batch import layout, pack, unpack, scene_state, SET_FIELDS
+from snowsimulation_b200.batch import layout, pack, unpack, scene_state, shard_scenes, SET_FIELDS
 from snowsimulation_b200.scene import UMAX
 
 
@@ -92,3 +93,35 @@ def test_config2_shape():
     assert frac.min() > 0.005 and frac.max() < 0.4
     assert all(w.init_links for w in ws)
     assert len({bytes(w.params) for w in ws}) == 1
+
+
+@pytest.mark.parametrize("ws", [1, 2, 3, 4, 8])
+def test_shard_scenes_covers_each_scene_once(ws):
+    sizes = [w.n_sph + w.n_dem for w in scene.config2(seed=0)]
+    parts = [shard_scenes(sizes, ws, r) for r in range(ws)]
+    flat = sorted(i for p in parts for i in p)
+    assert flat == list(range(len(sizes)))
+    for p in parts:
+        assert p == sorted(p)
+    # largest first to the lightest rank: no rank is heavier than the lightest by more
+    # than the largest scene
+    loads = [sum(sizes[i] for i in p) for p in parts]
+    assert max(loads) - min(loads) <= max(sizes)
+    # the same split on every call (each rank computes it alone)
+    assert parts == [shard_scenes(sizes, ws, r) for r in range(ws)]
+
+
+def test_shard_scenes_more_ranks_than_scenes():
+    sizes = [30, 10, 20]
+    parts = [shard_scenes(sizes, 5, r) for r in range(5)]
+    assert parts == [[0], [2], [1], [], []]
+
+
+def test_shard_scenes_equal_sizes_in_index_order():
+    assert [shard_scenes([5] * 6, 3, r) for r in range(3)] == [[0, 3], [1, 4], [2, 5]]
+
+
+@pytest.mark.parametrize("ws,rank", [(0, 0), (2, 2), (2, -1)])
+def test_shard_scenes_rejects_bad_rank(ws, rank):
+    with pytest.raises(ValueError):
+        shard_scenes([1, 2], ws, rank)

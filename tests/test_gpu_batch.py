@@ -62,6 +62,8 @@ def test_batched_equals_independent(cuda, use_graph):
     bw, sid = b.to_host()
     assert bw.n_sph == sum(len(a[0]["trackId"]) for a in alone)
     assert bw.n_dem == sum(len(a[1]["trackId"]) for a in alone)
+    # live particles per scene, counted on the device from the scene ids
+    assert b.scene_counts() == ([len(a[0]["trackId"]) for a in alone], [len(a[1]["trackId"]) for a in alone])
     _compare(worlds, bw, sid, alone)
 
 
