@@ -1130,16 +1130,29 @@ __global__ void k_heat_commit(const DevState* __restrict__ S, Sets X, float dTe,
 // per-cell helper), then the partials are added to the running total in cell order with
 // shuffles -- the same operations in the same order as one thread would do, with 27-way
 // parallelism for the small sets XSPH works on.
+// Most cells hold no neighbour of a given kind, and their partial is +0 in every component.
+// Adding +0 leaves a float as it is, except -0, which becomes +0 (round to nearest), and
+// doing it again changes nothing; so each run of +0 partials is replaced by one addition
+// of +0, and only the other partials are fetched and added, in cell order.  (A NaN in the
+// total comes from arithmetic here and is already the canonical NaN that +0 keeps.)
 __device__ __forceinline__ float3 warp_ordered_sum(float3 acc, float3 part)
 {
-#pragma unroll 1
-    for (int k = 0; k < 27; ++k) {
+    const bool nz = (__float_as_uint(part.x) | __float_as_uint(part.y) | __float_as_uint(part.z)) != 0u;
+    uint32_t m = __ballot_sync(0xffffffffu, nz) & ((1u << 27) - 1u);
+    const float3 zero = f3(0.f, 0.f, 0.f);
+    int next = 0;   // cells before `next` are in the total
+    while (m) {
+        const int k = __ffs(m) - 1;
+        m &= m - 1u;
+        if (k > next) acc = add3(acc, zero);   // the +0 partials of cells next .. k-1
         float3 v;
         v.x = __shfl_sync(0xffffffffu, part.x, k);
         v.y = __shfl_sync(0xffffffffu, part.y, k);
         v.z = __shfl_sync(0xffffffffu, part.z, k);
         acc = add3(acc, v);
+        next = k + 1;
     }
+    if (next < 27) acc = add3(acc, zero);
     return acc;
 }
 
