@@ -16,12 +16,13 @@ The line also carries "batched": 64 scenes of uneven size (log-uniform 2k-40k pa
 stepped as one batch, against the same scenes stepped one after another through the
 plain entry point (--no-batched skips it; on N ranks the 64 scenes are split between the
 ranks, each stepping its share as one batch with no exchange inside a step, and the block
-reports all scenes' particle-substeps over the slowest rank's time); "adjoint": a differentiable rollout of config 3
-to frame 60 (240 substeps, forward with checkpoints every 10 + backward) against the same
-substeps run plain (--no-adjoint skips it); "large": 3 frames of the 1.18M-particle
-config 4 in a widened domain (--no-large skips it); "long_window": every frame 0-99 of the
-scene from rest (--long-frames); "fp64_error": the first 24 frames against the FP64 oracle
-with the heat-energy drift of both runs (--fp64-frames, --no-fp64).
+reports all scenes' particle-substeps over the slowest rank's time); "adjoint": a
+differentiable rollout of config 3 to frame 60 (240 substeps, forward with checkpoints
+every 10 + backward) against the same substeps run plain (--no-adjoint skips it); "large":
+3 frames of the 1.18M-particle config 4 in a widened domain (--no-large skips it);
+"long_window": every frame 0-99 of the scene from rest (--long-frames); "fp64_error": the
+first 24 frames against the FP64 oracle with the heat-energy drift of both runs
+(--fp64-frames, --no-fp64).
 
 --precision-study runs the config-4 precision study instead (FP64 oracle comparison of the
 first frames, GPU heat-energy drift over 600 frames, per-kernel HBM fractions).
