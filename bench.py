@@ -2,8 +2,8 @@
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
-Workload: the README-scale scene (5,888 water + 147,928 snow particles, 52,016 boundary
-particles, seeded synthetic lattice), one step = one frame = 4 substeps of dt = 1/240 s
+Workload: the scene at the scale of the reference's published figures (5,888 water +
+147,928 snow particles, 52,016 boundary particles, seeded synthetic lattice), one step = one frame = 4 substeps of dt = 1/240 s
 with 3 solver iterations.  `value` is timed on the device with CUDA events around each
 frame (state resident in HBM, L2 flushed between frames); `e2e` goes through the C-ABI
 call with the per-frame host I/O of the reference (positions, velocities and temperatures

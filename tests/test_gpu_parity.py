@@ -82,7 +82,8 @@ def test_config0_frames_bit_exact(cuda, quirks):
 
 
 def test_config1_substep_bit_exact(cuda):
-    """Full README-scale scene (153,816 particles): initial links and one substep."""
+    """Full config-1 scene, the scale of the reference's published figures (153,816
+    particles): initial links and one substep."""
     o, g = _pair(scene.config1(), QUIRKS_REFERENCE)
     _assert_same(o, g, "config1 initial links")
     o.step(); g.step()
